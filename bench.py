@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Throughput of the plain-DEM frame step (DEM element-steps/s) on one B200 per rank.
+
+Workload: the large seeded field (1.5 x 1.5 km at ~70 %, power-law floes
+tessellated into ~245k elements, ~826k bonds, dilation 0.05 m), 7-vertex
+60 x 12 m hull on a piecewise-linear path at 2.5 m/s, 10 substeps of 0.005 s
+per 0.05 s frame, fp32.  A step is one frame (10 substeps) of the whole
+field; ``--steps`` defaults to 1000 frames = the workload's 10,000 substeps.
+
+* ``value``        element-steps/s = n * substeps * frames / device time, inputs
+                   resident in HBM, L2 flushed (256 MB write) before every frame,
+                   each frame timed with CUDA events on the launch stream;
+* ``e2e``          the same metric through the public API (``scan_segment``) with
+                   host buffers: per frame the setpoint row and v_water (n,2) are
+                   copied from pinned host memory and the frame's history (positions,
+                   rotations, bond_intact, eta, submergence, J, F) is copied back;
+* ``roofline``     algorithmic bytes per frame / mean frame time vs measured HBM;
+* ``cpu_baseline`` the NumPy oracle (float64, restated broad phase) on a window
+                   of the same field, on this host, one core.
+
+``--impl reference`` times the oracle port alone (the reference itself is JAX,
+which this image cannot run) with a process per host core, each on its own
+window of the field.  Multi-GPU (torchrun) runs independent replicas, one per
+rank ("scaling": "weak"); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "mbd-icenav_b200"))
+
+METRIC = "DEM elem-steps/s"
+UNIT = "elem-steps/s"
+N_SUB = 10
+DT = 0.05
+START_FRAME = 400  # the ship is ~60 m into the field by then, so contacts occur
+
+
+def _pkg():
+    import _pkg as loader
+    return loader.load_package()
+
+
+def cache_dir():
+    d = os.environ.get("MBD_ICENAV_CACHE", "/tmp/mbd_icenav_b200_cache")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def load_field(name: str, seed: int):
+    """Seeded field, cached as .npz for later runs in the same container."""
+    import numpy as np
+    from mbd_icenav_b200 import scene
+    path = os.path.join(cache_dir(), f"{name}_{seed}.npz")
+    if os.path.exists(path):
+        z = np.load(path, allow_pickle=False)
+        offs = z["poly_off"]
+        verts = z["poly_verts"]
+        polys = [verts[offs[i]:offs[i + 1]] for i in range(len(offs) - 1)]
+        f = scene.make_field.__globals__["IceField"](
+            name=name, polygons=polys, centroids=z["centroids"], bonds=[tuple(b) for b in z["bonds"].tolist()],
+            thicknesses=z["thicknesses"], parent_ids=z["parent_ids"], ship_length=float(z["ship"][0]),
+            ship_beam=float(z["ship"][1]),
+            ship_props=scene.ShipProperties(length=float(z["ship"][0]), beam=float(z["ship"][1]), draft=4.0),
+            hull_local=z["hull"], trajectory=z["trajectory"], current=tuple(z["current"].tolist()),
+            dt=DT, n_ice_steps=N_SUB, n_frames=len(z["trajectory"]) - 2, domain=tuple(z["domain"].tolist()))
+        return f
+    f = scene.make_field(name, seed=seed, n_frames=START_FRAME + 3000)
+    offs = np.cumsum([0] + [len(p) for p in f.polygons])
+    np.savez(path + ".tmp.npz", poly_off=offs, poly_verts=np.concatenate(f.polygons), centroids=f.centroids,
+             bonds=np.array(f.bonds, np.int64), thicknesses=f.thicknesses, parent_ids=f.parent_ids,
+             ship=np.array([f.ship_length, f.ship_beam]), hull=f.hull_local, trajectory=f.trajectory,
+             current=np.array(f.current), domain=np.array(f.domain))
+    os.replace(path + ".tmp.npz", path)
+    return f
+
+
+def algorithmic_bytes_per_frame(n: int, nb: int, V: int, k: int) -> int:
+    """Bytes each frame must move at minimum, fp32, bool = 1 B, i32 = 4 B.
+
+    Per substep and element: read pos 8 + vel 8 + rot 4 + w 4 + sub 4 + active 1
+    + mass 4 + inertia 4 + radius 4 + area 4 + thickness 4 + ship force 8 +
+    v_water 8, write pos 8 + vel 8 + rot 4 + w 4 = 89 B; per substep and bond:
+    i 4 + j 4 + rest length 4 + damage 4 + intact 1 = 17 B.  Per frame: ship
+    contact n (9V + 64) B and the bond update 50 B per bond.
+    """
+    return k * (89 * n + 17 * nb) + n * (9 * V + 64) + 50 * nb
+
+
+def peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(workload: str):
+    """Per-launch DRAM bytes of the frame kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(cache_dir(), f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        import statistics
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), float(p[3]), p[5], p[6], p[7], p[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for nm, v in zip(names, r[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def build_stepper(field, dtype_name: str, device):
+    import numpy as np
+    import torch
+    from mbd_icenav_b200 import sim
+    from mbd_icenav_b200.config import SimulationConfig
+    from mbd_icenav_b200.state import (build_ship_dynamics_data, build_static_data,
+                                       initial_ice_state_arrays, initial_ship_state_arrays, to_device)
+    from mbd_icenav_b200.vessel import SupplyVessel
+    dt = torch.float32 if dtype_name == "f32" else torch.float64
+    cfg = SimulationConfig()
+    static = build_static_data(field.polygons, field.centroids, field.bonds, field.thicknesses,
+                               field.parent_ids, cfg, dilation=0.05, dtype=dt, device=device)
+    sdyn = build_ship_dynamics_data(field.ship_props, cfg, field.ship_length, field.ship_beam,
+                                    field.hull_local, dtype=dt, device=device)
+    sv = SupplyVessel(mass=field.ship_props.mass, length=field.ship_length)
+    fs = sim.make_frame_step(static, cfg, sdyn, field.ship_length, field.ship_beam, N_SUB, DT, DT / N_SUB,
+                             False, sv.B, sv.T_n, device=device, dtype=dt)
+    st = to_device(initial_ice_state_arrays(field.n, field.centroids, len(field.bonds), field.parent_ids), dt, device)
+    eta0 = field.trajectory[START_FRAME]
+    sh = to_device(initial_ship_state_arrays(eta0[:2], float(eta0[2])), dt, device)
+    return fs, st, sh, static
+
+
+def run_ours(args, rank: int, world: int):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    _pkg()
+    device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(device)
+    field = load_field(args.config, args.seed)
+    fs, st, sh, static = build_stepper(field, args.dtype, device)
+    dt = fs.dtype
+    n, nb, V = fs.n, fs.n_bonds, fs.max_v
+    K, W = args.steps, args.warmup
+    total_frames = W + K + args.e2e_steps
+    sp_all = torch.as_tensor(field.setpoints(START_FRAME, total_frames), dtype=dt, device=device)
+    vw = torch.zeros((1, n, 2), dtype=dt, device=device)
+    vw[0, :, 0] = float(field.current[0])
+    vw[0, :, 1] = float(field.current[1])
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+
+    fr = 0
+    for _ in range(W):
+        st, sh, _ = fs.scan_segment(st, sh, sp_all[fr:fr + 1], vw, history=False)
+        fr += 1
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with ClockSampler(device.index) as clk:
+        torch.cuda.synchronize()
+        for i in range(K):
+            flush.fill_(i & 0xFF)  # evict L2 (126 MB) before every timed frame
+            starts[i].record(stream)
+            st, sh, _ = fs.scan_segment(st, sh, sp_all[fr:fr + 1], vw, history=False, check=False)
+            ends[i].record(stream)
+            fr += 1
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    rc = fs.lib.dem_sync_status(fs._h, fs._stream())
+    if rc != 0:
+        raise RuntimeError(f"device status {rc}: {fs._error()}")
+    frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_s = sum(frame_ms) / 1e3
+    t = torch.tensor([total_s], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_max = float(t.item())
+    value = world * n * N_SUB * K / total_max
+
+    # end to end through the public API with host buffers
+    E = args.e2e_steps
+    sp_h = sp_all[fr:fr + E].cpu().pin_memory()
+    vw_h = vw.cpu().pin_memory()
+    sp_d = torch.empty((1, 6), dtype=dt, device=device)
+    vw_d = torch.empty_like(vw)
+    outs_h = None
+    h2d = sp_d.numel() * sp_d.element_size() + vw_d.numel() * vw_d.element_size()
+    d2h = 0
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(E):
+        sp_d.copy_(sp_h[i:i + 1], non_blocking=True)
+        vw_d.copy_(vw_h, non_blocking=True)
+        st, sh, hist = fs.scan_segment(st, sh, sp_d, vw_d, history=True, check=False)
+        if outs_h is None:
+            outs_h = [torch.empty(h.shape, dtype=h.dtype, pin_memory=True) for h in hist]
+            d2h = sum(h.numel() * h.element_size() for h in hist)
+        for hh, hd in zip(outs_h, hist):
+            hh.copy_(hd, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = e0.elapsed_time(e1) / 1e3
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * N_SUB * E / float(t.item())
+    rc = fs.lib.dem_sync_status(fs._h, fs._stream())
+    if rc != 0:
+        raise RuntimeError(f"device status {rc}: {fs._error()}")
+    info = fs.info()
+
+    if rank != 0:
+        return None
+    bpf = algorithmic_bytes_per_frame(n, nb, V, N_SUB)
+    mean_s = total_s / K
+    achieved = bpf / mean_s / 1e9
+    peak, peak_kind = peak_hbm()
+    workload = f"{args.config}-seed{args.seed}-{args.dtype}"
+    traffic = committed_traffic(workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * total_max / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.dtype, "data": "synthetic (seeded field generator)",
+        "config": {"workload": f"plain DEM, {args.config} field: {n} elements, {nb} bonds, max_v {V}, "
+                               f"{N_SUB} substeps of {DT / N_SUB:g} s per step (frame)",
+                   "elements": n, "bonds": nb, "substeps_per_step": N_SUB, "seed": args.seed,
+                   "l2": "flushed before every timed step (256 MB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "launch": "one cooperative persistent kernel per frame",
+                   "neighbor_rebuilds": info["neighbor_rebuilds"],
+                   "max_neighbor_count": info["max_neighbor_count"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": f"{peak_kind} copy bandwidth",
+                     "algorithmic_bytes_per_launch": bpf,
+                     "traffic": traffic},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": E},
+        "gpu_launches": K,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(field, args.cpu_seconds)
+    return line
+
+
+# ── CPU side (the oracle is the checker/baseline only) ─────────────────────────
+
+def _window(field, center, n_keep):
+    import numpy as np
+    d = np.linalg.norm(field.centroids - np.asarray(center)[None, :2], axis=1)
+    keep = np.sort(np.argsort(d)[:n_keep])
+    remap = -np.ones(field.n, np.int64)
+    remap[keep] = np.arange(len(keep))
+    bonds = [(int(remap[i]), int(remap[j])) for i, j in field.bonds if remap[i] >= 0 and remap[j] >= 0]
+    _, parents = np.unique(field.parent_ids[keep], return_inverse=True)
+    return [field.polygons[k] for k in keep], field.centroids[keep], bonds, field.thicknesses[keep], parents
+
+
+def _oracle_for(field, window):
+    import numpy as np
+    from mbd_icenav_b200.config import SimulationConfig
+    from mbd_icenav_b200.state import build_static_arrays, initial_ice_state_arrays, ship_dynamics_arrays
+    from mbd_icenav_b200.vessel import SupplyVessel
+    from oracle.dem_oracle import OShip, OState, Oracle, params_from_config
+    polys, cents, bonds, thick, parents = window
+    cfg = SimulationConfig()
+    sa = build_static_arrays(polys, cents, bonds, thick, parents, cfg, dilation=0.05)
+    sd = ship_dynamics_arrays(field.ship_props, cfg, field.ship_length, field.ship_beam, field.hull_local)
+    sv = SupplyVessel(mass=field.ship_props.mass, length=field.ship_length)
+    o = Oracle(sa, sd, params_from_config(cfg, field.ship_length, field.ship_beam, N_SUB, DT, DT / N_SUB,
+                                          False, sv.T_n), sv.B, np.float64, pair_mode="grid")
+    st = OState(*initial_ice_state_arrays(len(polys), cents, len(bonds), parents))
+    return o, st, OShip
+
+
+def _oracle_frames(field, center, n_keep, seconds, min_frames=1, max_frames=10 ** 9):
+    """Run oracle frames on a window until `seconds` elapse; return (element-steps, seconds)."""
+    import numpy as np
+    o, st, OShip = _oracle_for(field, _window(field, center, n_keep))
+    eta0 = field.trajectory[START_FRAME]
+    sh = OShip(np.array(eta0, float), np.zeros(3), np.zeros(6), np.zeros(3))
+    n = o.n
+    vw = np.tile(np.asarray(field.current, float), (n, 1))
+    sp = field.setpoints(START_FRAME, max(min_frames, 1) + 10000)
+    t0 = time.perf_counter()
+    frames = 0
+    while frames < max_frames and (frames < min_frames or time.perf_counter() - t0 < seconds):
+        st, sh, _ = o.frame_step(st, sh, sp[frames % len(sp), :3], sp[frames % len(sp), 3:], vw,
+                                 st.dpdem_floe_eligible)
+        frames += 1
+    return n * N_SUB * frames, time.perf_counter() - t0, frames, n
+
+
+def cpu_baseline(field, seconds: float):
+    steps, secs, frames, n = _oracle_frames(field, field.trajectory[START_FRAME], 16384, seconds, min_frames=2)
+    return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"NumPy oracle (float64, restated broad phase), {frames} frames x {N_SUB} substeps "
+                      f"on a {n}-element window of the same field around the ship; NumPy runs on one core"}
+
+
+def _ref_worker(argv):
+    name, seed, center, n_keep, seconds, frames = argv
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "mbd-icenav_b200"))
+    _pkg()
+    field = load_field(name, seed)
+    return _oracle_frames(field, center, n_keep, seconds, min_frames=frames, max_frames=frames)
+
+
+def run_reference(args):
+    """Oracle port on all host cores: one process per core, each on its own window."""
+    import multiprocessing as mp
+    import numpy as np
+    _pkg()
+    field = load_field(args.config, args.seed)
+    cores = len(os.sched_getaffinity(0))
+    procs = max(1, min(cores, 32))
+    K, W = args.steps, args.warmup
+    budget = 150.0  # seconds of CPU time the whole run may take
+    per_step = budget / max(K + W, 1)
+    # ~2.5e5 element-steps/s per core for the port (measured); size the windows to fit
+    n_keep = int(np.clip(per_step * 2.5e5 / N_SUB, 256, 16384))
+    rng = np.random.default_rng(args.seed)
+    centers = field.centroids[rng.choice(field.n, procs, replace=False)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        jobs = [(args.config, args.seed, c, n_keep, 0.0, 1) for c in centers]
+        pool.map(_ref_worker, jobs)  # warm-up: field load + one frame per worker
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [(args.config, args.seed, c, n_keep, 0.0, K) for c in centers])
+        wall = time.perf_counter() - t0
+    steps = sum(r[0] for r in res)
+    value = steps / wall
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": K, "warmup": W, "ms_per_step": 1e3 * wall / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded field generator)",
+            "config": {"workload": f"plain DEM, {args.config} field, NumPy oracle port on windows of "
+                                   f"{n_keep} elements x {procs} processes",
+                       "elements_per_process": n_keep, "processes": procs},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                             "sample": f"{K} frames x {N_SUB} substeps on {procs} windows of {n_keep} "
+                                       f"elements (restated broad phase); the reference JAX code cannot "
+                                       f"be installed in this image"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["large", "medium", "small"], default="large")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_ours(args, rank, world)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,220 @@
+/*
+ * dem_b200.h — C ABI of the B200-native DPDEM ice–ship frame step.
+ *
+ * Drop-in boundary for the reference's per-frame physics,
+ * medea_ice_ship/jax_simulation.py:
+ *   - dem_create        replaces the factory _make_frame_step(static, cfg, ship_dyn,
+ *                       ship_length, ship_beam, n_ice_steps, dt, dt_ice,
+ *                       use_auto_icenav, B_mat, T_n)           (jax_simulation.py:302-361)
+ *   - dem_frame_step    replaces the returned frame_step(state, ship_state, setpoint,
+ *                       setpoint_next, v_water, dpdem_eligible, v_water_ship)
+ *                                                              (jax_simulation.py:397-699)
+ *   - dem_scan_segment  replaces JaxSimContext.scan_segment(state, ship_state,
+ *                       setpoints_K6, v_water_Kn2, v_water_ship_K2)
+ *                                                              (jax_simulation.py:1308-1335)
+ *   - dem_destroy / dem_get_error / dem_sync_status have no reference counterpart
+ *     (XLA owns its buffers; JAX raises Python exceptions).
+ *
+ * Array conventions (all arrays are DEVICE pointers owned by the caller):
+ *   - layouts are those of IceState / ShipState / IceStaticData
+ *     (medea_ice_ship/jax_ice_state.py:31-96): (n,2) arrays are row-major interleaved
+ *     xy, booleans are one byte (0/1), indices are int32;
+ *   - every floating-point array has the handle's dtype (DEM_F32 or DEM_F64);
+ *   - the library owns only its scratch (broad-phase grid, neighbour lists, bond CSR,
+ *     per-frame reductions, barrier words and the device status word).
+ *
+ * Semantics: functional like the reference — inputs are never modified, outputs
+ * are written to caller buffers.  Output element-kinematics buffers
+ * (positions, velocities, rotations, angular_vels) must not alias the inputs
+ * (DEM_ERR_ALIAS); every other output may alias its input.
+ *
+ * Errors: every call returns a status.  Launch/argument errors are returned
+ * directly.  Conditions found on the device (neighbour capacity exceeded, a grid
+ * barrier that waited past its limit) are written to a device status word that
+ * dem_sync_status reads; the step's inputs are untouched, so the caller may grow
+ * capacities (dem_set_capacity) and re-run the same call.  Kernels never trap.
+ *
+ * Threading: a handle is bound to one device and is not thread-safe.  Calls that
+ * overlap on the GPU (two streams) race on the handle's scratch.
+ */
+#ifndef DEM_B200_H
+#define DEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DEM_OK 0
+#define DEM_ERR_INVALID 1   /* bad argument, shape or null pointer          */
+#define DEM_ERR_CUDA 2      /* a CUDA runtime call failed                    */
+#define DEM_ERR_CAPACITY 3  /* neighbour / grid-bucket capacity exceeded     */
+#define DEM_ERR_TIMEOUT 4   /* a grid barrier wait exceeded its time limit   */
+#define DEM_ERR_ALIAS 5     /* an element-kinematics output aliases an input */
+
+#define DEM_F32 0
+#define DEM_F64 1
+
+#define DEM_LAUNCH_PERSISTENT 0  /* one cooperative launch per call, device-side grid barriers */
+#define DEM_LAUNCH_PHASED 1      /* one launch per phase (neighbour list rebuilt every substep) */
+
+typedef struct DemHandle DemHandle;
+
+/* Scalar constants of the frame step: the closure constants of _make_frame_step
+ * (jax_simulation.py:325-361), the IceProperties constants it reads
+ * (properties.py:6-12) and the ShipDynamicsData matrices (jax_ice_state.py:99-116). */
+typedef struct DemParams {
+    double half_len, half_beam;             /* analytic hull half-length / half-beam [m]   */
+    int32_t n_edge_samples;                 /* samples per polygon edge (cfg default 4)      */
+    int32_t n_ice_steps;                    /* substeps per frame                            */
+    double dt, dt_ice;                      /* frame and substep time steps [s]              */
+    double bond_stiffness_factor;
+    double hertz_factor, hertz_exponent, ice_ice_friction, friction_cap;
+    double c_d_drag, drag_ref_thickness, linear_drag_factor, drag_coefficient_moment;
+    double angular_damping, angular_cap_lo, angular_cap_hi;
+    double velocity_clip, position_clip;
+    double vc_surge, vc_sway, vc_yaw;       /* ship velocity clip                            */
+    double pen_crit_ref, pen_crit_thickness_ref;
+    double w_contact_cap, w_contact_radius_factor, side_push_factor;
+    double submergence_rate, submergence_pen_cap, rise_time_const;
+    double effective_strength_collision, max_fracture_thickness;
+    int32_t has_max_ship_ice_force;         /* 0: cfg.max_ship_ice_force is None             */
+    int32_t use_auto_icenav;
+    double max_ship_ice_force;
+    double ice_brake_threshold;
+    double bond_cohesion, bond_internal_friction, bond_G_c_I, bond_G_c_II, bond_eta_bk;
+    double youngs_modulus, water_density, flexural_strength_base;
+    double T_n;
+    double B_mat[18];                       /* (3,6) thruster configuration, row-major       */
+    double M3inv[9], D3[9], Kp[9], Kd[9], Ki[9];
+    double B_pinv[18];                      /* (6,3) row-major                               */
+    double n_max[6];
+    /* broad phase (no reference counterpart: the reference evaluates all pairs) */
+    double skin;                            /* Verlet skin [m]; 0 = rebuild every substep    */
+    int32_t max_neighbors;                  /* neighbour-list capacity per element           */
+    int32_t bucket_capacity;                /* elements per grid-hash bucket                 */
+} DemParams;
+
+/* IceStaticData (jax_ice_state.py:59-96) as device pointers.  pair_i/pair_j are not
+ * taken: the all-pairs contact list is implied and resolved by the broad phase. */
+typedef struct DemStatic {
+    int32_t n, max_v, n_bonds, n_floes, n_hull;
+    const void* local_polys_padded;   /* (n, max_v, 2) */
+    const uint8_t* poly_mask;         /* (n, max_v)    */
+    const int32_t* poly_n_verts;      /* (n,)          */
+    const void* masses;
+    const void* inertia;
+    const void* radii;
+    const void* areas;
+    const void* thicknesses;
+    const int32_t* bond_i;
+    const int32_t* bond_j;
+    const void* rest_lengths;
+    const void* bond_strengths;
+    const void* sigma_bar_bond;
+    const int32_t* initial_floe_of;   /* (n,) parent floe, 0 <= id < n_floes */
+    double k_n, k_s;
+    const void* ship_hull_local;      /* (n_hull, 2) ShipDynamicsData.ship_hull_local */
+} DemStatic;
+
+/* IceState (jax_ice_state.py:31-44). */
+typedef struct DemIceState {
+    void* positions;            /* (n,2) */
+    void* velocities;           /* (n,2) */
+    void* rotations;            /* (n,)  */
+    void* angular_vels;         /* (n,)  */
+    void* submergence;          /* (n,)  */
+    uint8_t* bond_intact;       /* (n_bonds,) */
+    void* bond_damage;
+    void* bond_delta_m_0;
+    void* bond_delta_m_max;
+    void* bond_delta_s;
+    uint8_t* elem_active;       /* (n,) */
+    uint8_t* dpdem_floe_eligible; /* (n_floes,) */
+} DemIceState;
+
+/* ShipState (jax_ice_state.py:47-52). */
+typedef struct DemShipState {
+    void* eta;       /* (3,) */
+    void* nu;        /* (3,) */
+    void* n_actual;  /* (6,) */
+    void* e_int;     /* (3,) */
+} DemShipState;
+
+/* frame_step's diag dict (jax_simulation.py:692-697); any field may be NULL. */
+typedef struct DemDiag {
+    void* pen_max;        /* (n,) */
+    void* force_mag;      /* (n,) */
+    void* F_ice_on_ship;  /* (2,) */
+    void* J_cumul_incr;   /* ()   */
+} DemDiag;
+
+/* scan_segment's stacked history tuple (jax_simulation.py:1316-1324); any field may be NULL. */
+typedef struct DemHistory {
+    void* positions;       /* (K,n,2)      */
+    void* rotations;       /* (K,n)        */
+    uint8_t* bond_intact;  /* (K,n_bonds)  */
+    void* eta;             /* (K,3)        */
+    void* submergence;     /* (K,n)        */
+    void* J_cumul_incr;    /* (K,)         */
+    void* F_ice_on_ship;   /* (K,2)        */
+} DemHistory;
+
+/* Counters for tuning and tests. */
+typedef struct DemInfo {
+    int32_t grid_blocks;        /* cooperative grid size of the persistent kernel  */
+    int32_t threads_per_block;
+    int64_t neighbor_rebuilds;  /* neighbour-list builds since create               */
+    int32_t max_neighbor_count; /* largest list seen since create                   */
+    int32_t max_bucket_count;   /* fullest grid bucket seen since create            */
+    int32_t hash_buckets;
+    double cell_size;
+} DemInfo;
+
+/* Replaces _make_frame_step (jax_simulation.py:302-361): binds static data and
+ * constants, builds the per-element bond lists and allocates scratch on `device`. */
+int dem_create(const DemParams* params, const DemStatic* static_data, int dtype, int device,
+               DemHandle** out);
+
+/* Replaces frame_step (jax_simulation.py:397-699).  setpoint / setpoint_next (3,),
+ * v_water (n,2), dpdem_eligible (n_floes,) and v_water_ship (2,) are device arrays;
+ * v_water_ship may be NULL (zero current).  `stream` is a cudaStream_t (NULL = default). */
+int dem_frame_step(DemHandle* h, const DemIceState* in, DemIceState* out,
+                   const DemShipState* ship_in, DemShipState* ship_out,
+                   const void* setpoint, const void* setpoint_next, const void* v_water,
+                   const uint8_t* dpdem_eligible, const void* v_water_ship,
+                   DemDiag* diag, void* stream);
+
+/* Replaces JaxSimContext.scan_segment (jax_simulation.py:1308-1335): K frames with
+ * setpoints (K,6) rows [sp, sp_next], v_water (K,n,2), v_water_ship (K,2) or NULL.
+ * Each frame uses the previous frame's dpdem_floe_eligible (jax_simulation.py:1314). */
+int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out,
+                     const DemShipState* ship_in, DemShipState* ship_out, int32_t K,
+                     const void* setpoints_K6, const void* v_water_Kn2,
+                     const void* v_water_ship_K2, DemHistory* hist, void* stream);
+
+/* Synchronise `stream`, return and clear the device status word (DEM_OK if clean). */
+int dem_sync_status(DemHandle* h, void* stream);
+
+/* Grow (or shrink) neighbour-list and grid-bucket capacities; reallocates scratch. */
+int dem_set_capacity(DemHandle* h, int32_t max_neighbors, int32_t bucket_capacity);
+
+/* DEM_LAUNCH_PERSISTENT (default) or DEM_LAUNCH_PHASED; both give identical results. */
+int dem_set_launch_mode(DemHandle* h, int32_t mode);
+
+int dem_get_info(DemHandle* h, DemInfo* info);
+
+/* Copy the last error message (NUL-terminated) into buf. */
+int dem_get_error(DemHandle* h, char* buf, size_t len);
+
+int dem_destroy(DemHandle* h);
+
+/* Library version string, e.g. "dem_b200 0.1 sm_100a". */
+const char* dem_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DEM_B200_H */

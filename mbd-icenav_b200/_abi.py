@@ -1,0 +1,142 @@
+"""ctypes bindings of ``include/dem_b200.h`` (the library's C ABI).
+
+The structures below mirror the header field by field.  ``load_library``
+returns the loaded ``libdem_b200.so`` and raises if it is missing: there is no
+fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB_PATH
+
+DEM_OK = 0
+DEM_ERR_INVALID = 1
+DEM_ERR_CUDA = 2
+DEM_ERR_CAPACITY = 3
+DEM_ERR_TIMEOUT = 4
+DEM_ERR_ALIAS = 5
+DEM_F32 = 0
+DEM_F64 = 1
+DEM_LAUNCH_PERSISTENT = 0
+DEM_LAUNCH_PHASED = 1
+
+_ERR_NAMES = {0: "DEM_OK", 1: "DEM_ERR_INVALID", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_CAPACITY",
+              4: "DEM_ERR_TIMEOUT", 5: "DEM_ERR_ALIAS"}
+
+_d = C.c_double
+_i = C.c_int32
+_vp = C.c_void_p
+_u8p = C.POINTER(C.c_uint8)
+
+
+class DemParams(C.Structure):
+    _fields_ = [
+        ("half_len", _d), ("half_beam", _d),
+        ("n_edge_samples", _i), ("n_ice_steps", _i),
+        ("dt", _d), ("dt_ice", _d),
+        ("bond_stiffness_factor", _d),
+        ("hertz_factor", _d), ("hertz_exponent", _d), ("ice_ice_friction", _d), ("friction_cap", _d),
+        ("c_d_drag", _d), ("drag_ref_thickness", _d), ("linear_drag_factor", _d),
+        ("drag_coefficient_moment", _d),
+        ("angular_damping", _d), ("angular_cap_lo", _d), ("angular_cap_hi", _d),
+        ("velocity_clip", _d), ("position_clip", _d),
+        ("vc_surge", _d), ("vc_sway", _d), ("vc_yaw", _d),
+        ("pen_crit_ref", _d), ("pen_crit_thickness_ref", _d),
+        ("w_contact_cap", _d), ("w_contact_radius_factor", _d), ("side_push_factor", _d),
+        ("submergence_rate", _d), ("submergence_pen_cap", _d), ("rise_time_const", _d),
+        ("effective_strength_collision", _d), ("max_fracture_thickness", _d),
+        ("has_max_ship_ice_force", _i), ("use_auto_icenav", _i),
+        ("max_ship_ice_force", _d), ("ice_brake_threshold", _d),
+        ("bond_cohesion", _d), ("bond_internal_friction", _d), ("bond_G_c_I", _d),
+        ("bond_G_c_II", _d), ("bond_eta_bk", _d),
+        ("youngs_modulus", _d), ("water_density", _d), ("flexural_strength_base", _d),
+        ("T_n", _d),
+        ("B_mat", _d * 18),
+        ("M3inv", _d * 9), ("D3", _d * 9), ("Kp", _d * 9), ("Kd", _d * 9), ("Ki", _d * 9),
+        ("B_pinv", _d * 18), ("n_max", _d * 6),
+        ("skin", _d), ("max_neighbors", _i), ("bucket_capacity", _i),
+    ]
+
+
+class DemStatic(C.Structure):
+    _fields_ = [
+        ("n", _i), ("max_v", _i), ("n_bonds", _i), ("n_floes", _i), ("n_hull", _i),
+        ("local_polys_padded", _vp), ("poly_mask", _vp), ("poly_n_verts", _vp),
+        ("masses", _vp), ("inertia", _vp), ("radii", _vp), ("areas", _vp), ("thicknesses", _vp),
+        ("bond_i", _vp), ("bond_j", _vp), ("rest_lengths", _vp), ("bond_strengths", _vp),
+        ("sigma_bar_bond", _vp), ("initial_floe_of", _vp),
+        ("k_n", _d), ("k_s", _d),
+        ("ship_hull_local", _vp),
+    ]
+
+
+class DemIceState(C.Structure):
+    _fields_ = [(name, _vp) for name in (
+        "positions", "velocities", "rotations", "angular_vels", "submergence", "bond_intact",
+        "bond_damage", "bond_delta_m_0", "bond_delta_m_max", "bond_delta_s", "elem_active",
+        "dpdem_floe_eligible")]
+
+
+class DemShipState(C.Structure):
+    _fields_ = [("eta", _vp), ("nu", _vp), ("n_actual", _vp), ("e_int", _vp)]
+
+
+class DemDiag(C.Structure):
+    _fields_ = [("pen_max", _vp), ("force_mag", _vp), ("F_ice_on_ship", _vp), ("J_cumul_incr", _vp)]
+
+
+class DemHistory(C.Structure):
+    _fields_ = [("positions", _vp), ("rotations", _vp), ("bond_intact", _vp), ("eta", _vp),
+                ("submergence", _vp), ("J_cumul_incr", _vp), ("F_ice_on_ship", _vp)]
+
+
+class DemInfo(C.Structure):
+    _fields_ = [("grid_blocks", _i), ("threads_per_block", _i), ("neighbor_rebuilds", C.c_int64),
+                ("max_neighbor_count", _i), ("max_bucket_count", _i), ("hash_buckets", _i),
+                ("cell_size", _d)]
+
+
+EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
+           "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_get_error",
+           "dem_destroy", "dem_version")
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libdem_b200.so (built by ``build.build_library``); raise if absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python mbd-icenav_b200/build.py` "
+                          "(there is no CPU fallback for the DEM frame step)")
+    lib = C.CDLL(path)
+    H = C.c_void_p
+    lib.dem_create.argtypes = [C.POINTER(DemParams), C.POINTER(DemStatic), _i, _i, C.POINTER(H)]
+    lib.dem_frame_step.argtypes = [H, C.POINTER(DemIceState), C.POINTER(DemIceState),
+                                   C.POINTER(DemShipState), C.POINTER(DemShipState),
+                                   _vp, _vp, _vp, _vp, _vp, C.POINTER(DemDiag), _vp]
+    lib.dem_scan_segment.argtypes = [H, C.POINTER(DemIceState), C.POINTER(DemIceState),
+                                     C.POINTER(DemShipState), C.POINTER(DemShipState), _i,
+                                     _vp, _vp, _vp, C.POINTER(DemHistory), _vp]
+    lib.dem_sync_status.argtypes = [H, _vp]
+    lib.dem_set_capacity.argtypes = [H, _i, _i]
+    lib.dem_set_launch_mode.argtypes = [H, _i]
+    lib.dem_get_info.argtypes = [H, C.POINTER(DemInfo)]
+    lib.dem_get_error.argtypes = [H, C.c_char_p, C.c_size_t]
+    lib.dem_destroy.argtypes = [H]
+    lib.dem_version.restype = C.c_char_p
+    for name in EXPORTS:
+        if name != "dem_version":
+            getattr(lib, name).restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+class DemError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code

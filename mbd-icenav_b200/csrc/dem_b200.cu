@@ -1,0 +1,687 @@
+// dem_b200.cu — C ABI of the DPDEM frame step (see include/dem_b200.h).
+//
+// Host side: validates arguments, builds the per-element bond lists once,
+// owns the scratch, and launches dem_frames_kernel either as one cooperative
+// persistent launch per call or one launch per phase.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dem_b200.h"
+#include "dem_kernels.cuh"
+
+using dem::IcePtrs;
+using dem::KArgs;
+using dem::ShipPtrs;
+
+struct DemHandle {
+    int dtype = DEM_F32;
+    int device = 0;
+    int mode = DEM_LAUNCH_PERSISTENT;
+    DemParams P{};
+    DemStatic S{};
+    size_t esz = 4;
+    int n = 0, V = 0, nb = 0, nf = 0, nh = 0;
+    double r_max = 0.0, hull_r = 0.0, k_n = 0.0, k_s = 0.0, min_bstr = 0.0;
+    double t_samp[dem::kMaxEdgeSamples] = {0};
+    int n_buckets = 0;
+    int grid_blocks = 0;
+    int sm_count = 0;
+    size_t smem = 0;
+    // derived
+    int* boff = nullptr;
+    int2* bslot = nullptr;
+    void* bstiff = nullptr;
+    void* vert_r = nullptr;
+    // scratch
+    int* bcnt = nullptr;
+    int* bitems = nullptr;
+    int2* ecell = nullptr;
+    int* ncnt = nullptr;
+    int* nbr = nullptr;
+    void* pos_ref = nullptr;
+    void* soi = nullptr;
+    void* fraw = nullptr;
+    uint8_t* crack = nullptr;
+    int* fcoll = nullptr;
+    unsigned long long* fmax = nullptr;
+    double* part = nullptr;
+    unsigned* gdisp = nullptr;
+    void* sp_pos[2] = {nullptr, nullptr};
+    void* sp_vel[2] = {nullptr, nullptr};
+    void* sp_rot[2] = {nullptr, nullptr};
+    void* sp_avel[2] = {nullptr, nullptr};
+    // frame ping-pong state for scans
+    void* t_pos = nullptr;
+    void* t_vel = nullptr;
+    void* t_rot = nullptr;
+    void* t_avel = nullptr;
+    void* t_sub = nullptr;
+    uint8_t* t_intact = nullptr;
+    void* t_dmg = nullptr;
+    void* t_dm0 = nullptr;
+    void* t_dmmax = nullptr;
+    void* t_ds = nullptr;
+    uint8_t* t_active = nullptr;
+    uint8_t* t_elig = nullptr;
+    void* ship_tmp = nullptr;  // 2 x 15
+    void* sprow = nullptr;     // (6,) setpoint row of dem_frame_step
+    unsigned* bar = nullptr;
+    int* status = nullptr;
+    long long* stats = nullptr;
+    int* host_status = nullptr;  // pinned
+    std::vector<void*> allocs;
+    std::string err;
+};
+
+namespace {
+
+int set_err(DemHandle* h, int code, const char* fmt, ...) {
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                        \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess)                                                                   \
+            return set_err((h), DEM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e));  \
+    } while (0)
+
+template <typename P>
+int dev_alloc(DemHandle* h, P** ptr, size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return set_err(h, DEM_ERR_CUDA, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    h->allocs.push_back(p);
+    *ptr = reinterpret_cast<P*>(p);
+    return DEM_OK;
+}
+
+void dev_free(DemHandle* h, void* p) {
+    if (!p) return;
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+    if (it != h->allocs.end()) {
+        cudaFree(p);
+        h->allocs.erase(it);
+    }
+}
+
+// numpy.linspace(start, stop, num) with endpoint=True, in float64
+void np_linspace(double start, double stop, int num, double* out) {
+    if (num <= 0) return;
+    if (num == 1) {
+        out[0] = start;
+        return;
+    }
+    const int div = num - 1;
+    const double step = (stop - start) / div;
+    for (int i = 0; i < num; ++i) out[i] = (double)i * step + start;
+    out[num - 1] = stop;
+}
+
+int next_pow2(long long v) {
+    int p = 1;
+    while (p < v && p < (1 << 30)) p <<= 1;
+    return p;
+}
+
+template <typename T>
+std::vector<double> to_host_f64(const void* dptr, size_t count) {
+    std::vector<T> tmp(count);
+    std::vector<double> out(count);
+    if (count) cudaMemcpy(tmp.data(), dptr, count * sizeof(T), cudaMemcpyDeviceToHost);
+    for (size_t i = 0; i < count; ++i) out[i] = (double)tmp[i];
+    return out;
+}
+
+std::vector<double> fetch(DemHandle* h, const void* dptr, size_t count) {
+    return h->dtype == DEM_F32 ? to_host_f64<float>(dptr, count) : to_host_f64<double>(dptr, count);
+}
+
+int alloc_neighbors(DemHandle* h) {
+    dev_free(h, h->nbr);
+    dev_free(h, h->bitems);
+    h->nbr = nullptr;
+    h->bitems = nullptr;
+    int rc;
+    if ((rc = dev_alloc(h, &h->nbr, sizeof(int) * (size_t)h->P.max_neighbors * std::max(h->n, 1)))) return rc;
+    if ((rc = dev_alloc(h, &h->bitems, sizeof(int) * (size_t)h->P.bucket_capacity * h->n_buckets))) return rc;
+    return DEM_OK;
+}
+
+template <typename T>
+int occupancy_grid(DemHandle* h) {
+    int per_sm = 0;
+    CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dem::dem_frames_kernel<T>, dem::kThreads,
+                                                              h->smem));
+    if (per_sm < 1) return set_err(h, DEM_ERR_CUDA, "persistent kernel cannot be resident");
+    h->grid_blocks = per_sm * h->sm_count;
+    return DEM_OK;
+}
+
+template <typename T>
+IcePtrs<T> ice_ptrs(const DemIceState* s) {
+    IcePtrs<T> p;
+    p.pos = (T*)s->positions;
+    p.vel = (T*)s->velocities;
+    p.rot = (T*)s->rotations;
+    p.avel = (T*)s->angular_vels;
+    p.sub = (T*)s->submergence;
+    p.intact = s->bond_intact;
+    p.dmg = (T*)s->bond_damage;
+    p.dm0 = (T*)s->bond_delta_m_0;
+    p.dmmax = (T*)s->bond_delta_m_max;
+    p.ds = (T*)s->bond_delta_s;
+    p.active = s->elem_active;
+    p.elig = s->dpdem_floe_eligible;
+    return p;
+}
+
+template <typename T>
+ShipPtrs<T> ship_ptrs(const DemShipState* s) {
+    ShipPtrs<T> p;
+    p.eta = (T*)s->eta;
+    p.nu = (T*)s->nu;
+    p.na = (T*)s->n_actual;
+    p.ei = (T*)s->e_int;
+    return p;
+}
+
+int check_state(DemHandle* h, const DemIceState* s, const char* what) {
+    if (!s) return set_err(h, DEM_ERR_INVALID, "%s state is NULL", what);
+    if (!s->positions || !s->velocities || !s->rotations || !s->angular_vels || !s->submergence ||
+        !s->elem_active || !s->dpdem_floe_eligible)
+        return set_err(h, DEM_ERR_INVALID, "%s state has a NULL element field", what);
+    if (h->nb > 0 && (!s->bond_intact || !s->bond_damage || !s->bond_delta_m_0 || !s->bond_delta_m_max ||
+                      !s->bond_delta_s))
+        return set_err(h, DEM_ERR_INVALID, "%s state has a NULL bond field", what);
+    return DEM_OK;
+}
+
+int check_ship(DemHandle* h, const DemShipState* s, const char* what) {
+    if (!s || !s->eta || !s->nu || !s->n_actual || !s->e_int)
+        return set_err(h, DEM_ERR_INVALID, "%s ship state has a NULL field", what);
+    return DEM_OK;
+}
+
+template <typename T>
+int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipState* ship_in,
+           DemShipState* ship_out, int K, const void* setpoints, const void* vw, const void* vws,
+           const uint8_t* elig0, DemDiag* diag, DemHistory* hist, cudaStream_t stream) {
+    KArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.P = h->P;
+    a.n = h->n;
+    a.V = h->V;
+    a.nb = h->nb;
+    a.nf = h->nf;
+    a.S = h->nh;
+    a.K = K;
+    a.k_sub = h->P.n_ice_steps;
+    a.nchunks = (h->n + dem::kThreads - 1) / dem::kThreads;
+    a.n_buckets = h->n_buckets;
+    a.bucket_cap = h->P.bucket_capacity;
+    a.max_nb = h->P.max_neighbors;
+    a.mode = h->mode;
+    a.k_n = (T)h->k_n;
+    a.k_s = (T)h->k_s;
+    a.min_bstr = (T)h->min_bstr;
+    double cell = (2.0 * h->r_max + h->P.skin) * 1.0001;
+    a.cell = (T)(cell > 1e-6 ? cell : 1.0);  // zero radii and skin: no pair can touch
+    a.skin = (T)h->P.skin;
+    a.hull_r = (T)h->hull_r;
+    for (int i = 0; i < dem::kMaxEdgeSamples; ++i) a.t_samp[i] = (T)h->t_samp[i];
+    a.polys = (const T*)h->S.local_polys_padded;
+    a.pmask = h->S.poly_mask;
+    a.mass = (const T*)h->S.masses;
+    a.inertia = (const T*)h->S.inertia;
+    a.radii = (const T*)h->S.radii;
+    a.areas = (const T*)h->S.areas;
+    a.thick = (const T*)h->S.thicknesses;
+    a.rest = (const T*)h->S.rest_lengths;
+    a.bstr = (const T*)h->S.bond_strengths;
+    a.sbar = (const T*)h->S.sigma_bar_bond;
+    a.hull = (const T*)h->S.ship_hull_local;
+    a.bi = h->S.bond_i;
+    a.bj = h->S.bond_j;
+    a.floe_of = h->S.initial_floe_of;
+    a.boff = h->boff;
+    a.bslot = h->bslot;
+    a.bstiff = (const T*)h->bstiff;
+    a.vert_r = (const T*)h->vert_r;
+    a.bcnt = h->bcnt;
+    a.bitems = h->bitems;
+    a.ecell = h->ecell;
+    a.ncnt = h->ncnt;
+    a.nbr = h->nbr;
+    a.pos_ref = (T*)h->pos_ref;
+    a.soi = (T*)h->soi;
+    a.fraw = (T*)h->fraw;
+    a.crack = h->crack;
+    a.fcoll = h->fcoll;
+    a.fmax = h->fmax;
+    a.part = h->part;
+    a.gdisp = h->gdisp;
+    for (int i = 0; i < 2; ++i) {
+        a.sp_pos[i] = (T*)h->sp_pos[i];
+        a.sp_vel[i] = (T*)h->sp_vel[i];
+        a.sp_rot[i] = (T*)h->sp_rot[i];
+        a.sp_avel[i] = (T*)h->sp_avel[i];
+    }
+    a.in = ice_ptrs<T>(in);
+    a.out = ice_ptrs<T>(out);
+    DemIceState tmp;
+    tmp.positions = h->t_pos;
+    tmp.velocities = h->t_vel;
+    tmp.rotations = h->t_rot;
+    tmp.angular_vels = h->t_avel;
+    tmp.submergence = h->t_sub;
+    tmp.bond_intact = h->t_intact;
+    tmp.bond_damage = h->t_dmg;
+    tmp.bond_delta_m_0 = h->t_dm0;
+    tmp.bond_delta_m_max = h->t_dmmax;
+    tmp.bond_delta_s = h->t_ds;
+    tmp.elem_active = h->t_active;
+    tmp.dpdem_floe_eligible = h->t_elig;
+    a.tmp = ice_ptrs<T>(&tmp);
+    a.ship_in = ship_ptrs<T>(ship_in);
+    a.ship_out = ship_ptrs<T>(ship_out);
+    T* st = (T*)h->ship_tmp;
+    for (int i = 0; i < 2; ++i) {
+        a.ship_tmp[i].eta = st + 15 * i;
+        a.ship_tmp[i].nu = st + 15 * i + 3;
+        a.ship_tmp[i].na = st + 15 * i + 6;
+        a.ship_tmp[i].ei = st + 15 * i + 12;
+    }
+    a.setpoints = (const T*)setpoints;
+    a.vw = (const T*)vw;
+    a.vws = (const T*)vws;
+    a.elig0 = elig0;
+    if (diag) {
+        a.d_pen = (T*)diag->pen_max;
+        a.d_fmag = (T*)diag->force_mag;
+        a.d_F = (T*)diag->F_ice_on_ship;
+        a.d_J = (T*)diag->J_cumul_incr;
+    }
+    if (hist) {
+        a.h_pos = (T*)hist->positions;
+        a.h_rot = (T*)hist->rotations;
+        a.h_intact = hist->bond_intact;
+        a.h_eta = (T*)hist->eta;
+        a.h_sub = (T*)hist->submergence;
+        a.h_J = (T*)hist->J_cumul_incr;
+        a.h_F = (T*)hist->F_ice_on_ship;
+    }
+    a.bar = h->bar;
+    a.status = h->status;
+    a.stats = h->stats;
+
+    // per-call scratch reset (the kernel keeps it clean between frames)
+    CUDA_TRY(h, cudaMemsetAsync(h->bcnt, 0, sizeof(int) * h->n_buckets, stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->fcoll, 0, sizeof(int) * std::max(h->nf, 1), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->fmax, 0, sizeof(unsigned long long) * std::max(h->nf, 1), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->gdisp, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * 2, stream));
+
+    const int k = h->P.n_ice_steps;
+    const int per_frame = 3 + 3 * k;
+    if (h->mode == DEM_LAUNCH_PERSISTENT) {
+        int lo = 0, hi = K * per_frame;
+        void* args[] = {(void*)&a, (void*)&lo, (void*)&hi};
+        CUDA_TRY(h, cudaLaunchCooperativeKernel((const void*)dem::dem_frames_kernel<T>, dim3(h->grid_blocks),
+                                                dim3(dem::kThreads), args, h->smem, stream));
+    } else {
+        long long work = std::max<long long>(std::max(h->n, h->nb), 1);
+        int blocks = (int)std::min<long long>((work + dem::kThreads - 1) / dem::kThreads, (long long)h->sm_count * 16);
+        blocks = std::max(blocks, 1);
+        for (int f = 0; f < K; ++f) {
+            for (int p = 0; p < per_frame; ++p) {
+                if (p >= 2 && p < per_frame - 1) {
+                    int s = (p - 2) / 3, sub = (p - 2) % 3;
+                    if (s == 0 && sub < 2) continue;
+                }
+                int ph = f * per_frame + p;
+                dem::dem_frames_kernel<T><<<blocks, dem::kThreads, h->smem, stream>>>(a, ph, ph + 1);
+                CUDA_TRY(h, cudaGetLastError());
+            }
+        }
+    }
+    return DEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dem_version(void) { return "dem_b200 0.1 sm_100a"; }
+
+int dem_create(const DemParams* params, const DemStatic* s, int dtype, int device, DemHandle** out) {
+    if (!params || !s || !out) return DEM_ERR_INVALID;
+    *out = nullptr;
+    DemHandle* h = new DemHandle();
+    h->dtype = dtype;
+    h->device = device;
+    h->P = *params;
+    h->S = *s;
+    h->esz = dtype == DEM_F64 ? 8 : 4;
+    h->n = s->n;
+    h->V = s->max_v;
+    h->nb = s->n_bonds;
+    h->nf = s->n_floes;
+    h->nh = s->n_hull;
+    auto fail = [&](int rc) {
+        *out = h;  // keep the handle so dem_get_error can report; caller destroys it
+        return rc;
+    };
+    if (dtype != DEM_F32 && dtype != DEM_F64) return fail(set_err(h, DEM_ERR_INVALID, "dtype must be DEM_F32 or DEM_F64"));
+    if (h->n < 1) return fail(set_err(h, DEM_ERR_INVALID, "n must be >= 1"));
+    if (h->V < 1 || h->V > dem::kMaxV) return fail(set_err(h, DEM_ERR_INVALID, "max_v=%d outside [1,%d]", h->V, dem::kMaxV));
+    if (h->nb < 0 || h->nf < 1) return fail(set_err(h, DEM_ERR_INVALID, "bad n_bonds/n_floes"));
+    if (h->nh < 1 || h->nh > dem::kMaxHull) return fail(set_err(h, DEM_ERR_INVALID, "n_hull=%d outside [1,%d]", h->nh, dem::kMaxHull));
+    if (h->P.n_ice_steps < 1) return fail(set_err(h, DEM_ERR_INVALID, "n_ice_steps must be >= 1"));
+    if (h->P.n_edge_samples < 0 || h->P.n_edge_samples > dem::kMaxEdgeSamples)
+        return fail(set_err(h, DEM_ERR_INVALID, "n_edge_samples outside [0,%d]", dem::kMaxEdgeSamples));
+    if (h->P.max_neighbors < 1 || h->P.max_neighbors > dem::kMaxNbLocal)
+        return fail(set_err(h, DEM_ERR_INVALID, "max_neighbors outside [1,%d]", dem::kMaxNbLocal));
+    if (h->P.bucket_capacity < 1) return fail(set_err(h, DEM_ERR_INVALID, "bucket_capacity must be >= 1"));
+    if (!(h->P.skin >= 0.0)) return fail(set_err(h, DEM_ERR_INVALID, "skin must be >= 0"));
+    if (!s->local_polys_padded || !s->poly_mask || !s->masses || !s->inertia || !s->radii || !s->areas ||
+        !s->thicknesses || !s->initial_floe_of || !s->ship_hull_local)
+        return fail(set_err(h, DEM_ERR_INVALID, "static data has a NULL array"));
+    if (h->nb > 0 && (!s->bond_i || !s->bond_j || !s->rest_lengths || !s->bond_strengths || !s->sigma_bar_bond))
+        return fail(set_err(h, DEM_ERR_INVALID, "static data has a NULL bond array"));
+
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(ce)));
+    cudaDeviceProp prop;
+    ce = cudaGetDeviceProperties(&prop, device);
+    if (ce != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "cudaGetDeviceProperties: %s", cudaGetErrorString(ce)));
+    h->sm_count = prop.multiProcessorCount;
+    if (!prop.cooperativeLaunch) h->mode = DEM_LAUNCH_PHASED;
+
+    // host copies of the static data the set-up needs (one-time)
+    const int n = h->n, nb = h->nb, nf = h->nf;
+    std::vector<double> radii = fetch(h, s->radii, n);
+    std::vector<double> polys = fetch(h, s->local_polys_padded, (size_t)n * h->V * 2);
+    std::vector<double> hull = fetch(h, s->ship_hull_local, (size_t)h->nh * 2);
+    std::vector<int> floe((size_t)n);
+    cudaMemcpy(floe.data(), s->initial_floe_of, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    std::vector<int> bi(nb), bj(nb);
+    std::vector<double> bstr;
+    if (nb) {
+        cudaMemcpy(bi.data(), s->bond_i, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+        cudaMemcpy(bj.data(), s->bond_j, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+        bstr = fetch(h, s->bond_strengths, nb);
+    }
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "copying static data: %s", cudaGetErrorString(ce)));
+    for (int e = 0; e < n; ++e)
+        if (floe[e] < 0 || floe[e] >= nf) return fail(set_err(h, DEM_ERR_INVALID, "initial_floe_of[%d]=%d outside [0,%d)", e, floe[e], nf));
+    for (int b = 0; b < nb; ++b)
+        if (bi[b] < 0 || bi[b] >= n || bj[b] < 0 || bj[b] >= n || bi[b] == bj[b])
+            return fail(set_err(h, DEM_ERR_INVALID, "bond %d=(%d,%d) invalid", b, bi[b], bj[b]));
+    h->r_max = 0.0;
+    for (double r : radii) {
+        if (!(r >= 0.0) || !std::isfinite(r)) return fail(set_err(h, DEM_ERR_INVALID, "radii must be finite and >= 0"));
+        h->r_max = std::max(h->r_max, r);
+    }
+    std::vector<double> vr(n, 0.0);
+    for (int e = 0; e < n; ++e)
+        for (int k = 0; k < h->V; ++k) {
+            double x = polys[((size_t)e * h->V + k) * 2], y = polys[((size_t)e * h->V + k) * 2 + 1];
+            vr[e] = std::max(vr[e], std::sqrt(x * x + y * y));
+        }
+    for (int e = 0; e < n; ++e) vr[e] = vr[e] * (1.0 + 1e-5) + 1e-4;  // conservative (rounded up)
+    h->hull_r = 0.0;
+    for (int i = 0; i < h->nh; ++i) h->hull_r = std::max(h->hull_r, std::hypot(hull[2 * i], hull[2 * i + 1]));
+    h->hull_r = h->hull_r * (1.0 + 1e-5) + 1e-4;
+    h->k_n = s->k_n;
+    h->k_s = s->k_s;
+    h->min_bstr = 0.0;
+    if (nb) {
+        h->min_bstr = bstr[0];
+        for (double v : bstr) h->min_bstr = std::min(h->min_bstr, v);
+    }
+    np_linspace(1.0 / (h->P.n_edge_samples + 1), (double)h->P.n_edge_samples / (h->P.n_edge_samples + 1),
+                h->P.n_edge_samples, h->t_samp);
+
+    // per-element bond slots: bonds with e == bond_i (ascending), then e == bond_j (ascending)
+    std::vector<int> ci(n, 0), cj(n, 0), off(n + 1, 0);
+    for (int b = 0; b < nb; ++b) {
+        ci[bi[b]]++;
+        cj[bj[b]]++;
+    }
+    for (int e = 0; e < n; ++e) off[e + 1] = off[e] + ci[e] + cj[e];
+    std::vector<int> pi(n), pj(n);
+    for (int e = 0; e < n; ++e) {
+        pi[e] = off[e];
+        pj[e] = off[e] + ci[e];
+    }
+    std::vector<int2> slots((size_t)std::max(2 * nb, 1));
+    for (int b = 0; b < nb; ++b) {
+        slots[pi[bi[b]]++] = make_int2(b, bj[b]);
+        slots[pj[bj[b]]++] = make_int2((int)((unsigned)b | 0x80000000u), bi[b]);
+    }
+
+    int rc;
+    const size_t es = h->esz;
+    h->n_buckets = std::max(1024, next_pow2(2LL * n));
+    if ((rc = dev_alloc(h, &h->boff, sizeof(int) * (n + 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bslot, sizeof(int2) * slots.size()))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bstiff, es * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->vert_r, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bcnt, sizeof(int) * h->n_buckets))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->ecell, sizeof(int2) * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->ncnt, sizeof(int) * n))) return fail(rc);
+    if ((rc = alloc_neighbors(h))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->pos_ref, es * 2 * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fraw, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->crack, n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fcoll, sizeof(int) * nf))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fmax, sizeof(unsigned long long) * nf))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->part, sizeof(double) * 3 * ((n + dem::kThreads - 1) / dem::kThreads)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->gdisp, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
+    for (int i = 0; i < 2; ++i) {
+        if ((rc = dev_alloc(h, &h->sp_pos[i], es * 2 * n))) return fail(rc);
+        if ((rc = dev_alloc(h, &h->sp_vel[i], es * 2 * n))) return fail(rc);
+        if ((rc = dev_alloc(h, &h->sp_rot[i], es * n))) return fail(rc);
+        if ((rc = dev_alloc(h, &h->sp_avel[i], es * n))) return fail(rc);
+    }
+    if ((rc = dev_alloc(h, &h->t_pos, es * 2 * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_vel, es * 2 * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_rot, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_avel, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_sub, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_intact, std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_dmg, es * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_dm0, es * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_dmmax, es * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_ds, es * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_active, n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->t_elig, nf))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->ship_tmp, es * 30))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->sprow, es * 6))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bar, sizeof(unsigned) * 2))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->status, sizeof(int)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->stats, sizeof(long long) * 4))) return fail(rc);
+    ce = cudaMallocHost(&h->host_status, sizeof(int));
+    if (ce != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "cudaMallocHost: %s", cudaGetErrorString(ce)));
+
+#define CREATE_TRY(call)                                                                                  \
+    do {                                                                                                  \
+        cudaError_t _e = (call);                                                                          \
+        if (_e != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e))); \
+    } while (0)
+    CREATE_TRY(cudaMemcpy(h->boff, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CREATE_TRY(cudaMemcpy(h->bslot, slots.data(), sizeof(int2) * slots.size(), cudaMemcpyHostToDevice));
+    if (h->dtype == DEM_F32) {
+        std::vector<float> v(n);
+        for (int e = 0; e < n; ++e) v[e] = std::nextafter((float)vr[e], INFINITY);
+        CREATE_TRY(cudaMemcpy(h->vert_r, v.data(), 4 * n, cudaMemcpyHostToDevice));
+    } else {
+        CREATE_TRY(cudaMemcpy(h->vert_r, vr.data(), 8 * n, cudaMemcpyHostToDevice));
+    }
+    CREATE_TRY(cudaMemset(h->bcnt, 0, sizeof(int) * h->n_buckets));
+    CREATE_TRY(cudaMemset(h->status, 0, sizeof(int)));
+    CREATE_TRY(cudaMemset(h->stats, 0, sizeof(long long) * 4));
+    CREATE_TRY(cudaMemset(h->bar, 0, sizeof(unsigned) * 2));
+    if (nb) {
+        int blocks = (nb + 255) / 256;
+        if (h->dtype == DEM_F32)
+            dem::bond_stiffness_kernel<float><<<blocks, 256>>>((const float*)s->thicknesses, s->bond_i, s->bond_j, nb,
+                                                               h->P.youngs_modulus, h->P.bond_stiffness_factor,
+                                                               (float*)h->bstiff);
+        else
+            dem::bond_stiffness_kernel<double><<<blocks, 256>>>((const double*)s->thicknesses, s->bond_i, s->bond_j,
+                                                                nb, h->P.youngs_modulus, h->P.bond_stiffness_factor,
+                                                                (double*)h->bstiff);
+        CREATE_TRY(cudaGetLastError());
+    }
+    h->smem = (size_t)h->nh * 2 * es + 16;
+    if ((rc = (h->dtype == DEM_F32 ? occupancy_grid<float>(h) : occupancy_grid<double>(h)))) return fail(rc);
+    CREATE_TRY(cudaDeviceSynchronize());
+#undef CREATE_TRY
+    *out = h;
+    return DEM_OK;
+}
+
+int dem_frame_step(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipState* ship_in,
+                   DemShipState* ship_out, const void* setpoint, const void* setpoint_next, const void* v_water,
+                   const uint8_t* dpdem_eligible, const void* v_water_ship, DemDiag* diag, void* stream) {
+    if (!h) return DEM_ERR_INVALID;
+    int rc;
+    if ((rc = check_state(h, in, "input"))) return rc;
+    if ((rc = check_state(h, out, "output"))) return rc;
+    if ((rc = check_ship(h, ship_in, "input"))) return rc;
+    if ((rc = check_ship(h, ship_out, "output"))) return rc;
+    if (!setpoint || !setpoint_next || !v_water || !dpdem_eligible)
+        return set_err(h, DEM_ERR_INVALID, "setpoint / setpoint_next / v_water / dpdem_eligible is NULL");
+    if (out->positions == in->positions || out->velocities == in->velocities || out->rotations == in->rotations ||
+        out->angular_vels == in->angular_vels)
+        return set_err(h, DEM_ERR_ALIAS, "output element kinematics alias the input");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    // pack [setpoint, setpoint_next] into the (1,6) row the kernel reads
+    const size_t es = h->esz;
+    void* sprow = h->sprow;
+    CUDA_TRY(h, cudaMemcpyAsync(sprow, setpoint, es * 3, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync((char*)sprow + es * 3, setpoint_next, es * 3, cudaMemcpyDeviceToDevice, st));
+    if (h->dtype == DEM_F32)
+        rc = launch<float>(h, in, out, ship_in, ship_out, 1, sprow, v_water, v_water_ship, dpdem_eligible, diag,
+                           nullptr, st);
+    else
+        rc = launch<double>(h, in, out, ship_in, ship_out, 1, sprow, v_water, v_water_ship, dpdem_eligible, diag,
+                            nullptr, st);
+    return rc;
+}
+
+int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipState* ship_in,
+                     DemShipState* ship_out, int32_t K, const void* setpoints_K6, const void* v_water_Kn2,
+                     const void* v_water_ship_K2, DemHistory* hist, void* stream) {
+    if (!h) return DEM_ERR_INVALID;
+    int rc;
+    if (K < 1) return set_err(h, DEM_ERR_INVALID, "K must be >= 1");
+    if ((rc = check_state(h, in, "input"))) return rc;
+    if ((rc = check_state(h, out, "output"))) return rc;
+    if ((rc = check_ship(h, ship_in, "input"))) return rc;
+    if ((rc = check_ship(h, ship_out, "output"))) return rc;
+    if (!setpoints_K6 || !v_water_Kn2) return set_err(h, DEM_ERR_INVALID, "setpoints / v_water is NULL");
+    if (out->positions == in->positions || out->velocities == in->velocities || out->rotations == in->rotations ||
+        out->angular_vels == in->angular_vels)
+        return set_err(h, DEM_ERR_ALIAS, "output element kinematics alias the input");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (h->dtype == DEM_F32)
+        return launch<float>(h, in, out, ship_in, ship_out, K, setpoints_K6, v_water_Kn2, v_water_ship_K2,
+                             in->dpdem_floe_eligible, nullptr, hist, st);
+    return launch<double>(h, in, out, ship_in, ship_out, K, setpoints_K6, v_water_Kn2, v_water_ship_K2,
+                          in->dpdem_floe_eligible, nullptr, hist, st);
+}
+
+int dem_sync_status(DemHandle* h, void* stream) {
+    if (!h) return DEM_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(h, cudaMemcpyAsync(h->host_status, h->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    int v = *h->host_status;
+    if (v != 0) {
+        CUDA_TRY(h, cudaMemsetAsync(h->status, 0, sizeof(int), st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        if (v == DEM_ERR_CAPACITY)
+            return set_err(h, DEM_ERR_CAPACITY, "neighbour or grid-bucket capacity exceeded (max_neighbors=%d, bucket_capacity=%d)",
+                           h->P.max_neighbors, h->P.bucket_capacity);
+        if (v == DEM_ERR_TIMEOUT) return set_err(h, DEM_ERR_TIMEOUT, "grid barrier wait exceeded its limit");
+        return set_err(h, v, "device status %d", v);
+    }
+    return DEM_OK;
+}
+
+int dem_set_capacity(DemHandle* h, int32_t max_neighbors, int32_t bucket_capacity) {
+    if (!h) return DEM_ERR_INVALID;
+    if (max_neighbors < 1 || max_neighbors > dem::kMaxNbLocal)
+        return set_err(h, DEM_ERR_INVALID, "max_neighbors outside [1,%d]", dem::kMaxNbLocal);
+    if (bucket_capacity < 1) return set_err(h, DEM_ERR_INVALID, "bucket_capacity must be >= 1");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    h->P.max_neighbors = max_neighbors;
+    h->P.bucket_capacity = bucket_capacity;
+    return alloc_neighbors(h);
+}
+
+int dem_set_launch_mode(DemHandle* h, int32_t mode) {
+    if (!h) return DEM_ERR_INVALID;
+    if (mode != DEM_LAUNCH_PERSISTENT && mode != DEM_LAUNCH_PHASED) return set_err(h, DEM_ERR_INVALID, "bad launch mode");
+    h->mode = mode;
+    return DEM_OK;
+}
+
+int dem_get_info(DemHandle* h, DemInfo* info) {
+    if (!h || !info) return DEM_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    long long st[4] = {0, 0, 0, 0};
+    CUDA_TRY(h, cudaMemcpy(st, h->stats, sizeof(st), cudaMemcpyDeviceToHost));
+    info->grid_blocks = h->grid_blocks;
+    info->threads_per_block = dem::kThreads;
+    info->neighbor_rebuilds = st[0];
+    info->max_neighbor_count = (int)st[1];
+    info->max_bucket_count = (int)st[2];
+    info->hash_buckets = h->n_buckets;
+    info->cell_size = 2.0 * h->r_max + h->P.skin;
+    return DEM_OK;
+}
+
+int dem_get_error(DemHandle* h, char* buf, size_t len) {
+    if (!h || !buf || len == 0) return DEM_ERR_INVALID;
+    std::snprintf(buf, len, "%s", h->err.c_str());
+    return DEM_OK;
+}
+
+int dem_destroy(DemHandle* h) {
+    if (!h) return DEM_OK;
+    cudaSetDevice(h->device);
+    cudaDeviceSynchronize();
+    for (void* p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    if (h->host_status) cudaFreeHost(h->host_status);
+    delete h;
+    return DEM_OK;
+}
+
+}  // extern "C"

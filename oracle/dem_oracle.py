@@ -602,43 +602,33 @@ class Oracle:
 # ── free functions ──────────────────────────────────────────────────────────
 
 def grid_pairs(pos: np.ndarray, radii: np.ndarray, margin: float = 0.0):
-    """All (i < j) with |p_i - p_j| < r_i + r_j + margin, lexicographic order (uniform grid)."""
+    """All (i < j) with |p_i - p_j| < r_i + r_j + margin, lexicographic order.
+
+    Candidates come from a KD-tree ball query of radius 2 max(r) + margin
+    (a superset), then the per-pair test keeps a further rounding margin so
+    that every pair the reference's predicate can count is kept.
+    """
+    from scipy.spatial import cKDTree
+
     n = pos.shape[0]
+    empty = (np.zeros(0, np.int64), np.zeros(0, np.int64))
     if n < 2:
-        return np.zeros(0, np.int64), np.zeros(0, np.int64)
-    cell = 2.0 * float(radii.max()) + margin + 1e-6
-    c = np.floor(pos / cell).astype(np.int64)
-    c -= c.min(axis=0)
-    ncx = int(c[:, 0].max()) + 1
-    key = c[:, 1] * ncx + c[:, 0]
-    order = np.argsort(key, kind="stable")
-    ks = key[order]
-    uniq, start = np.unique(ks, return_index=True)
-    end = np.append(start[1:], len(ks))
-    lut = dict(zip(uniq.tolist(), zip(start.tolist(), end.tolist())))
-    out_i, out_j = [], []
-    for dx in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            nk = (c[:, 1] + dy) * ncx + (c[:, 0] + dx)
-            valid = (c[:, 0] + dx >= 0) & (c[:, 0] + dx < ncx) & (c[:, 1] + dy >= 0)
-            for e in np.nonzero(valid)[0]:
-                rng = lut.get(int(nk[e]))
-                if rng is None:
-                    continue
-                others = order[rng[0]:rng[1]]
-                others = others[others > e]
-                if len(others):
-                    out_i.append(np.full(len(others), e))
-                    out_j.append(others)
-    if not out_i:
-        return np.zeros(0, np.int64), np.zeros(0, np.int64)
-    pi = np.concatenate(out_i)
-    pj = np.concatenate(out_j)
+        return empty
+    ok = np.isfinite(pos).all(axis=1)
+    idx = np.nonzero(ok)[0]
+    if len(idx) < 2:
+        return empty
+    tree = cKDTree(pos[idx])
+    pr = tree.query_pairs(r=2.0 * float(radii.max()) + margin + 1e-6, output_type="ndarray")
+    if len(pr) == 0:
+        return empty
+    a, b = idx[pr[:, 0]], idx[pr[:, 1]]
+    pi, pj = np.minimum(a, b), np.maximum(a, b)
     d = np.sqrt(((pos[pj] - pos[pi]) ** 2).sum(1))
     keep = d < radii[pi] + radii[pj] + margin + 1e-6 * (1.0 + np.abs(pos[pi]).max(1))
     pi, pj = pi[keep], pj[keep]
     o = np.lexsort((pj, pi))
-    return pi[o], pj[o]
+    return pi[o].astype(np.int64), pj[o].astype(np.int64)
 
 
 def hull_point_test(px, py, ship_x, ship_y, heading, half_len, half_beam, dt,

@@ -119,3 +119,41 @@ def rel_err(a, b, floor=None):
     if scale == 0.0:
         return float(np.max(np.abs(a - b))) if a.size else 0.0
     return float(np.max(np.abs(a - b)) / scale)
+
+
+# ── GPU-side construction from the same golden data ─────────────────────────
+
+def gpu_frame_step(g, prefix, torch_dtype, **kw):
+    """FrameStep (libdem_b200) bound to a golden scenario's static data."""
+    import torch
+    from mbd_icenav_b200 import sim
+    from mbd_icenav_b200.config import IceMaterial
+    L, B, k, dt, dti, auto, flex = SCENARIOS[prefix]
+    dev = torch.device("cuda", 0)
+    st = static_from_golden(g, prefix)
+    sd = shipdyn_from_golden(g, prefix)
+    mat = IceMaterial(flexural_strength_base=flex)
+    return sim.make_frame_step(st, default_cfg(), sd, L, B, k, dt, dti, auto, B_THRUST, 1.0,
+                               material=mat, device=dev, dtype=torch_dtype, **kw)
+
+
+def to_gpu_state(st, ship, torch_dtype):
+    import torch
+    from mbd_icenav_b200.state import IceState, ShipState
+    dev = torch.device("cuda", 0)
+    f = lambda a: torch.as_tensor(np.asarray(a, np.float64)).to(dev, torch_dtype)
+    b = lambda a: torch.as_tensor(np.asarray(a, bool)).to(dev)
+    ice = IceState(positions=f(st.positions), velocities=f(st.velocities), rotations=f(st.rotations),
+                   angular_vels=f(st.angular_vels), submergence=f(st.submergence),
+                   bond_intact=b(st.bond_intact), bond_damage=f(st.bond_damage),
+                   bond_delta_m_0=f(st.bond_delta_m_0), bond_delta_m_max=f(st.bond_delta_m_max),
+                   bond_delta_s=f(st.bond_delta_s), elem_active=b(st.elem_active),
+                   dpdem_floe_eligible=b(st.dpdem_floe_eligible))
+    sh = ShipState(eta=f(ship.eta), nu=f(ship.nu), n_actual=f(ship.n_actual), e_int=f(ship.e_int))
+    return ice, sh
+
+
+def to_np_state(st, ship):
+    ice = OState(*[t.detach().cpu().numpy() for t in st])
+    sh = OShip(*[t.detach().cpu().numpy() for t in ship])
+    return ice, sh

@@ -1,0 +1,57 @@
+"""The C-ABI library loads and exports every entry point its header declares (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "dem_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(dem_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_the_boundary():
+    names = _declared()
+    for need in ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_destroy", "dem_get_error",
+                 "dem_sync_status"):
+        assert need in names
+
+
+def test_library_exports_every_declared_symbol():
+    from mbd_icenav_b200 import _abi, build
+    build.build_library()
+    lib = ctypes.CDLL(build.LIB_PATH)
+    for name in _declared():
+        assert hasattr(lib, name), name
+    assert set(_abi.EXPORTS) <= set(_declared())
+    assert lib.dem_version is not None
+
+
+def test_struct_layout_matches_header():
+    """ctypes mirrors must have the header's field order (checked by name against the source)."""
+    from mbd_icenav_b200 import _abi
+    src = open(os.path.join(ROOT, "include", "dem_b200.h")).read()
+    body = src[src.index("typedef struct DemParams"):src.index("} DemParams;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = []
+    for line in body.splitlines()[1:]:
+        line = line.strip().rstrip(";")
+        if not line:
+            continue
+        decl = line.split(None, 1)[1]
+        for part in decl.split(","):
+            fields.append(part.strip().split("[")[0])
+    assert fields == [f for f, _ in _abi.DemParams._fields_]
+
+
+def test_null_arguments_are_rejected_without_a_gpu():
+    from mbd_icenav_b200 import _abi
+    lib = _abi.load_library()
+    assert lib.dem_create(None, None, 0, 0, None) == _abi.DEM_ERR_INVALID
+    assert lib.dem_frame_step(None, None, None, None, None, None, None, None, None, None, None, None) \
+        == _abi.DEM_ERR_INVALID
+    assert lib.dem_destroy(None) == _abi.DEM_OK
