@@ -202,6 +202,9 @@ def run_ours(args, rank: int, world: int):
     torch.cuda.set_device(device)
     field = load_field(args.config, args.seed)
     fs, st, sh, static = build_stepper(field, args.dtype, device)
+    if args.launch == "phased":
+        from mbd_icenav_b200 import _abi
+        fs.set_launch_mode(_abi.DEM_LAUNCH_PHASED)
     dt = fs.dtype
     n, nb, V = fs.n, fs.n_bonds, fs.max_v
     K, W = args.steps, args.warmup
@@ -279,6 +282,8 @@ def run_ours(args, rank: int, world: int):
     if rc != 0:
         raise RuntimeError(f"device status {rc}: {fs._error()}")
     info = fs.info()
+    if args.phase_times and args.launch == "persistent":
+        print_phase_times(fs, st, sh, sp_all[fr:fr + 1], vw)
 
     if rank != 0:
         return None
@@ -297,7 +302,8 @@ def run_ours(args, rank: int, world: int):
                    "elements": n, "bonds": nb, "substeps_per_step": N_SUB, "seed": args.seed,
                    "l2": "flushed before every timed step (256 MB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "launch": "one cooperative persistent kernel per frame",
+                   "launch": ("one cooperative persistent kernel per frame" if args.launch == "persistent"
+                              else "one kernel launch per phase"),
                    "neighbor_rebuilds": info["neighbor_rebuilds"],
                    "max_neighbor_count": info["max_neighbor_count"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -306,12 +312,40 @@ def run_ours(args, rank: int, world: int):
                      "traffic": traffic},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": E},
-        "gpu_launches": K,
+        "gpu_launches": K if args.launch == "persistent" else None,
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(field, args.cpu_seconds)
     return line
+
+
+def print_phase_times(fs, st, sh, sp, vw, frames: int = 5):
+    """Per-phase device time of a few frames (profiling switch of the library)."""
+    import collections
+    import torch
+    k = fs.n_ice_steps
+    per = 5 + 4 * k
+    names = ["cull", "near", "cforce", "reduce"] + [f"{x}" for s in range(k)
+                                                     for x in ("reref", "mark", "build", "force")] + ["fracture"]
+    acc = collections.defaultdict(list)
+    fs.set_profiling(True)
+    for _ in range(frames):
+        st, sh, _ = fs.scan_segment(st, sh, sp, vw, history=False)
+        torch.cuda.synchronize()
+        pts = fs.phase_times()
+        prev = 0
+        for ph, t in pts:
+            acc[names[ph % per]].append((t - prev) / 1e3)
+            prev = t
+    fs.set_profiling(False)
+    tot = 0.0
+    for nm in ("cull", "near", "cforce", "reduce", "reref", "mark", "build", "force", "fracture"):
+        v = acc.get(nm, [])
+        s = sum(v) / frames
+        tot += s
+        sys.stderr.write(f"phase {nm:9s} {s:9.1f} us/frame  ({len(v) / frames:.1f} runs/frame)\n")
+    sys.stderr.write(f"phase total     {tot:9.1f} us/frame\n")
 
 
 # ── CPU side (the oracle is the checker/baseline only) ─────────────────────────
@@ -428,6 +462,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch", choices=["persistent", "phased"], default="persistent")
+    ap.add_argument("--phase-times", action="store_true",
+                    help="after the run, time one profiled frame per phase (device clock) to stderr")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -206,6 +206,16 @@ int dem_set_launch_mode(DemHandle* h, int32_t mode);
 
 int dem_get_info(DemHandle* h, DemInfo* info);
 
+/* Record, in persistent launches, the device time at which each phase ends
+ * (profiling aid; off by default). */
+int dem_set_profiling(DemHandle* h, int32_t on);
+
+/* Phase end times of the last persistent call: pairs [phase index, ns] (at most
+ * max_pairs), their count, and the launch's start time in ns (globaltimer).
+ * Phase indices count 5 + 4 k per frame: cull, near contact, contact forces,
+ * reduce, then per substep re-reference, mark, list build, force, and fracture. */
+int dem_get_phase_times(DemHandle* h, int64_t* pairs, int32_t max_pairs, int32_t* count, int64_t* start_ns);
+
 /* Copy the last error message (NUL-terminated) into buf. */
 int dem_get_error(DemHandle* h, char* buf, size_t len);
 

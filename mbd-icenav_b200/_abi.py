@@ -99,8 +99,8 @@ class DemInfo(C.Structure):
 
 
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
-           "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_get_error",
-           "dem_destroy", "dem_version")
+           "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_set_profiling",
+           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version")
 
 _LIB = None
 
@@ -126,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     lib.dem_set_capacity.argtypes = [H, _i, _i]
     lib.dem_set_launch_mode.argtypes = [H, _i]
     lib.dem_get_info.argtypes = [H, C.POINTER(DemInfo)]
+    lib.dem_set_profiling.argtypes = [H, _i]
+    lib.dem_get_phase_times.argtypes = [H, C.POINTER(C.c_int64), _i, C.POINTER(_i), C.POINTER(C.c_int64)]
     lib.dem_get_error.argtypes = [H, C.c_char_p, C.c_size_t]
     lib.dem_destroy.argtypes = [H]
     lib.dem_version.restype = C.c_char_p

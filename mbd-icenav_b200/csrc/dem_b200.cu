@@ -37,24 +37,31 @@ struct DemHandle {
     // derived
     int* boff = nullptr;
     int2* bslot = nullptr;
-    void* bstiff = nullptr;
+    void* slot_rest = nullptr;
+    void* slot_stiff = nullptr;
     void* vert_r = nullptr;
-    // scratch
+    // broad phase (persists across calls)
     int* bcnt = nullptr;
     int* bitems = nullptr;
     int2* ecell = nullptr;
     int* ncnt = nullptr;
     int* nbr = nullptr;
     void* pos_ref = nullptr;
+    uint8_t* esc = nullptr;
+    uint8_t* dirty = nullptr;
+    unsigned* esc_cnt = nullptr;
+    int* near_list = nullptr;
+    int* near_cnt = nullptr;
+    void* cpen = nullptr;
+    void* cnx = nullptr;
+    void* cny = nullptr;
     void* soi = nullptr;
     void* fraw = nullptr;
     uint8_t* crack = nullptr;
     int* fcoll = nullptr;
     unsigned long long* fmax = nullptr;
     double* part = nullptr;
-    unsigned* gdisp = nullptr;
-    void* sp_pos[2] = {nullptr, nullptr};
-    void* sp_vel[2] = {nullptr, nullptr};
+    void* kin[2] = {nullptr, nullptr};
     void* sp_rot[2] = {nullptr, nullptr};
     void* sp_avel[2] = {nullptr, nullptr};
     // frame ping-pong state for scans
@@ -70,6 +77,11 @@ struct DemHandle {
     void* t_ds = nullptr;
     uint8_t* t_active = nullptr;
     uint8_t* t_elig = nullptr;
+    void* slotrec = nullptr;
+    void* r3 = nullptr;
+    double* fscal = nullptr;
+    unsigned long long* ptimes = nullptr;
+    bool profiling = false;
     void* ship_tmp = nullptr;  // 2 x 15
     void* sprow = nullptr;     // (6,) setpoint row of dem_frame_step
     unsigned* bar = nullptr;
@@ -161,6 +173,17 @@ int alloc_neighbors(DemHandle* h) {
     int rc;
     if ((rc = dev_alloc(h, &h->nbr, sizeof(int) * (size_t)h->P.max_neighbors * std::max(h->n, 1)))) return rc;
     if ((rc = dev_alloc(h, &h->bitems, sizeof(int) * (size_t)h->P.bucket_capacity * h->n_buckets))) return rc;
+    return DEM_OK;
+}
+
+// Forget the persistent broad-phase state: reference positions become NaN so the
+// next call rebuilds every list (after a capacity change or a device error).
+int reset_broad_phase(DemHandle* h, cudaStream_t st) {
+    CUDA_TRY(h, cudaMemsetAsync(h->bcnt, 0, sizeof(int) * (size_t)h->n_buckets, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->pos_ref, 0xFF, h->esz * 2 * (size_t)h->n, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->esc, 0, (size_t)h->n, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->dirty, 0, (size_t)h->n, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->ncnt, 0, sizeof(int) * (size_t)h->n, st));
     return DEM_OK;
 }
 
@@ -262,27 +285,38 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.floe_of = h->S.initial_floe_of;
     a.boff = h->boff;
     a.bslot = h->bslot;
-    a.bstiff = (const T*)h->bstiff;
+    a.slot_rest = (const T*)h->slot_rest;
+    a.slot_stiff = (const T*)h->slot_stiff;
     a.vert_r = (const T*)h->vert_r;
     a.bcnt = h->bcnt;
     a.bitems = h->bitems;
+    a.near_list = h->near_list;
+    a.near_cnt = h->near_cnt;
+    a.cpen = (T*)h->cpen;
+    a.cnx = (T*)h->cnx;
+    a.cny = (T*)h->cny;
     a.ecell = h->ecell;
     a.ncnt = h->ncnt;
     a.nbr = h->nbr;
     a.pos_ref = (T*)h->pos_ref;
+    a.esc = h->esc;
+    a.dirty = h->dirty;
+    a.esc_cnt = h->esc_cnt;
     a.soi = (T*)h->soi;
     a.fraw = (T*)h->fraw;
     a.crack = h->crack;
     a.fcoll = h->fcoll;
     a.fmax = h->fmax;
     a.part = h->part;
-    a.gdisp = h->gdisp;
     for (int i = 0; i < 2; ++i) {
-        a.sp_pos[i] = (T*)h->sp_pos[i];
-        a.sp_vel[i] = (T*)h->sp_vel[i];
+        a.kin[i] = (T*)h->kin[i];
         a.sp_rot[i] = (T*)h->sp_rot[i];
         a.sp_avel[i] = (T*)h->sp_avel[i];
     }
+    a.slotrec = h->slotrec;
+    a.r3 = (const T*)h->r3;
+    a.fscal = h->fscal;
+    a.ptimes = h->profiling ? h->ptimes : nullptr;
     a.in = ice_ptrs<T>(in);
     a.out = ice_ptrs<T>(out);
     DemIceState tmp;
@@ -332,14 +366,15 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.stats = h->stats;
 
     // per-call scratch reset (the kernel keeps it clean between frames)
-    CUDA_TRY(h, cudaMemsetAsync(h->bcnt, 0, sizeof(int) * h->n_buckets, stream));
     CUDA_TRY(h, cudaMemsetAsync(h->fcoll, 0, sizeof(int) * std::max(h->nf, 1), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->fmax, 0, sizeof(unsigned long long) * std::max(h->nf, 1), stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->gdisp, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->esc_cnt, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * 2, stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->near_cnt, 0, sizeof(int), stream));
+    if (h->profiling) CUDA_TRY(h, cudaMemsetAsync(h->ptimes, 0, sizeof(unsigned long long) * 2, stream));
 
     const int k = h->P.n_ice_steps;
-    const int per_frame = 3 + 3 * k;
+    const int per_frame = 5 + 4 * k;
     if (h->mode == DEM_LAUNCH_PERSISTENT) {
         int lo = 0, hi = K * per_frame;
         void* args[] = {(void*)&a, (void*)&lo, (void*)&hi};
@@ -351,10 +386,6 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
         blocks = std::max(blocks, 1);
         for (int f = 0; f < K; ++f) {
             for (int p = 0; p < per_frame; ++p) {
-                if (p >= 2 && p < per_frame - 1) {
-                    int s = (p - 2) / 3, sub = (p - 2) % 3;
-                    if (s == 0 && sub < 2) continue;
-                }
                 int ph = f * per_frame + p;
                 dem::dem_frames_kernel<T><<<blocks, dem::kThreads, h->smem, stream>>>(a, ph, ph + 1);
                 CUDA_TRY(h, cudaGetLastError());
@@ -483,23 +514,30 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     h->n_buckets = std::max(1024, next_pow2(2LL * n));
     if ((rc = dev_alloc(h, &h->boff, sizeof(int) * (n + 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bslot, sizeof(int2) * slots.size()))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->bstiff, es * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->slot_rest, es * slots.size()))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->slot_stiff, es * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->vert_r, es * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->bcnt, sizeof(int) * h->n_buckets))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bcnt, sizeof(int) * (size_t)h->n_buckets))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->near_list, sizeof(int) * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->near_cnt, sizeof(int)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->cpen, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->cnx, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->cny, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ecell, sizeof(int2) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ncnt, sizeof(int) * n))) return fail(rc);
     if ((rc = alloc_neighbors(h))) return fail(rc);
     if ((rc = dev_alloc(h, &h->pos_ref, es * 2 * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->esc, n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->dirty, n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->esc_cnt, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fraw, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->crack, n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fcoll, sizeof(int) * nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fmax, sizeof(unsigned long long) * nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->part, sizeof(double) * 3 * ((n + dem::kThreads - 1) / dem::kThreads)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->gdisp, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
     for (int i = 0; i < 2; ++i) {
-        if ((rc = dev_alloc(h, &h->sp_pos[i], es * 2 * n))) return fail(rc);
-        if ((rc = dev_alloc(h, &h->sp_vel[i], es * 2 * n))) return fail(rc);
+        if ((rc = dev_alloc(h, &h->kin[i], es * 4 * n))) return fail(rc);
         if ((rc = dev_alloc(h, &h->sp_rot[i], es * n))) return fail(rc);
         if ((rc = dev_alloc(h, &h->sp_avel[i], es * n))) return fail(rc);
     }
@@ -516,6 +554,10 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->t_active, n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->t_elig, nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ship_tmp, es * 30))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->slotrec, (es == 4 ? 16 : 32) * slots.size()))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->r3, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fscal, sizeof(double) * 4))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->ptimes, sizeof(unsigned long long) * (2 + 2 * dem::kMaxPhaseTimes)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->sprow, es * 6))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bar, sizeof(unsigned) * 2))) return fail(rc);
     if ((rc = dev_alloc(h, &h->status, sizeof(int)))) return fail(rc);
@@ -537,20 +579,32 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     } else {
         CREATE_TRY(cudaMemcpy(h->vert_r, vr.data(), 8 * n, cudaMemcpyHostToDevice));
     }
-    CREATE_TRY(cudaMemset(h->bcnt, 0, sizeof(int) * h->n_buckets));
+    if ((rc = reset_broad_phase(h, 0))) return fail(rc);
     CREATE_TRY(cudaMemset(h->status, 0, sizeof(int)));
     CREATE_TRY(cudaMemset(h->stats, 0, sizeof(long long) * 4));
     CREATE_TRY(cudaMemset(h->bar, 0, sizeof(unsigned) * 2));
     if (nb) {
-        int blocks = (nb + 255) / 256;
+        int n_slots = 2 * nb;
+        int blocks = (n_slots + 255) / 256;
         if (h->dtype == DEM_F32)
-            dem::bond_stiffness_kernel<float><<<blocks, 256>>>((const float*)s->thicknesses, s->bond_i, s->bond_j, nb,
-                                                               h->P.youngs_modulus, h->P.bond_stiffness_factor,
-                                                               (float*)h->bstiff);
+            dem::slot_setup_kernel<float><<<blocks, 256>>>((const float*)s->thicknesses, (const float*)s->rest_lengths,
+                                                           s->bond_i, s->bond_j, h->bslot, n_slots, h->P.youngs_modulus,
+                                                           h->P.bond_stiffness_factor, (float*)h->slot_rest,
+                                                           (float*)h->slot_stiff);
         else
-            dem::bond_stiffness_kernel<double><<<blocks, 256>>>((const double*)s->thicknesses, s->bond_i, s->bond_j,
-                                                                nb, h->P.youngs_modulus, h->P.bond_stiffness_factor,
-                                                                (double*)h->bstiff);
+            dem::slot_setup_kernel<double><<<blocks, 256>>>((const double*)s->thicknesses,
+                                                            (const double*)s->rest_lengths, s->bond_i, s->bond_j,
+                                                            h->bslot, n_slots, h->P.youngs_modulus,
+                                                            h->P.bond_stiffness_factor, (double*)h->slot_rest,
+                                                            (double*)h->slot_stiff);
+        CREATE_TRY(cudaGetLastError());
+    }
+    {
+        int blocks = (n + 255) / 256;
+        if (h->dtype == DEM_F32)
+            dem::cube_kernel<float><<<blocks, 256>>>((const float*)s->radii, n, (float*)h->r3);
+        else
+            dem::cube_kernel<double><<<blocks, 256>>>((const double*)s->radii, n, (double*)h->r3);
         CREATE_TRY(cudaGetLastError());
     }
     h->smem = (size_t)h->nh * 2 * es + 16;
@@ -623,6 +677,8 @@ int dem_sync_status(DemHandle* h, void* stream) {
     int v = *h->host_status;
     if (v != 0) {
         CUDA_TRY(h, cudaMemsetAsync(h->status, 0, sizeof(int), st));
+        int rc = reset_broad_phase(h, st);
+        if (rc) return rc;
         CUDA_TRY(h, cudaStreamSynchronize(st));
         if (v == DEM_ERR_CAPACITY)
             return set_err(h, DEM_ERR_CAPACITY, "neighbour or grid-bucket capacity exceeded (max_neighbors=%d, bucket_capacity=%d)",
@@ -642,7 +698,12 @@ int dem_set_capacity(DemHandle* h, int32_t max_neighbors, int32_t bucket_capacit
     CUDA_TRY(h, cudaDeviceSynchronize());
     h->P.max_neighbors = max_neighbors;
     h->P.bucket_capacity = bucket_capacity;
-    return alloc_neighbors(h);
+    int rc = alloc_neighbors(h);
+    if (rc) return rc;
+    rc = reset_broad_phase(h, 0);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    return DEM_OK;
 }
 
 int dem_set_launch_mode(DemHandle* h, int32_t mode) {
@@ -664,6 +725,29 @@ int dem_get_info(DemHandle* h, DemInfo* info) {
     info->max_bucket_count = (int)st[2];
     info->hash_buckets = h->n_buckets;
     info->cell_size = 2.0 * h->r_max + h->P.skin;
+    return DEM_OK;
+}
+
+int dem_set_profiling(DemHandle* h, int32_t on) {
+    if (!h) return DEM_ERR_INVALID;
+    h->profiling = on != 0;
+    return DEM_OK;
+}
+
+int dem_get_phase_times(DemHandle* h, int64_t* pairs, int32_t max_pairs, int32_t* count, int64_t* start_ns) {
+    if (!h || !count) return DEM_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    std::vector<unsigned long long> buf(2 + 2 * (size_t)dem::kMaxPhaseTimes);
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    CUDA_TRY(h, cudaMemcpy(buf.data(), h->ptimes, sizeof(unsigned long long) * buf.size(), cudaMemcpyDeviceToHost));
+    int c = (int)std::min<unsigned long long>(buf[0], (unsigned long long)dem::kMaxPhaseTimes);
+    c = std::min(c, std::max(max_pairs, 0));
+    for (int i = 0; i < c && pairs; ++i) {
+        pairs[2 * i] = (int64_t)buf[2 + 2 * i];
+        pairs[2 * i + 1] = (int64_t)buf[3 + 2 * i];
+    }
+    *count = c;
+    if (start_ns) *start_ns = (int64_t)buf[1];
     return DEM_OK;
 }
 

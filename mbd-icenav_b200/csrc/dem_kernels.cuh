@@ -38,6 +38,21 @@ constexpr int kMaxV = 32;              // upper bound of max_v (padded vertices 
 constexpr int kMaxHull = 256;          // upper bound of hull outline points
 constexpr int kMaxEdgeSamples = 16;
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s per barrier wait
+constexpr int kMaxPhaseTimes = 4096;
+
+// Per-frame record of one bond slot (see phase_reduce): partner index with the
+// slot's role in the sign bit, rest length, stiffness E*mean(h)*factor, and
+// (1 - damage), or -1 when the bond adds no force this frame (broken, or its
+// endpoints differ in active state; jax_simulation.py:86-96).
+template <typename T> struct SlotRec;
+template <> struct __align__(16) SlotRec<float> {
+    int o;
+    float rest, stiff, omd;
+};
+template <> struct __align__(16) SlotRec<double> {
+    int o, pad;
+    double rest, stiff, omd;
+};
 
 template <typename T>
 struct IcePtrs {
@@ -67,23 +82,35 @@ struct KArgs {
     // derived at create
     const int* boff;    // (n+1) CSR offsets of per-element bond slots
     const int2* bslot;  // (2 nb) {bond | role<<31, partner}; role 0: element is bond_i
-    const T* bstiff;    // (nb) E * mean(h) * factor
+    const T* slot_rest; // (2 nb) rest length of each slot's bond
+    const T* slot_stiff;// (2 nb) E * mean(h) * factor of each slot's bond
     const T* vert_r;    // (n) max local vertex radius, rounded up
-    // scratch
+    // broad phase: grids, reference positions and lists persist across calls
     int* bcnt;          // (n_buckets) grid-hash bucket fill
-    int* bitems;        // (n_buckets * bucket_cap)
-    int2* ecell;        // (n) grid cell of each element at the last build
+    int* bitems;        // (n_buckets * bucket_cap) entries; stale ones are filtered by home cell
+    int2* ecell;        // (n) home cell of each reference position
     int* ncnt;          // (n) neighbour count
     int* nbr;           // (max_nb * n) neighbour lists, slot-major
-    T* pos_ref;         // (n,2) positions at the last build
+    T* pos_ref;         // (n,2) reference positions (NaN before the first build)
+    uint8_t* esc;       // (n) moved more than 0.45 skin from its reference
+    uint8_t* dirty;     // (n) neighbour list must be rebuilt
+    unsigned* esc_cnt;  // (k_sub + 2) escaped elements found before substep s
+    // per-frame scratch
+    int* near_list;     // (n) elements whose bounding circle reaches the hull
+    int* near_cnt;      // (1)
+    T *cpen, *cnx, *cny;  // (n) max penetration contact per element
     T* soi;             // (n,2) ship force on ice (with buoyancy), constant over substeps
     T* fraw;            // (n) contact force magnitude before the thrust cap
     uint8_t* crack;     // (n) element touches a broken bond
     int* fcoll;         // (nf) floe touched by the ship this frame
     unsigned long long* fmax;  // (nf) max force magnitude per floe (ordered bits)
     double* part;       // (nchunks * 3) per-chunk sums: soi_x, soi_y, moment
-    unsigned* gdisp;    // (k_sub + 2) max squared displacement since the last build, per substep
-    T *sp_pos[2], *sp_vel[2], *sp_rot[2], *sp_avel[2];  // substep ping-pong
+    T* kin[2];          // (n,4) {x, y, vx, vy} of the substep being read / written
+    T *sp_rot[2], *sp_avel[2];  // substep ping-pong of own-element angles
+    void* slotrec;      // (2 nb) SlotRec<T>: per-frame bond slot records
+    const T* r3;        // (n) radius^3 (dtype pow, once at create)
+    double* fscal;      // (4) frame scalars: thrust scale, F_x, F_y, M
+    unsigned long long* ptimes;  // (2 * kMaxPhaseTimes) [phase, globaltimer ns] or null
     // call arguments
     IcePtrs<T> in, out, tmp;
     ShipPtrs<T> ship_in, ship_out, ship_tmp[2];
@@ -178,11 +205,45 @@ __device__ __forceinline__ int bucket_of(int2 c, int n_buckets) {
     return (int)(h & (unsigned)(n_buckets - 1));
 }
 
-// insert element e (position p) into the grid; record its cell and reference position
+// Neighbour lists are Verlet lists over reference positions: list(e) holds every
+// o with |ref_e - ref_o| < r_e + r_o + skin.  An element whose position leaves the
+// ball of radius 0.45 skin around its reference "escapes": it takes its current
+// position as new reference, and every element within reach of that new
+// reference rebuilds its list.  With |p - ref| <= skin/2 for every element, any
+// pair closer than r_e + r_o is in both lists, so the contact set equals the
+// all-pairs one of the reference (jax_ice_state.py:212-214).
+
 template <typename T>
-__device__ __forceinline__ void grid_insert(const KArgs<T>& a, int e, T px, T py) {
-    a.pos_ref[2 * e] = px;
-    a.pos_ref[2 * e + 1] = py;
+__device__ __forceinline__ bool escaped(const KArgs<T>& a, int e, T px, T py) {
+    const T rx = a.pos_ref[2 * e], ry = a.pos_ref[2 * e + 1];
+    const bool fp = jfinite(px) && jfinite(py);
+    const bool fr = jfinite(rx) && jfinite(ry);
+    if (fp != fr) return true;
+    if (!fp) return false;
+    // |p - ref| > 0.45 skin, evaluated with a 1 % lower threshold so rounding of
+    // the test can only make an element escape early, never late
+    const T dx = px - rx, dy = py - ry;
+    const T h = a.skin * T(0.45 * 0.99);
+    return dx * dx + dy * dy > h * h;
+}
+
+// one atomic per CTA: add the CTA's count of `v` to *ctr (all threads must call)
+__device__ __forceinline__ void cta_count_add(unsigned* ctr, int v) {
+    __shared__ int s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_cnt, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt) atomicAdd(ctr, (unsigned)s_cnt);
+    __syncthreads();
+}
+
+// Grid-hash buckets of fixed capacity.  An element that escapes is appended to
+// the bucket of its new home cell; its old entry goes stale and is ignored
+// (its home cell no longer matches) until the next compaction drops it.
+template <typename T>
+__device__ __forceinline__ void grid_put(const KArgs<T>& a, int e, T px, T py) {
     if (!(jfinite(px) && jfinite(py))) {
         a.ecell[e] = make_int2(INT_MIN, INT_MIN);
         return;
@@ -199,51 +260,68 @@ __device__ __forceinline__ void grid_insert(const KArgs<T>& a, int e, T px, T py
     if (slot + 1 > a.bucket_cap / 2) atomicMax((unsigned long long*)&a.stats[2], (unsigned long long)(slot + 1));
 }
 
-// Build element e's candidate list: every element within r_e + r_o + skin at the
-// positions of the last insert, sorted so that indices above e come first
-// (ascending), then indices below e (ascending) — the order in which the
-// reference's scatter-adds reach e (pairs (e, j>e) through pair_i, then pairs
-// (i<e, e) through pair_j; jax_simulation.py:152-162).
-template <typename T>
-__device__ void build_neighbors(const KArgs<T>& a, int e) {
-    T px = a.pos_ref[2 * e], py = a.pos_ref[2 * e + 1];
+// Visit every element o != e whose reference lies within r_e + r_o + skin of
+// ref_e (a conservative superset: the test is done in double with a margin).
+// An element can sit twice in one bucket (a stale and a current entry when its
+// old and new cells hash together); callers that collect must deduplicate.
+template <typename T, typename Fn>
+__device__ __forceinline__ void for_each_near(const KArgs<T>& a, int e, Fn fn) {
     int2 c = a.ecell[e];
-    int cnt = 0;
-    int loc[kMaxNbLocal];
-    if (c.x != INT_MIN) {
-        const T re = a.radii[e];
-        for (int dy = -1; dy <= 1; ++dy) {
-            for (int dx = -1; dx <= 1; ++dx) {
-                int2 cc = make_int2(c.x + dx, c.y + dy);
-                int b = bucket_of(cc, a.n_buckets);
-                int m = min(a.bcnt[b], a.bucket_cap);
-                for (int k = 0; k < m; ++k) {
-                    int o = a.bitems[(size_t)b * a.bucket_cap + k];
-                    if (o == e) continue;
-                    int2 oc = a.ecell[o];
-                    if (oc.x != cc.x || oc.y != cc.y) continue;  // hash collision
-                    T ox = a.pos_ref[2 * o] - px, oy = a.pos_ref[2 * o + 1] - py;
-                    double d2 = (double)ox * ox + (double)oy * oy;
-                    double lim = ((double)re + (double)a.radii[o] + (double)a.skin) * (1.0 + 1e-5) + 1e-6;
-                    if (d2 < lim * lim) {
-                        if (cnt < a.max_nb) loc[cnt] = o;
-                        ++cnt;
+    if (c.x == INT_MIN) return;
+    const T px = a.pos_ref[2 * e], py = a.pos_ref[2 * e + 1];
+    const double re = (double)a.radii[e] + (double)a.skin;
+    for (int dy = -1; dy <= 1; ++dy) {
+        for (int dx = -1; dx <= 1; ++dx) {
+            int2 cc = make_int2(c.x + dx, c.y + dy);
+            int b = bucket_of(cc, a.n_buckets);
+            int m = min(a.bcnt[b], a.bucket_cap);
+            const int* it = a.bitems + (size_t)b * a.bucket_cap;
+            for (int k0 = 0; k0 < m; k0 += 2) {
+                int ob[2];
+                int2 oc[2];
+                T ox[2], oy[2], orr[2];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    ob[j] = (k0 + j < m) ? it[k0 + j] : -1;
+                    if (ob[j] >= 0) {
+                        oc[j] = a.ecell[ob[j]];
+                        ox[j] = a.pos_ref[2 * ob[j]];
+                        oy[j] = a.pos_ref[2 * ob[j] + 1];
+                        orr[j] = a.radii[ob[j]];
                     }
+                }
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    int o = ob[j];
+                    if (o < 0 || o == e) continue;
+                    if (oc[j].x != cc.x || oc[j].y != cc.y) continue;  // stale entry or hash collision
+                    double ddx = (double)ox[j] - (double)px, ddy = (double)oy[j] - (double)py;
+                    double lim = (re + (double)orr[j]) * (1.0 + 1e-5) + 1e-6;
+                    if (ddx * ddx + ddy * ddy < lim * lim) fn(o);
                 }
             }
         }
     }
-    if (cnt > a.max_nb) {
-        atomicMax(a.status, DEM_ERR_CAPACITY);
-    }
-    {
-        unsigned am = __activemask();
-        int wmax = __reduce_max_sync(am, cnt);
-        if ((threadIdx.x & 31) == (__ffs(am) - 1) && wmax > 0)
-            atomicMax((unsigned long long*)&a.stats[1], (unsigned long long)wmax);
-    }
-    int m = min(cnt, a.max_nb);
-    // insertion sort (lists are short)
+}
+
+// Build element e's list sorted so that indices above e come first (ascending),
+// then indices below e (ascending) — the order in which the reference's
+// scatter-adds reach e: pairs (e, j>e) through pair_i, then pairs (i<e, e)
+// through pair_j (jax_simulation.py:152-162).
+template <typename T>
+__device__ void build_neighbors(const KArgs<T>& a, int e) {
+    int cnt = 0;
+    int loc[kMaxNbLocal];
+    const int cap = a.max_nb;
+    for_each_near(a, e, [&](int o) {
+        for (int i = 0; i < min(cnt, cap); ++i)
+            if (loc[i] == o) return;  // duplicate entry of one element
+        if (cnt < cap) loc[cnt] = o;
+        ++cnt;
+    });
+    if (cnt > cap) atomicMax(a.status, DEM_ERR_CAPACITY);
+    if (cnt > 16) atomicMax((unsigned long long*)&a.stats[1], (unsigned long long)cnt);
+    int m = min(cnt, cap);
     for (int i = 1; i < m; ++i) {
         int v = loc[i];
         int j = i - 1;
@@ -259,6 +337,71 @@ __device__ void build_neighbors(const KArgs<T>& a, int e) {
     for (int i = split; i < m; ++i) a.nbr[(size_t)(w++) * a.n + e] = loc[i];
     for (int i = 0; i < split; ++i) a.nbr[(size_t)(w++) * a.n + e] = loc[i];
     a.ncnt[e] = m;
+}
+
+// R1: escaped elements take their current position as reference and are
+// appended to the bucket of their new home cell.
+template <typename T>
+__device__ void phase_reref(const KArgs<T>& a, const T* kin) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    for (int e = gtid; e < a.n; e += gsz) {
+        if (!a.esc[e]) continue;
+        const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+        a.pos_ref[2 * e] = px;
+        a.pos_ref[2 * e + 1] = py;
+        grid_put(a, e, px, py);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&a.stats[0], 1ull);
+}
+
+// R2: an escaped element and every element within reach of its new reference
+// need a new list.
+template <typename T>
+__device__ void phase_mark(const KArgs<T>& a) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    for (int e = gtid; e < a.n; e += gsz) {
+        if (!a.esc[e]) continue;
+        a.dirty[e] = 1;
+        for_each_near(a, e, [&](int o) { a.dirty[o] = 1; });
+    }
+}
+
+// R3: rebuild the marked lists (all of them when most elements escaped).
+template <typename T>
+__device__ void phase_build(const KArgs<T>& a, bool all) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    for (int e = gtid; e < a.n; e += gsz) {
+        if (all || a.dirty[e]) build_neighbors(a, e);
+        a.dirty[e] = 0;
+        a.esc[e] = 0;
+    }
+}
+
+// Drop stale and duplicate bucket entries (run while nothing reads the grid).
+template <typename T>
+__device__ void compact_buckets(const KArgs<T>& a) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    for (int b = gtid; b < a.n_buckets; b += gsz) {
+        int m = a.bcnt[b];
+        if (m == 0) continue;
+        m = min(m, a.bucket_cap);
+        int* it = a.bitems + (size_t)b * a.bucket_cap;
+        int w = 0;
+        for (int k = 0; k < m; ++k) {
+            int o = it[k];
+            int2 c = a.ecell[o];
+            if (c.x == INT_MIN || bucket_of(c, a.n_buckets) != b) continue;
+            bool dup = false;
+            for (int q = 0; q < w; ++q)
+                if (it[q] == o) dup = true;
+            if (!dup) it[w++] = o;
+        }
+        a.bcnt[b] = w;
+    }
 }
 
 // ─── ship contact (jax_geometry.py) ─────────────────────────────────────────
@@ -309,135 +452,6 @@ __device__ __forceinline__ void hull_point(const HullPose<T>& H, T px, T py, T& 
     pen = jmax(praw, T(0));
 }
 
-// Per-element maximum-penetration contact: pass 1 (ice vertices + edge samples
-// vs the analytic hull), pass 2 (hull outline points inside the ice polygon),
-// element-wise max (jax_geometry.py:515-594).  hullw: hull outline in world frame.
-template <typename T>
-__device__ void element_contact(const KArgs<T>& a, int e, const HullPose<T>& H, const T* hullw,
-                                T px, T py, T rot, T& pen_o, T& nx_o, T& ny_o) {
-    const int V = a.V;
-    const int E = a.P.n_edge_samples;
-    T c, s;
-    jsincos(rot, &s, &c);
-    T wx[kMaxV], wy[kMaxV];
-    bool mk[kMaxV];
-    const T* lp = a.polys + (size_t)e * V * 2;
-    for (int k = 0; k < V; ++k) {
-        T lx = lp[2 * k], ly = lp[2 * k + 1];
-        wx[k] = c * lx - s * ly + px;
-        wy[k] = s * lx + c * ly + py;
-        mk[k] = a.pmask[(size_t)e * V + k] != 0;
-    }
-    // pass 1: points ordered vertex k, then its E edge samples (jax_geometry.py:190-211)
-    T best1 = T(0), bnx1 = T(0), bny1 = T(0);
-    bool first = true;
-    for (int k = 0; k < V; ++k) {
-        int k1 = (k + 1 == V) ? 0 : k + 1;
-        for (int j = 0; j <= E; ++j) {
-            T qx, qy;
-            if (j == 0) {
-                qx = wx[k];
-                qy = wy[k];
-            } else {
-                T t = a.t_samp[j - 1];
-                T omt = T(1) - t;
-                qx = wx[k] * omt + wx[k1] * t;
-                qy = wy[k] * omt + wy[k1] * t;
-            }
-            T p, nx, ny;
-            hull_point(H, qx, qy, p, nx, ny);
-            if (!mk[k]) p = T(0);
-            // argmax, first index wins
-            if (first || p > best1) {
-                best1 = p;
-                bnx1 = nx;
-                bny1 = ny;
-                first = false;
-            }
-        }
-    }
-    // pass 2 (jax_geometry.py:300-510)
-    T best2 = T(0), bnx2 = T(0), bny2 = T(0);
-    {
-        T mx[kMaxV], my[kMaxV], mc[kMaxV];
-        for (int k = 0; k < V; ++k) {
-            mx[k] = mk[k] ? wx[k] : T(0);
-            my[k] = mk[k] ? wy[k] : T(0);
-            mc[k] = mk[k] ? T(1) : T(0);
-        }
-        T n_real = jmax(np_pairwise_sum(mc, V), T(1));
-        T cxc = np_pairwise_sum(mx, V) / n_real;
-        T cyc = np_pairwise_sum(my, V) / n_real;
-        T enx[kMaxV], eny[kMaxV];
-        for (int k = 0; k < V; ++k) {
-            int k1 = (k + 1 == V) ? 0 : k + 1;
-            T ex = wx[k1] - wx[k], ey = wy[k1] - wy[k];
-            T nxe = ey, nye = -ex;
-            T nlen = jsqrt(nxe * nxe + nye * nye + T(1e-20));
-            nxe = nxe / nlen;
-            nye = nye / nlen;
-            T midx = (wx[k] + wx[k1]) / T(2), midy = (wy[k] + wy[k1]) / T(2);
-            T dotc = (midx - cxc) * nxe + (midy - cyc) * nye;
-            if (dotc < T(0)) {
-                nxe = -nxe;
-                nye = -nye;
-            }
-            enx[k] = nxe;
-            eny[k] = nye;
-        }
-        bool firsts = true;
-        for (int si = 0; si < a.S; ++si) {
-            T hx = hullw[2 * si], hy = hullw[2 * si + 1];
-            int crossings = 0;
-            T dmin = T(0);
-            int kbest = 0;
-            for (int k = 0; k < V; ++k) {
-                int k1 = (k + 1 == V) ? 0 : k + 1;
-                T xi = wx[k], yi = wy[k], xj = wx[k1], yj = wy[k1];
-                bool cond_y = (yi > hy) != (yj > hy);
-                T x_int = (xj - xi) * (hy - yi) / (yj - yi + T(1e-10)) + xi;
-                if (cond_y && (hx < x_int)) ++crossings;
-                T vx = xj - xi, vy = yj - yi;
-                T wx_ = hx - xi, wy_ = hy - yi;
-                T c1 = wx_ * vx + wy_ * vy;
-                T c2 = vx * vx + vy * vy + T(1e-20);
-                T t = jclip(c1 / c2, T(0), T(1));
-                T qx = xi + t * vx, qy = yi + t * vy;
-                T ddx = hx - qx, ddy = hy - qy;
-                T d = jsqrt(ddx * ddx + ddy * ddy + T(1e-20));
-                if (k == 0 || d < dmin) {  // argmin, first index wins
-                    dmin = d;
-                    kbest = k;
-                }
-            }
-            bool inside = (crossings % 2) == 1;
-            T p = inside ? dmin : T(0);
-            T nx = inside ? enx[kbest] : T(0);
-            T ny = inside ? eny[kbest] : T(0);
-            if (firsts || p > best2) {  // argmax over hull points
-                best2 = p;
-                bnx2 = nx;
-                bny2 = ny;
-                firsts = false;
-            }
-        }
-        if (!(best2 > T(0))) {
-            best2 = T(0);
-            bnx2 = T(0);
-            bny2 = T(0);
-        }
-    }
-    if (best2 > best1) {
-        pen_o = best2;
-        nx_o = bnx2;
-        ny_o = bny2;
-    } else {
-        pen_o = best1;
-        nx_o = bnx1;
-        ny_o = bny1;
-    }
-}
-
 // ─── fixed-order block sum (deterministic, independent of the grid size) ────
 template <int N>
 __device__ __forceinline__ void block_sum3(double v0, double v1, double v2, double* out3) {
@@ -462,27 +476,212 @@ __device__ __forceinline__ void block_sum3(double v0, double v1, double v2, doub
     __syncthreads();
 }
 
-// ─── P_CONTACT ──────────────────────────────────────────────────────────────
 template <typename T>
-__device__ void phase_contact(const KArgs<T>& a, const Frame<T>& F, T* hullw_sh) {
-    const DemParams& P = a.P;
-    const T sx = F.ship_src.eta[0], sy = F.ship_src.eta[1], spsi = F.ship_src.eta[2];
+__device__ __forceinline__ HullPose<T> hull_pose(const KArgs<T>& a, const Frame<T>& F) {
     HullPose<T> H;
-    H.sx = sx;
-    H.sy = sy;
+    H.sx = F.ship_src.eta[0];
+    H.sy = F.ship_src.eta[1];
+    const T spsi = F.ship_src.eta[2];
     jsincos(-spsi, &H.s_neg, &H.c_neg);
     jsincos(spsi, &H.s_h, &H.c_h);
-    H.hl = T(P.half_len);
-    H.hb = T(P.half_beam);
-    H.hb005 = T(P.half_beam * 0.05);
+    H.hl = T(a.P.half_len);
+    H.hb = T(a.P.half_beam);
+    H.hb005 = T(a.P.half_beam * 0.05);
+    return H;
+}
+
+// ─── P_CULL: elements whose bounding circle reaches the hull; escapes ───────
+template <typename T>
+__device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    const T sx = F.ship_src.eta[0], sy = F.ship_src.eta[1];
+    const T reach = a.hull_r * T(1.0001) + T(1e-3);
+    // per-floe scratch of this frame (read last by the previous frame's fracture)
+    for (int fl = gtid; fl < a.nf; fl += gsz) {
+        a.fcoll[fl] = 0;
+        a.fmax[fl] = 0ull;
+    }
+    int nesc = 0;
+    for (int e = gtid; e < a.n; e += gsz) {
+        typename vec2_of<T>::type p = ld2(F.src.pos, e);
+        const T ddx = p.x - sx, ddy = p.y - sy;
+        const T lim = reach + a.vert_r[e];
+        // every query point of e lies within vert_r of its centroid and every hull
+        // point within hull_r of the ship: farther elements get pen = 0, which is
+        // what all of their point tests return (jax_geometry.py:104-134, :359-368);
+        // the test keeps NaN positions (comparison false) on the exact path
+        if (!(ddx * ddx + ddy * ddy > lim * lim * T(1.0001))) {
+            const int slot = atomicAdd(a.near_cnt, 1);
+            a.near_list[slot] = e;
+        } else {
+            a.cpen[e] = T(0);
+            a.cnx[e] = T(0);
+            a.cny[e] = T(0);
+        }
+        if (escaped(a, e, p.x, p.y)) {
+            a.esc[e] = 1;
+            ++nesc;
+        }
+    }
+    cta_count_add(&a.esc_cnt[0], nesc);
+}
+
+// ─── P_NEAR: one warp per near element (jax_geometry.py:515-594) ────────────
+// Pass 1: the element's vertices and edge samples vs the analytic hull; pass 2:
+// the hull outline points inside the element's polygon; element-wise max.  Lanes
+// split the points; argmax/argmin keep the reference's first-index ties.
+template <typename T>
+struct Best {
+    T p, nx, ny;
+    int i;
+};
+
+template <typename T>
+__device__ __forceinline__ void better(Best<T>& b, T p, T nx, T ny, int i) {
+    if (p > b.p || (p == b.p && i < b.i)) {
+        b.p = p;
+        b.nx = nx;
+        b.ny = ny;
+        b.i = i;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ Best<T> warp_best(Best<T> b) {
+    for (int off = 16; off > 0; off >>= 1) {
+        Best<T> o;
+        o.p = __shfl_xor_sync(0xffffffffu, b.p, off);
+        o.nx = __shfl_xor_sync(0xffffffffu, b.nx, off);
+        o.ny = __shfl_xor_sync(0xffffffffu, b.ny, off);
+        o.i = __shfl_xor_sync(0xffffffffu, b.i, off);
+        better(b, o.p, o.nx, o.ny, o.i);
+    }
+    return b;
+}
+
+template <typename T>
+__device__ void phase_near(const KArgs<T>& a, const Frame<T>& F, T* hullw) {
+    const HullPose<T> H = hull_pose(a, F);
     // hull outline in world frame: ship_hull_local @ R.T + [x, y] (jax_geometry.py:568-572)
     for (int i = threadIdx.x; i < a.S; i += blockDim.x) {
         T lx = a.hull[2 * i], ly = a.hull[2 * i + 1];
-        hullw_sh[2 * i] = lx * H.c_h + ly * (-H.s_h) + sx;
-        hullw_sh[2 * i + 1] = lx * H.s_h + ly * H.c_h + sy;
+        hullw[2 * i] = lx * H.c_h + ly * (-H.s_h) + H.sx;
+        hullw[2 * i + 1] = lx * H.s_h + ly * H.c_h + H.sy;
     }
     __syncthreads();
-    const T reach_base = a.hull_r;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nnear = *((volatile int*)a.near_cnt);
+    const int V = a.V;
+    const int E = a.P.n_edge_samples;
+    const int P1 = V * (1 + E);
+    for (int q = warp; q < nnear; q += nwarps) {
+        const int e = a.near_list[q];
+        typename vec2_of<T>::type pe = ld2(F.src.pos, e);
+        T c, sn;
+        jsincos(F.src.rot[e], &sn, &c);
+        const T* lp = a.polys + (size_t)e * V * 2;
+        const uint8_t* mk = a.pmask + (size_t)e * V;
+        // world vertex k (jax_geometry.py:176-180)
+        auto wv = [&](int k, T& x, T& y) {
+            T lx = lp[2 * k], ly = lp[2 * k + 1];
+            x = c * lx - sn * ly + pe.x;
+            y = sn * lx + c * ly + pe.y;
+        };
+        // pass 1: point index = vertex * (1 + E) + sample (jax_geometry.py:190-211)
+        Best<T> b1 = {T(0), T(0), T(0), INT_MAX};
+        for (int pt = lane; pt < P1; pt += 32) {
+            const int k = pt / (1 + E), j = pt % (1 + E);
+            T qx, qy;
+            wv(k, qx, qy);
+            if (j > 0) {
+                T x1, y1;
+                wv((k + 1 == V) ? 0 : k + 1, x1, y1);
+                T t = a.t_samp[j - 1];
+                T omt = T(1) - t;
+                qx = qx * omt + x1 * t;
+                qy = qy * omt + y1 * t;
+            }
+            T p, nx, ny;
+            hull_point(H, qx, qy, p, nx, ny);
+            if (!mk[k]) p = T(0);
+            better(b1, p, nx, ny, pt);
+        }
+        b1 = warp_best(b1);
+        // pass 2 (jax_geometry.py:300-510)
+        T wx[kMaxV], wy[kMaxV], mx[kMaxV], my[kMaxV], mc[kMaxV];
+        for (int k = 0; k < V; ++k) {
+            wv(k, wx[k], wy[k]);
+            const bool m = mk[k] != 0;
+            mx[k] = m ? wx[k] : T(0);
+            my[k] = m ? wy[k] : T(0);
+            mc[k] = m ? T(1) : T(0);
+        }
+        const T n_real = jmax(np_pairwise_sum(mc, V), T(1));
+        const T cxc = np_pairwise_sum(mx, V) / n_real;
+        const T cyc = np_pairwise_sum(my, V) / n_real;
+        Best<T> b2 = {T(0), T(0), T(0), INT_MAX};
+        for (int si = lane; si < a.S; si += 32) {
+            const T hx = hullw[2 * si], hy = hullw[2 * si + 1];
+            int crossings = 0;
+            T dmin = T(0);
+            int kbest = 0;
+            for (int k = 0; k < V; ++k) {
+                const int k1 = (k + 1 == V) ? 0 : k + 1;
+                const T xi = wx[k], yi = wy[k], xj = wx[k1], yj = wy[k1];
+                const bool cond_y = (yi > hy) != (yj > hy);
+                const T x_int = (xj - xi) * (hy - yi) / (yj - yi + T(1e-10)) + xi;
+                if (cond_y && (hx < x_int)) ++crossings;
+                const T vx = xj - xi, vy = yj - yi;
+                const T c1 = (hx - xi) * vx + (hy - yi) * vy;
+                const T c2 = vx * vx + vy * vy + T(1e-20);
+                const T t = jclip(c1 / c2, T(0), T(1));
+                const T ddx = hx - (xi + t * vx), ddy = hy - (yi + t * vy);
+                const T d = jsqrt(ddx * ddx + ddy * ddy + T(1e-20));
+                if (k == 0 || d < dmin) {  // argmin, first index wins
+                    dmin = d;
+                    kbest = k;
+                }
+            }
+            T p = T(0), nx = T(0), ny = T(0);
+            if ((crossings % 2) == 1) {
+                // outward normal of the closest edge (jax_geometry.py:389-405)
+                const int k = kbest, k1 = (k + 1 == V) ? 0 : k + 1;
+                const T ex = wx[k1] - wx[k], ey = wy[k1] - wy[k];
+                T nxe = ey, nye = -ex;
+                const T nlen = jsqrt(nxe * nxe + nye * nye + T(1e-20));
+                nxe = nxe / nlen;
+                nye = nye / nlen;
+                const T midx = (wx[k] + wx[k1]) / T(2), midy = (wy[k] + wy[k1]) / T(2);
+                const T dotc = (midx - cxc) * nxe + (midy - cyc) * nye;
+                if (dotc < T(0)) {
+                    nxe = -nxe;
+                    nye = -nye;
+                }
+                p = dmin;
+                nx = nxe;
+                ny = nye;
+            }
+            better(b2, p, nx, ny, si);
+        }
+        b2 = warp_best(b2);
+        if (lane == 0) {
+            // pass 2 replaces pass 1 only where strictly deeper (jax_geometry.py:585-590)
+            const bool use2 = (b2.p > T(0)) && (b2.p > b1.p);
+            a.cpen[e] = use2 ? b2.p : b1.p;
+            a.cnx[e] = use2 ? b2.nx : b1.nx;
+            a.cny[e] = use2 ? b2.ny : b1.ny;
+        }
+    }
+}
+
+// ─── P_CFORCE: ship force on ice, submergence, reductions (jax_simulation.py:431-496)
+template <typename T>
+__device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
+    const DemParams& P = a.P;
+    const T sx = F.ship_src.eta[0], sy = F.ship_src.eta[1];
     const T wcf = T(P.w_contact_radius_factor), wcap = T(P.w_contact_cap);
     const T flex = T(P.flexural_strength_base);
     const T pcr = T(P.pen_crit_ref), pct = T(P.pen_crit_thickness_ref);
@@ -491,42 +690,35 @@ __device__ void phase_contact(const KArgs<T>& a, const Frame<T>& F, T* hullw_sh)
     const T inv_rise = T(1.0 / P.rise_time_const);
     const T dt = T(P.dt);
     const T rho_g = T(P.water_density * 9.81);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.near_cnt = 0;  // P_NEAR is done with it
     for (int chunk = blockIdx.x; chunk < a.nchunks; chunk += gridDim.x) {
         int e = chunk * kThreads + threadIdx.x;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
         if (e < a.n) {
             typename vec2_of<T>::type p = ld2(F.src.pos, e);
-            T rot = F.src.rot[e];
-            T pen = T(0), nx = T(0), ny = T(0);
-            T ddx = p.x - sx, ddy = p.y - sy;
-            double dist = sqrt((double)ddx * ddx + (double)ddy * ddy);
-            if (!(dist > (double)reach_base + (double)a.vert_r[e] + 1e-3)) {
-                element_contact(a, e, H, hullw_sh, p.x, p.y, rot, pen, nx, ny);
-            }
-            bool has = pen > T(0);
-            T h = a.thick[e];
-            T w_contact = jmin(wcf * a.radii[e], wcap);
-            T sigma_f = flex * jsqrt(h);
-            T f_break = sigma_f * w_contact * (h * h);
-            T pen_crit = pcr * (h / pct);
-            T fm = has ? f_break * jmin(pen / jmax(pen_crit, T(1e-10)), T(1)) : T(0);
+            const T pen = a.cpen[e], nx = a.cnx[e], ny = a.cny[e];
+            const bool has = pen > T(0);
+            const T h = a.thick[e];
+            const T w_contact = jmin(wcf * a.radii[e], wcap);
+            const T sigma_f = flex * jsqrt(h);
+            const T f_break = sigma_f * w_contact * (h * h);
+            const T pen_crit = pcr * (h / pct);
+            const T fm = has ? f_break * jmin(pen / jmax(pen_crit, T(1e-10)), T(1)) : T(0);
             T so_x = fm * nx;
             T so_y = fm * ny;
-            T rel_y = p.y - sy;
-            so_y = so_y + spf * fm * jsign(rel_y);
+            so_y = so_y + spf * fm * jsign(p.y - sy);
             // moment on the ship uses the force before the thrust cap (jax_simulation.py:474-477)
-            T rx = p.x - sx, ry = p.y - sy;
-            T mom = has ? (rx * (-so_y) - ry * (-so_x)) : T(0);
+            const T rx = p.x - sx, ry = p.y - sy;
+            const T mom = has ? (rx * (-so_y) - ry * (-so_x)) : T(0);
             s0 = (double)so_x;
             s1 = (double)so_y;
             s2 = (double)mom;
             // submergence and buoyancy (jax_simulation.py:480-496)
-            T sub = F.src.sub[e];
-            T pen_c = jmin(pen, scap);
-            T new_sub = has ? jmin(sub + srate * pen_c * dt, h)
-                            : jmax(T(0), sub - inv_rise * sub * dt);
-            T z_sub = jmin(new_sub, h);
-            T f_buoy = rho_g * a.areas[e] * z_sub;
+            const T sub = F.src.sub[e];
+            const T pen_c = jmin(pen, scap);
+            const T new_sub = has ? jmin(sub + srate * pen_c * dt, h) : jmax(T(0), sub - inv_rise * sub * dt);
+            const T z_sub = jmin(new_sub, h);
+            const T f_buoy = rho_g * a.areas[e] * z_sub;
             if (has) {
                 so_x = so_x + f_buoy * nx;
                 so_y = so_y + f_buoy * ny;
@@ -535,7 +727,7 @@ __device__ void phase_contact(const KArgs<T>& a, const Frame<T>& F, T* hullw_sh)
             a.fraw[e] = fm;
             F.dst.sub[e] = new_sub;
             if (a.d_pen) a.d_pen[e] = pen;
-            int fl = a.floe_of[e];
+            const int fl = a.floe_of[e];
             if (has) atomicMax(&a.fcoll[fl], 1);
             if (fm > T(0)) {
                 if (sizeof(T) == 4)
@@ -543,17 +735,6 @@ __device__ void phase_contact(const KArgs<T>& a, const Frame<T>& F, T* hullw_sh)
                 else
                     atomicMax(&a.fmax[fl], d2ord((double)fm));
             }
-            // crack front: element touches a bond that is broken at frame start
-            uint8_t ck = 0;
-            for (int sl = a.boff[e]; sl < a.boff[e + 1]; ++sl) {
-                int b = a.bslot[sl].x & 0x7fffffff;
-                if (!F.src.intact[b]) {
-                    ck = 1;
-                    break;
-                }
-            }
-            a.crack[e] = ck;
-            grid_insert(a, e, p.x, p.y);
         }
         double r3[3];
         block_sum3<kThreads>(s0, s1, s2, r3);
@@ -685,111 +866,134 @@ __device__ __forceinline__ T thrust_scale_of(const KArgs<T>& a, const double* to
 }
 
 template <typename T>
-__device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F, T* scale_out) {
-    __shared__ double tot3[3];
-    double r[3];
-    frame_totals(a, r);
-    if (threadIdx.x == 0) {
-        tot3[0] = r[0];
-        tot3[1] = r[1];
-        tot3[2] = r[2];
-    }
-    __syncthreads();
-    const T scale = thrust_scale_of(a, tot3);
-    *scale_out = scale;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // reaction on the ship (jax_simulation.py:470-478)
-        T Fx = -(T(tot3[0]) * scale), Fy = -(T(tot3[1]) * scale), M = T(tot3[2]);
-        T tau[3] = {Fx, Fy, M};
-        T J = jsqrt(Fx * Fx + Fy * Fy) * T(a.P.dt);
-        T sp[3] = {F.sp[0], F.sp[1], F.sp[2]};
-        const T* eta = F.ship_src.eta;
-        if (a.P.ice_brake_threshold > 0.0) {  // jax_simulation.py:658-669
-            T thr = T(a.P.ice_brake_threshold);
-            T bf = jclip(thr / jmax(fabs(tau[0]), thr), T(0.1), T(1));
-            sp[0] = eta[0] + bf * (F.sp[0] - eta[0]);
-            sp[1] = eta[1] + bf * (F.sp[1] - eta[1]);
+__device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
+    typedef typename vec2_of<T>::type V2;
+    if (blockIdx.x == 0) {
+        __shared__ double tot3[3];
+        double r[3];
+        frame_totals(a, r);
+        if (threadIdx.x == 0) {
+            tot3[0] = r[0];
+            tot3[1] = r[1];
+            tot3[2] = r[2];
         }
-        T eta_o[3], nu_o[3], na_o[6], ei_o[3];
-        ship_step<T>(a.P, eta, F.ship_src.nu, F.ship_src.na, F.ship_src.ei, sp, F.sp + 3, tau, F.vws,
-                     eta_o, nu_o, na_o, ei_o);
-        for (int i = 0; i < 3; ++i) {
-            F.ship_dst.eta[i] = eta_o[i];
-            F.ship_dst.nu[i] = nu_o[i];
-            F.ship_dst.ei[i] = ei_o[i];
-        }
-        for (int i = 0; i < 6; ++i) F.ship_dst.na[i] = na_o[i];
-        if (a.d_F) {
-            a.d_F[0] = Fx;
-            a.d_F[1] = Fy;
-        }
-        if (a.d_J) a.d_J[0] = J;
-        if (a.h_eta)
-            for (int i = 0; i < 3; ++i) a.h_eta[F.f * 3 + i] = eta_o[i];
-        if (a.h_J) a.h_J[F.f] = J;
-        if (a.h_F) {
-            a.h_F[F.f * 2] = Fx;
-            a.h_F[F.f * 2 + 1] = Fy;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const T scale = thrust_scale_of(a, tot3);
+            // reaction on the ship (jax_simulation.py:470-478)
+            T Fx = -(T(tot3[0]) * scale), Fy = -(T(tot3[1]) * scale), M = T(tot3[2]);
+            a.fscal[0] = (double)scale;
+            a.fscal[1] = (double)Fx;
+            a.fscal[2] = (double)Fy;
+            a.fscal[3] = (double)M;
+            T tau[3] = {Fx, Fy, M};
+            T J = jsqrt(Fx * Fx + Fy * Fy) * T(a.P.dt);
+            T sp[3] = {F.sp[0], F.sp[1], F.sp[2]};
+            const T* eta = F.ship_src.eta;
+            if (a.P.ice_brake_threshold > 0.0) {  // jax_simulation.py:658-669
+                T thr = T(a.P.ice_brake_threshold);
+                T bf = jclip(thr / jmax(fabs(tau[0]), thr), T(0.1), T(1));
+                sp[0] = eta[0] + bf * (F.sp[0] - eta[0]);
+                sp[1] = eta[1] + bf * (F.sp[1] - eta[1]);
+            }
+            T eta_o[3], nu_o[3], na_o[6], ei_o[3];
+            ship_step<T>(a.P, eta, F.ship_src.nu, F.ship_src.na, F.ship_src.ei, sp, F.sp + 3, tau, F.vws,
+                         eta_o, nu_o, na_o, ei_o);
+            for (int i = 0; i < 3; ++i) {
+                F.ship_dst.eta[i] = eta_o[i];
+                F.ship_dst.nu[i] = nu_o[i];
+                F.ship_dst.ei[i] = ei_o[i];
+            }
+            for (int i = 0; i < 6; ++i) F.ship_dst.na[i] = na_o[i];
+            if (a.d_F) {
+                a.d_F[0] = Fx;
+                a.d_F[1] = Fy;
+            }
+            if (a.d_J) a.d_J[0] = J;
+            if (a.h_eta)
+                for (int i = 0; i < 3; ++i) a.h_eta[F.f * 3 + i] = eta_o[i];
+            if (a.h_J) a.h_J[F.f] = J;
+            if (a.h_F) {
+                a.h_F[F.f * 2] = Fx;
+                a.h_F[F.f * 2 + 1] = Fy;
+            }
         }
     }
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
-    // floe eligibility (jax_simulation.py:513-524)
-    const T thr = a.min_bstr * T(a.P.effective_strength_collision);
-    for (int fl = gtid; fl < a.nf; fl += gsz) {
-        uint8_t el = F.elig_in[fl];
-        if (a.nb > 0 && a.fcoll[fl]) {
-            unsigned long long bits = a.fmax[fl];
-            T fmx = (sizeof(T) == 4) ? T(__uint_as_float((unsigned)bits)) : T(__longlong_as_double((long long)bits));
-            // max(force * scale) == max(force) * scale: rounding is monotone
-            if (fmx * scale > thr) el = 1;
-        }
-        F.dst.elig[fl] = el;
-    }
-    // activation, diag force and neighbour lists
+    SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
     for (int e = gtid; e < a.n; e += gsz) {
-        F.dst.active[e] = (F.src.active[e] || a.fcoll[a.floe_of[e]]) ? 1 : 0;
-        if (a.d_fmag) a.d_fmag[e] = a.fraw[e] * scale;
-        build_neighbors(a, e);
+        // activation (jax_simulation.py:498-509)
+        const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
+        F.dst.active[e] = ae ? 1 : 0;
+        // packed kinematics read by substep 0
+        const V2 p = ld2(F.src.pos, e), v = ld2(F.src.vel, e);
+        T* k0 = a.kin[0] + 4 * (size_t)e;
+        k0[0] = p.x;
+        k0[1] = p.y;
+        k0[2] = v.x;
+        k0[3] = v.y;
+        // bond slot records for this frame; crack front = touches a broken bond
+        uint8_t ck = 0;
+        const int s0 = a.boff[e], s1 = a.boff[e + 1];
+        for (int sl = s0; sl < s1; ++sl) {
+            const int2 ent = a.bslot[sl];
+            const int b = ent.x & 0x7fffffff;
+            const int o = ent.y;
+            const bool in = F.src.intact[b] != 0;
+            ck |= (uint8_t)!in;
+            const bool ao = F.src.active[o] || a.fcoll[a.floe_of[o]];
+            SlotRec<T> r;
+            r.o = (ent.x < 0) ? (int)((unsigned)o | 0x80000000u) : o;
+            r.rest = a.slot_rest[sl];
+            r.stiff = a.slot_stiff[sl];
+            r.omd = (in && ao == ae) ? T(1) - F.src.dmg[b] : T(-1);
+            rec[sl] = r;
+        }
+        a.crack[e] = ck;
     }
-}
-
-// ─── P_INSERT (mid-frame rebuild) ───────────────────────────────────────────
-template <typename T>
-__device__ void phase_insert(const KArgs<T>& a, const T* pos) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    for (int e = gtid; e < a.n; e += gsz) {
-        typename vec2_of<T>::type p = ld2(pos, e);
-        grid_insert(a, e, p.x, p.y);
-    }
-}
-
-template <typename T>
-__device__ void phase_nbr(const KArgs<T>& a) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    for (int e = gtid; e < a.n; e += gsz) build_neighbors(a, e);
 }
 
 // ─── P_FORCE: one substep (jax_simulation.py:63-268, 363-395) ───────────────
+// One thread per element, gather form: each element sums its own bond and
+// contact terms in the reference's scatter order, so no atomics are needed.
+// Kinematics are packed {x, y, vx, vy} (one 16-byte load per neighbour) and bond
+// slots are 16-byte records; loads of a batch are issued before any is used.
+// Contact distances and every predicate are computed unfused (-fmad=false);
+// force values use explicit fma where the reference's products are summed.
+constexpr int kBatch = 4;
+
+template <typename T> struct vec4_of;
+template <> struct vec4_of<float> { typedef float4 type; };
+template <> struct vec4_of<double> { typedef double4 type; };
+
 template <typename T>
-__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, bool clear_buckets,
-                            unsigned* gdisp_slot) {
+__device__ __forceinline__ typename vec4_of<T>::type ld4(const T* p, int i) {
+    return reinterpret_cast<const typename vec4_of<T>::type*>(p)[i];
+}
+
+__device__ __forceinline__ float jfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double jfma(double a, double b, double c) { return fma(a, b, c); }
+
+template <typename T>
+__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s) {
+    typedef typename vec2_of<T>::type V2;
+    typedef typename vec4_of<T>::type V4;
     const DemParams& P = a.P;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
     const int k = a.k_sub;
-    const T* pin = (s == 0) ? F.src.pos : a.sp_pos[(s - 1) & 1];
-    const T* vin = (s == 0) ? F.src.vel : a.sp_vel[(s - 1) & 1];
+    const T* kin = a.kin[s & 1];
+    T* kout = a.kin[(s + 1) & 1];
     const T* rin = (s == 0) ? F.src.rot : a.sp_rot[(s - 1) & 1];
     const T* ain = (s == 0) ? F.src.avel : a.sp_avel[(s - 1) & 1];
-    T* pout = (s == k - 1) ? F.dst.pos : a.sp_pos[s & 1];
-    T* vout = (s == k - 1) ? F.dst.vel : a.sp_vel[s & 1];
-    T* rout = (s == k - 1) ? F.dst.rot : a.sp_rot[s & 1];
-    T* aout = (s == k - 1) ? F.dst.avel : a.sp_avel[s & 1];
+    const bool last = (s == k - 1);
+    T* rout = last ? F.dst.rot : a.sp_rot[s & 1];
+    T* aout = last ? F.dst.avel : a.sp_avel[s & 1];
     const uint8_t* act = F.dst.active;
+    const SlotRec<T>* rec = reinterpret_cast<const SlotRec<T>*>(a.slotrec);
     const T hf = T(P.hertz_factor), hexp = T(P.hertz_exponent);
+    const bool h15 = (P.hertz_exponent == 1.5);
     const T mu = T(P.ice_ice_friction), fcap = T(P.friction_cap);
     const T c_drag = T(0.5 * P.water_density * P.c_d_drag);
     const T href = T(P.drag_ref_thickness);
@@ -798,166 +1002,174 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, bool cl
     const T dti = T(P.dt_ice);
     const T damp = T(P.angular_damping), alo = T(P.angular_cap_lo), ahi = T(P.angular_cap_hi);
     const T vclip = T(P.velocity_clip), pclip = T(P.position_clip);
-    float dmax2 = 0.0f;
-    if (clear_buckets)
-        for (int b = gtid; b < a.n_buckets; b += gsz) a.bcnt[b] = 0;
+    const bool check_escape = !last;
+    int nesc = 0;
     for (int e = gtid; e < a.n; e += gsz) {
-        typename vec2_of<T>::type pe = ld2(pin, e);
-        typename vec2_of<T>::type ve = ld2(vin, e);
+        const V4 ke = ld4(kin, e);
         const bool ae = act[e] != 0;
         // bond forces (jax_simulation.py:63-108): slots with e == bond_i first, then e == bond_j
         T fbx = T(0), fby = T(0), mb = T(0);
         const int s0 = a.boff[e], s1 = a.boff[e + 1];
-        for (int sl = s0; sl < s1; ++sl) {
-            int2 ent = a.bslot[sl];
-            int b = ent.x & 0x7fffffff;
-            bool role_j = (ent.x < 0);
-            int o = ent.y;
-            if (!F.src.intact[b]) continue;
-            if ((act[o] != 0) != ae) continue;  // endpoints must share the active state
-            typename vec2_of<T>::type po = ld2(pin, o);
-            T dx, dy;
-            if (!role_j) {
-                dx = po.x - pe.x;
-                dy = po.y - pe.y;
-            } else {
-                dx = pe.x - po.x;
-                dy = pe.y - po.y;
+        for (int base = s0; base < s1; base += kBatch) {
+            SlotRec<T> r[kBatch];
+            V4 ko[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+                if (base + j < s1) {
+                    r[j] = rec[base + j];
+                    ko[j] = ld4(kin, r[j].o & 0x7fffffff);
+                } else {
+                    r[j].omd = T(-1);
+                }
             }
-            T dist = jsqrt(dx * dx + dy * dy);
-            T dsafe = jmax(dist, T(1e-10));
-            T bx = dx / dsafe, by = dy / dsafe;
-            T stretch = dist - a.rest[b];
-            T fmag = a.bstiff[b] * stretch * (T(1) - F.src.dmg[b]);
-            T fx = bx * fmag, fy = by * fmag;
-            T cr = T(0.5) * (dx * fy - dy * fx);
-            if (!role_j) {
-                fbx += fx;
-                fby += fy;
-                mb += cr;
-            } else {
-                fbx += -fx;
-                fby += -fy;
-                mb += -cr;
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+                if (r[j].omd < T(0)) continue;  // broken, or active/frozen endpoints
+                const bool role_j = r[j].o < 0;
+                const T dx = role_j ? ke.x - ko[j].x : ko[j].x - ke.x;
+                const T dy = role_j ? ke.y - ko[j].y : ko[j].y - ke.y;
+                const T dist = jsqrt(dx * dx + dy * dy);
+                const T inv = T(1) / jmax(dist, T(1e-10));
+                const T fmag = r[j].stiff * (dist - r[j].rest) * r[j].omd;
+                const T fx = (dx * inv) * fmag, fy = (dy * inv) * fmag;
+                const T cr = T(0.5) * jfma(dx, fy, -(dy * fx));
+                if (!role_j) {
+                    fbx += fx;
+                    fby += fy;
+                    mb += cr;
+                } else {
+                    fbx -= fx;
+                    fby -= fy;
+                    mb -= cr;
+                }
             }
         }
         // ice-ice contact (jax_simulation.py:111-164)
         T fix = T(0), fiy = T(0), mi = T(0);
         const T re = a.radii[e];
         const int nc = a.ncnt[e];
-        for (int q = 0; q < nc; ++q) {
-            int o = a.nbr[(size_t)q * a.n + e];
-            typename vec2_of<T>::type po = ld2(pin, o);
-            const bool e_is_i = e < o;
-            T dx = e_is_i ? po.x - pe.x : pe.x - po.x;
-            T dy = e_is_i ? po.y - pe.y : pe.y - po.y;
-            T dist = jsqrt(dx * dx + dy * dy);
-            T ro = a.radii[o];
-            T min_dist = e_is_i ? re + ro : ro + re;
-            T overlap = jmax(min_dist - dist, T(0));
-            if (!(dist > T(1e-6))) overlap = T(0);
-            if (!(overlap > T(0))) continue;  // non-overlapping pairs add exact zeros
-            T dsafe = jmax(dist, T(1e-10));
-            T ux = dx / dsafe, uy = dy / dsafe;
-            T fn = hf * jpow(overlap, hexp);
-            T fnx = ux * fn, fny = uy * fn;
-            typename vec2_of<T>::type vo = ld2(vin, o);
-            T vrx = e_is_i ? vo.x - ve.x : ve.x - vo.x;
-            T vry = e_is_i ? vo.y - ve.y : ve.y - vo.y;
-            T vdot = vrx * ux + vry * uy;
-            T vtx = vrx - vdot * ux, vty = vry - vdot * uy;
-            T vtm = jsqrt(vtx * vtx + vty * vty);
-            T vts = jmax(vtm, T(1e-10));
-            T thx = -vtx / vts, thy = -vty / vts;
-            T ftm = jmin(mu * fn, fcap);
-            T ftx = T(0), fty = T(0);
-            if (vtm > T(1e-6)) {
-                ftx = thx * ftm;
-                fty = thy * ftm;
+        for (int base = 0; base < nc; base += kBatch) {
+            int idx[kBatch];
+            V4 ko[kBatch];
+            T ro[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) idx[j] = (base + j < nc) ? a.nbr[(size_t)(base + j) * a.n + e] : -1;
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+                if (idx[j] >= 0) {
+                    ko[j] = ld4(kin, idx[j]);
+                    ro[j] = a.radii[idx[j]];
+                }
             }
-            T oix = -fnx - ftx, oiy = -fny - fty;
-            T cr = -(dx * oiy - dy * oix);
-            if (e_is_i) {
-                fix += -fnx + ftx;
-                fiy += -fny + fty;
-                mi += T(0.5) * cr;
-            } else {
-                fix += fnx - ftx;
-                fiy += fny - fty;
-                mi += T(-0.5) * cr;
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+                const int o = idx[j];
+                if (o < 0) continue;
+                const bool e_is_i = e < o;
+                const T dx = e_is_i ? ko[j].x - ke.x : ke.x - ko[j].x;
+                const T dy = e_is_i ? ko[j].y - ke.y : ke.y - ko[j].y;
+                // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
+                const T dist = jsqrt(dx * dx + dy * dy);
+                const T min_dist = e_is_i ? re + ro[j] : ro[j] + re;
+                T overlap = jmax(min_dist - dist, T(0));
+                if (!(dist > T(1e-6))) overlap = T(0);
+                if (!(overlap > T(0))) continue;  // non-overlapping pairs add exact zeros
+                const T inv = T(1) / jmax(dist, T(1e-10));
+                const T ux = dx * inv, uy = dy * inv;
+                const T fn = hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, hexp));
+                const T fnx = ux * fn, fny = uy * fn;
+                const T vrx = e_is_i ? ko[j].z - ke.z : ke.z - ko[j].z;
+                const T vry = e_is_i ? ko[j].w - ke.w : ke.w - ko[j].w;
+                const T vdot = jfma(vrx, ux, vry * uy);
+                const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
+                const T vtm = jsqrt(vtx * vtx + vty * vty);
+                T ftx = T(0), fty = T(0);
+                if (vtm > T(1e-6)) {
+                    const T ftm = jmin(mu * fn, fcap) / vtm;
+                    ftx = -vtx * ftm;
+                    fty = -vty * ftm;
+                }
+                const T oix = -fnx - ftx, oiy = -fny - fty;
+                const T cr = -jfma(dx, oiy, -(dy * oix));
+                if (e_is_i) {
+                    fix += ftx - fnx;
+                    fiy += fty - fny;
+                    mi += T(0.5) * cr;
+                } else {
+                    fix += fnx - ftx;
+                    fiy += fny - fty;
+                    mi -= T(0.5) * cr;
+                }
             }
         }
         // drag (jax_simulation.py:167-192)
-        T h = a.thick[e], A = a.areas[e];
-        T a_drag = A * (h / href);
-        typename vec2_of<T>::type w = ld2(F.vw, e);
-        T vrx = ve.x - w.x, vry = ve.y - w.y;
-        T vm = jsqrt(vrx * vrx + vry * vry);
-        T vms = jmax(vm, T(1e-12));
+        const T h = a.thick[e], A = a.areas[e];
+        const T a_drag = A * (h / href);
+        const V2 w = ld2(F.vw, e);
+        const T vrx = ke.z - w.x, vry = ke.w - w.y;
+        const T vm = jsqrt(vrx * vrx + vry * vry);
         T fdx, fdy;
         if (vm > T(1e-6)) {
-            T mag = c_drag * a_drag * (vms * vms);
-            fdx = (vrx / vms) * mag;
-            fdy = (vry / vms) * mag;
+            const T q = c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
+            fdx = vrx * q;
+            fdy = vry * q;
         } else {
-            T cl = c_drag * a_drag * lin;
+            const T cl = c_drag * a_drag * lin;
             fdx = cl * vrx;
             fdy = cl * vry;
         }
         // rotational drag (jax_simulation.py:195-212)
-        T av = ain[e];
-        T sub = F.dst.sub[e];
-        T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
-        T r3 = jpow(re, T(3));
-        T md = c_rot * r3 * av * fabs(av) * a_sub;
-        typename vec2_of<T>::type so = ld2(a.soi, e);
-        T Fx = ((fbx + fix) - fdx) + so.x;
-        T Fy = ((fby + fiy) - fdy) + so.y;
-        T Mz = (mb + mi) + md;
+        const T av = ain[e];
+        const T sub = F.dst.sub[e];
+        const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
+        const T md = c_rot * a.r3[e] * av * fabs(av) * a_sub;
+        const V2 so = ld2(a.soi, e);
+        const T Fx = ((fbx + fix) - fdx) + so.x;
+        const T Fy = ((fby + fiy) - fdy) + so.y;
+        const T Mz = (mb + mi) + md;
         // semi-implicit Euler (jax_simulation.py:215-268)
-        T m = a.mass[e];
-        T nvx = jclip(ve.x + (Fx / m) * dti, -vclip, vclip);
-        T nvy = jclip(ve.y + (Fy / m) * dti, -vclip, vclip);
-        T npx = pe.x + nvx * dti, npy = pe.y + nvy * dti;
-        T alpha = Mz / a.inertia[e];
+        const T m = a.mass[e];
+        T nvx = jclip(ke.z + (Fx / m) * dti, -vclip, vclip);
+        T nvy = jclip(ke.w + (Fy / m) * dti, -vclip, vclip);
+        T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
+        const T alpha = Mz / a.inertia[e];
         T nav = jclip(av * damp + alpha * dti, alo, ahi);
-        T rot = rin[e];
+        const T rot = rin[e];
         T nrot = rot + nav * dti;
         if (!jfinite(nvx)) nvx = T(0);
         if (!jfinite(nvy)) nvy = T(0);
-        if (!jfinite(npx)) npx = pe.x;
-        if (!jfinite(npy)) npy = pe.y;
+        if (!jfinite(npx)) npx = ke.x;
+        if (!jfinite(npy)) npy = ke.y;
         npx = jclip(npx, -pclip, pclip);
         npy = jclip(npy, -pclip, pclip);
         if (!ae) {
-            nvx = ve.x;
-            nvy = ve.y;
-            npx = pe.x;
-            npy = pe.y;
+            nvx = ke.z;
+            nvy = ke.w;
+            npx = ke.x;
+            npy = ke.y;
             nav = av;
             nrot = rot;
         }
-        st2(pout, e, npx, npy);
-        st2(vout, e, nvx, nvy);
+        if (last) {
+            st2(F.dst.pos, e, npx, npy);
+            st2(F.dst.vel, e, nvx, nvy);
+        } else {
+            T* ko = kout + 4 * (size_t)e;
+            typename vec4_of<T>::type v4;
+            v4.x = npx;
+            v4.y = npy;
+            v4.z = nvx;
+            v4.w = nvy;
+            reinterpret_cast<typename vec4_of<T>::type*>(ko)[0] = v4;
+        }
         rout[e] = nrot;
         aout[e] = nav;
-        // displacement since the last neighbour-list build
-        T ddx = npx - a.pos_ref[2 * e], ddy = npy - a.pos_ref[2 * e + 1];
-        float d2 = (float)((double)ddx * ddx + (double)ddy * ddy);
-        if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
-        dmax2 = fmaxf(dmax2, d2);
+        if (check_escape && escaped(a, e, npx, npy)) {
+            a.esc[e] = 1;
+            ++nesc;
+        }
     }
-    // CTA max, one atomic per CTA
-    __shared__ float shm[kThreads / 32];
-    for (int off = 16; off > 0; off >>= 1) dmax2 = fmaxf(dmax2, __shfl_xor_sync(0xffffffffu, dmax2, off));
-    if ((threadIdx.x & 31) == 0) shm[threadIdx.x >> 5] = dmax2;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float m = shm[0];
-        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, shm[i]);
-        if (m > 0.0f) atomicMax(gdisp_slot, f2ord(m));
-    }
-    __syncthreads();
+    if (check_escape) cta_count_add(&a.esc_cnt[s + 1], nesc);
 }
 
 // ─── bond damage (jax_bond_fracture.py:133-208) ─────────────────────────────
@@ -992,7 +1204,9 @@ __device__ void bond_damage(const DemParams& P, T delta_n, T delta_s, T sigma_n,
     T g_II = g_ratio / (T(1) + g_ratio + T(1e-10));
     T g_tot = g_I + g_II + T(1e-10);
     T ratio = g_II / g_tot;
-    T g_c = T(P.bond_G_c_I) + T(P.bond_G_c_II - P.bond_G_c_I) * jpow(ratio, T(P.bond_eta_bk));
+    const T dG = T(P.bond_G_c_II - P.bond_G_c_I);
+    // (G_c^II - G_c^I) * ratio^eta with ratio in [0, 1]: exactly 0 when the energies are equal
+    T g_c = T(P.bond_G_c_I) + ((dG != T(0)) ? dG * jpow(ratio, T(P.bond_eta_bk)) : dG * T(0));
     T snc = jclip(sigma_n, -SC, SC), stc = jclip(sigma_t, -SC, SC);
     T snp = jmax(snc, T(0));
     T sm0_raw = jsqrt(jclip(snp * snp + stc * stc + T(1e-20), T(0), T(1e24)));
@@ -1014,6 +1228,17 @@ __device__ void bond_damage(const DemParams& P, T delta_n, T delta_s, T sigma_n,
     nint = intact && (nd < T(1));
 }
 
+// DPDEM floe eligibility after this frame's contact (jax_simulation.py:511-524):
+// max(force * scale) == max(force) * scale because rounding is monotone.
+template <typename T>
+__device__ __forceinline__ bool new_elig(const KArgs<T>& a, const Frame<T>& F, int fl, T scale) {
+    if (F.elig_in[fl]) return true;
+    if (a.nb == 0 || !a.fcoll[fl]) return false;
+    const unsigned long long bits = a.fmax[fl];
+    const T fmx = (sizeof(T) == 4) ? T(__uint_as_float((unsigned)bits)) : T(__longlong_as_double((long long)bits));
+    return fmx * scale > a.min_bstr * T(a.P.effective_strength_collision);
+}
+
 // ─── P_FRACTURE (jax_simulation.py:534-653) + history ───────────────────────
 template <typename T>
 __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
@@ -1032,7 +1257,7 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
         T dsafe = jmax(dist, T(1e-10));
         T bx = dx / dsafe, by = dy / dsafe;
         bool both_act = F.dst.active[i] && F.dst.active[j];
-        bool floe_ok = F.dst.elig[a.floe_of[i]] && F.dst.elig[a.floe_of[j]];
+        bool floe_ok = new_elig(a, F, a.floe_of[i], scale) && new_elig(a, F, a.floe_of[j], scale);
         bool breakable = (a.thick[i] <= mft) && (a.thick[j] <= mft);
         T fmi = a.fraw[i] * scale, fmj = a.fraw[j] * scale;
         bool near = (fmi > T(0)) || (fmj > T(0));
@@ -1053,17 +1278,19 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
         T sn = (kn * (dn_d / L0)) * (T(1) - cur_d);
         T st = (ks * (new_ds / L0)) * (T(1) - cur_d);
         bool intact = F.src.intact[b] != 0;
-        T nd, nmax, n0;
-        bool nint;
-        bond_damage<T>(P, delta_n, new_ds, sn, st, a.sbar[b], cur_d, F.src.dmmax[b], F.src.dm0[b], intact,
-                       nd, nmax, n0, nint);
         T od = cur_d, omax = F.src.dmmax[b], o0 = F.src.dm0[b];
+        bool fin = intact;
         if (dpdem_ok) {
+            // the damage law's result is only selected for DPDEM-eligible bonds
+            // (jnp.where at jax_simulation.py:620-623); elsewhere the old state stays
+            T nd, nmax, n0;
+            bool nint;
+            bond_damage<T>(P, delta_n, new_ds, sn, st, a.sbar[b], cur_d, omax, o0, intact, nd, nmax, n0, nint);
             od = nd;
             omax = nmax;
             o0 = n0;
+            if (breakable) fin = nint;
         }
-        bool fin = (dpdem_ok && breakable) ? nint : intact;
         // direct collision breaking (jax_simulation.py:629-637)
         bool coll_on = (fmi > T(0)) || (fmj > T(0));
         T coll_f = jmax(fmi, fmj);
@@ -1084,99 +1311,92 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
         if (a.h_rot) a.h_rot[(size_t)F.f * a.n + e] = F.dst.rot[e];
         if (a.h_sub) a.h_sub[(size_t)F.f * a.n + e] = F.dst.sub[e];
     }
-    // per-frame scratch for the next frame
-    for (int fl = gtid; fl < a.nf; fl += gsz) {
-        a.fcoll[fl] = 0;
-        a.fmax[fl] = 0ull;
-    }
-    for (int i = gtid; i < a.k_sub + 2; i += gsz) a.gdisp[i] = 0u;
+    for (int fl = gtid; fl < a.nf; fl += gsz) F.dst.elig[fl] = new_elig(a, F, fl, scale) ? 1 : 0;
+    if (a.d_fmag)
+        for (int e = gtid; e < a.n; e += gsz) a.d_fmag[e] = a.fraw[e] * scale;
+    for (int i = gtid; i < a.k_sub + 2; i += gsz) a.esc_cnt[i] = 0u;
 }
 
 // ─── the kernel ─────────────────────────────────────────────────────────────
-// Phase numbering inside a frame: 0 contact, 1 reduce, then for substep s:
-// 2+3s insert, 3+3s neighbour build, 4+3s force; last: 2+3k fracture.
+// Phase numbering inside a frame: 0 cull, 1 near-element contact, 2 contact
+// forces, 3 reduce + vessel, then for substep s: 4+4s re-reference, 5+4s mark,
+// 6+4s list build, 7+4s force; last: 4+4k fracture.  The three list phases run
+// only when elements escaped (esc_cnt[s] > 0), a decision every CTA takes from
+// the same word after a barrier.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) dem_frames_kernel(KArgs<T> a, int ph_lo, int ph_hi) {
+__global__ void __launch_bounds__(kThreads, 2) dem_frames_kernel(KArgs<T> a, int ph_lo, int ph_hi) {
     extern __shared__ unsigned char smem_raw[];
     T* hullw = reinterpret_cast<T*>(smem_raw);
     const int k = a.k_sub;
-    const int per_frame = 3 + 3 * k;
+    const int per_frame = 5 + 4 * k;
     const bool persistent = (a.mode == DEM_LAUNCH_PERSISTENT);
-    // persistent-mode state (uniform across CTAs)
-    bool dirty = false;
-    bool need_rebuild = false;
+    if (persistent && a.ptimes && blockIdx.x == 0 && threadIdx.x == 0) a.ptimes[1] = globaltimer_ns();
     for (int ph = ph_lo; ph < ph_hi; ++ph) {
         const int f = ph / per_frame;
         const int p = ph % per_frame;
         Frame<T> F = make_frame(a, f);
         if (p == 0) {
-            phase_contact(a, F, hullw);
-            dirty = true;
+            phase_cull(a, F);
         } else if (p == 1) {
-            T sc;
-            phase_reduce(a, F, &sc);
+            phase_near(a, F, hullw);
+        } else if (p == 2) {
+            phase_cforce(a, F);
+        } else if (p == 3) {
+            phase_reduce(a, F);
         } else if (p == per_frame - 1) {
-            // recompute the frame's thrust scale (phased launches keep no state)
-            __shared__ double tot3[3];
-            double r[3];
-            frame_totals(a, r);
-            if (threadIdx.x == 0) {
-                tot3[0] = r[0];
-                tot3[1] = r[1];
-                tot3[2] = r[2];
-            }
-            __syncthreads();
-            T sc = thrust_scale_of(a, tot3);
-            phase_fracture(a, F, sc);
+            phase_fracture(a, F, T(*((volatile double*)&a.fscal[0])));
         } else {
-            const int s = (p - 2) / 3;
-            const int sub = (p - 2) % 3;
-            if (sub == 0 || sub == 1) {
-                // neighbour-list rebuild before substep s (s >= 1 only: frame start built in P0/P1)
-                bool run;
-                if (persistent) {
-                    run = (s >= 1) && need_rebuild;
-                } else {
-                    run = (s >= 1);
-                }
-                if (!run) continue;  // uniform across CTAs: no barrier for skipped phases
+            const int s = (p - 4) / 4;
+            const int sub = (p - 4) % 4;
+            const unsigned cnt = *((volatile unsigned*)&a.esc_cnt[s]);
+            if (sub < 3) {
+                const bool all = (unsigned long long)cnt * 8ull > (unsigned long long)a.n;
+                if (cnt == 0u || (sub == 1 && all)) continue;  // uniform: no barrier either
                 if (sub == 0) {
-                    const T* pos = a.sp_pos[(s - 1) & 1];
-                    phase_insert(a, pos);
-                    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&a.stats[0], 1ull);
+                    phase_reref(a, a.kin[s & 1]);
+                } else if (sub == 1) {
+                    phase_mark(a);
                 } else {
-                    phase_nbr(a);
-                    dirty = true;
+                    phase_build(a, all);
                 }
             } else {
-                bool clear = persistent ? dirty : true;
-                // substep s owns slot s: it is written only in this phase and read only
-                // after the following barrier, so every CTA reads the same value
-                phase_force(a, F, s, clear, &a.gdisp[s]);
-                dirty = false;
+                if (cnt != 0u) compact_buckets(a);  // nothing reads the grid in this phase
+                phase_force(a, F, s);
             }
         }
         if (persistent && ph + 1 < ph_hi) {
             if (!grid_barrier(a)) return;
-            // decide on a rebuild after each force phase (all CTAs read the same word)
-            if (p >= 2 && p < per_frame - 1 && ((p - 2) % 3) == 2) {
-                unsigned bits = *((volatile unsigned*)&a.gdisp[(p - 2) / 3]);
-                float d2 = __uint_as_float(bits);
-                double lim = 0.45 * (double)a.skin;
-                need_rebuild = !(a.skin > T(0)) || !((double)d2 < lim * lim);
+            if (a.ptimes && blockIdx.x == 0 && threadIdx.x == 0) {
+                // phase end times (debug/profiling): entry i = [phase, globaltimer]
+                const unsigned long long i = atomicAdd(a.ptimes, 1ull);
+                if (i < (unsigned long long)kMaxPhaseTimes) {
+                    a.ptimes[2 + 2 * i] = (unsigned long long)ph;
+                    a.ptimes[3 + 2 * i] = globaltimer_ns();
+                }
             }
         }
     }
 }
 
-// bond stiffness E * ((h_i + h_j) * 0.5) * factor, in the dtype (jax_simulation.py:81-82)
+// r^3 per element in the dtype (radii ** 3, jax_simulation.py:205)
 template <typename T>
-__global__ void bond_stiffness_kernel(const T* thick, const int* bi, const int* bj, int nb, double E,
-                                      double factor, T* out) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+__global__ void cube_kernel(const T* r, int n, T* out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) out[e] = jpow(r[e], T(3));
+}
+
+// per-slot bond constants: rest length and E * ((h_i + h_j) * 0.5) * factor in
+// the dtype (jax_simulation.py:81-82)
+template <typename T>
+__global__ void slot_setup_kernel(const T* thick, const T* rest, const int* bi, const int* bj,
+                                  const int2* slots, int n_slots, double E, double factor, T* slot_rest,
+                                  T* slot_stiff) {
+    int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= n_slots) return;
+    int b = slots[sl].x & 0x7fffffff;
     T avg = (thick[bi[b]] + thick[bj[b]]) * T(0.5);
-    out[b] = T(E) * avg * T(factor);
+    slot_stiff[sl] = T(E) * avg * T(factor);
+    slot_rest[sl] = rest[b];
 }
 
 }  // namespace dem

@@ -213,6 +213,18 @@ class FrameStep:
         self._check(self.lib.dem_get_info(self._h, C.byref(inf)))
         return {k: getattr(inf, k) for k, _ in _abi.DemInfo._fields_}
 
+    def set_profiling(self, on: bool = True):
+        """Record device time stamps at every phase end of persistent launches."""
+        self._check(self.lib.dem_set_profiling(self._h, 1 if on else 0))
+
+    def phase_times(self):
+        """[(phase index, ns since launch start)] of the last profiled persistent call."""
+        buf = (C.c_int64 * (2 * 4096))()
+        cnt = C.c_int32()
+        t0 = C.c_int64()
+        self._check(self.lib.dem_get_phase_times(self._h, buf, 4096, C.byref(cnt), C.byref(t0)))
+        return [(int(buf[2 * i]), int(buf[2 * i + 1]) - int(t0.value)) for i in range(cnt.value)]
+
     def close(self):
         if getattr(self, "_h", None):
             self.lib.dem_destroy(self._h)
