@@ -171,6 +171,9 @@ typedef struct DemInfo {
     int32_t max_bucket_count;   /* fullest grid bucket seen since create            */
     int32_t hash_buckets;
     double cell_size;
+    int64_t escaped_total;       /* elements re-referenced since create             */
+    int64_t rebuilt_lists_total; /* neighbour lists rebuilt since create            */
+    int32_t capacity_flags;      /* last DEM_ERR_CAPACITY: 1 grid bucket, 2 neighbour list, 3 both */
 } DemInfo;
 
 /* Replaces _make_frame_step (jax_simulation.py:302-361): binds static data and
@@ -212,8 +215,10 @@ int dem_set_profiling(DemHandle* h, int32_t on);
 
 /* Phase end times of the last persistent call: pairs [phase index, ns] (at most
  * max_pairs), their count, and the launch's start time in ns (globaltimer).
- * Phase indices count 5 + 4 k per frame: cull, near contact, contact forces,
- * reduce, then per substep re-reference, mark, list build, force, and fracture. */
+ * Phase indices count 5 + 3 k per frame: cull, near contact, contact forces,
+ * reduce, then per substep escape round, all-lists rebuild and force, and
+ * fracture.  Phases skipped on the device (no escapes, no full rebuild) record
+ * no entry. */
 int dem_get_phase_times(DemHandle* h, int64_t* pairs, int32_t max_pairs, int32_t* count, int64_t* start_ns);
 
 /* Copy the last error message (NUL-terminated) into buf. */

@@ -95,7 +95,8 @@ class DemHistory(C.Structure):
 class DemInfo(C.Structure):
     _fields_ = [("grid_blocks", _i), ("threads_per_block", _i), ("neighbor_rebuilds", C.c_int64),
                 ("max_neighbor_count", _i), ("max_bucket_count", _i), ("hash_buckets", _i),
-                ("cell_size", _d)]
+                ("cell_size", _d), ("escaped_total", C.c_int64), ("rebuilt_lists_total", C.c_int64),
+                ("capacity_flags", _i)]
 
 
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
@@ -105,11 +106,15 @@ EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status"
 _LIB = None
 
 
-def load_library(path: str = LIB_PATH):
-    """Load libdem_b200.so (built by ``build.build_library``); raise if absent."""
+def load_library(path: str = None):
+    """Load libdem_b200.so (built by ``build.build_library``); raise if absent.
+
+    ``DEM_B200_LIB`` may name another build of the same library (for tuning runs).
+    """
     global _LIB
     if _LIB is not None:
         return _LIB
+    path = path or os.environ.get("DEM_B200_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise ImportError(f"{path} is missing: build it with `python mbd-icenav_b200/build.py` "
                           "(there is no CPU fallback for the DEM frame step)")

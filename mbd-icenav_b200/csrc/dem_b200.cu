@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -47,8 +48,16 @@ struct DemHandle {
     int* ncnt = nullptr;
     int* nbr = nullptr;
     void* pos_ref = nullptr;
-    uint8_t* esc = nullptr;
-    uint8_t* dirty = nullptr;
+    unsigned* dirty = nullptr;
+    int capacity_flags = 0;   // what overflowed at the last DEM_ERR_CAPACITY (1 bucket, 2 list)
+    unsigned round_base = 0;  // dirty stamps issued so far (since the last clear)
+    int* bflag = nullptr;
+    int* comp_list = nullptr;
+    int* comp_cnt = nullptr;
+    int* esc_list = nullptr;
+    int* dirty_list = nullptr;
+    int* dirty_cnt = nullptr;
+    int* slot_owner = nullptr;
     unsigned* esc_cnt = nullptr;
     int* near_list = nullptr;
     int* near_cnt = nullptr;
@@ -62,6 +71,7 @@ struct DemHandle {
     unsigned long long* fmax = nullptr;
     double* part = nullptr;
     void* kin[2] = {nullptr, nullptr};
+    void* kvel[2] = {nullptr, nullptr};
     void* sp_rot[2] = {nullptr, nullptr};
     void* sp_avel[2] = {nullptr, nullptr};
     // frame ping-pong state for scans
@@ -180,9 +190,11 @@ int alloc_neighbors(DemHandle* h) {
 // next call rebuilds every list (after a capacity change or a device error).
 int reset_broad_phase(DemHandle* h, cudaStream_t st) {
     CUDA_TRY(h, cudaMemsetAsync(h->bcnt, 0, sizeof(int) * (size_t)h->n_buckets, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->bitems, 0xFF, sizeof(int) * (size_t)h->n_buckets * h->P.bucket_capacity, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->comp_cnt, 0, sizeof(int), st));
     CUDA_TRY(h, cudaMemsetAsync(h->pos_ref, 0xFF, h->esz * 2 * (size_t)h->n, st));
-    CUDA_TRY(h, cudaMemsetAsync(h->esc, 0, (size_t)h->n, st));
-    CUDA_TRY(h, cudaMemsetAsync(h->dirty, 0, (size_t)h->n, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->dirty, 0, sizeof(unsigned) * (size_t)h->n, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->bflag, 0, sizeof(int) * (size_t)h->n_buckets, st));
     CUDA_TRY(h, cudaMemsetAsync(h->ncnt, 0, sizeof(int) * (size_t)h->n, st));
     return DEM_OK;
 }
@@ -299,8 +311,14 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.ncnt = h->ncnt;
     a.nbr = h->nbr;
     a.pos_ref = (T*)h->pos_ref;
-    a.esc = h->esc;
     a.dirty = h->dirty;
+    a.bflag = h->bflag;
+    a.comp_list = h->comp_list;
+    a.comp_cnt = h->comp_cnt;
+    a.esc_list = h->esc_list;
+    a.dirty_list = h->dirty_list;
+    a.dirty_cnt = h->dirty_cnt;
+    a.slot_owner = h->slot_owner;
     a.esc_cnt = h->esc_cnt;
     a.soi = (T*)h->soi;
     a.fraw = (T*)h->fraw;
@@ -310,6 +328,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.part = h->part;
     for (int i = 0; i < 2; ++i) {
         a.kin[i] = (T*)h->kin[i];
+        a.kvel[i] = (T*)h->kvel[i];
         a.sp_rot[i] = (T*)h->sp_rot[i];
         a.sp_avel[i] = (T*)h->sp_avel[i];
     }
@@ -369,12 +388,24 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     CUDA_TRY(h, cudaMemsetAsync(h->fcoll, 0, sizeof(int) * std::max(h->nf, 1), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->fmax, 0, sizeof(unsigned long long) * std::max(h->nf, 1), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->esc_cnt, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->dirty_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
+    {
+        // every rebuild round of every call gets its own dirty stamp; clear the
+        // stamps before the counter would wrap
+        const unsigned need = (unsigned)K * (unsigned)h->P.n_ice_steps + 1u;
+        if (h->round_base > 0xFFFFFFFFu - need) {
+            CUDA_TRY(h, cudaMemsetAsync(h->dirty, 0, sizeof(unsigned) * (size_t)h->n, stream));
+            h->round_base = 0;
+        }
+        a.round_base = h->round_base;
+        h->round_base += need;
+    }
     CUDA_TRY(h, cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * 2, stream));
     CUDA_TRY(h, cudaMemsetAsync(h->near_cnt, 0, sizeof(int), stream));
     if (h->profiling) CUDA_TRY(h, cudaMemsetAsync(h->ptimes, 0, sizeof(unsigned long long) * 2, stream));
 
     const int k = h->P.n_ice_steps;
-    const int per_frame = 5 + 4 * k;
+    const int per_frame = dem::phases_per_frame(k);
     if (h->mode == DEM_LAUNCH_PERSISTENT) {
         int lo = 0, hi = K * per_frame;
         void* args[] = {(void*)&a, (void*)&lo, (void*)&hi};
@@ -478,7 +509,9 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
             vr[e] = std::max(vr[e], std::sqrt(x * x + y * y));
         }
     for (int e = 0; e < n; ++e) vr[e] = vr[e] * (1.0 + 1e-5) + 1e-4;  // conservative (rounded up)
-    h->hull_r = 0.0;
+    // reach of the ship: its outline points (pass 2) and the corners of the
+    // analytic hull box |x| <= half_len, |y| <= half_beam (pass 1)
+    h->hull_r = std::hypot(h->P.half_len, h->P.half_beam);
     for (int i = 0; i < h->nh; ++i) h->hull_r = std::max(h->hull_r, std::hypot(hull[2 * i], hull[2 * i + 1]));
     h->hull_r = h->hull_r * (1.0 + 1e-5) + 1e-4;
     h->k_n = s->k_n;
@@ -527,8 +560,14 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->ncnt, sizeof(int) * n))) return fail(rc);
     if ((rc = alloc_neighbors(h))) return fail(rc);
     if ((rc = dev_alloc(h, &h->pos_ref, es * 2 * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->esc, n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->dirty, n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->dirty, sizeof(unsigned) * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bflag, sizeof(int) * (size_t)h->n_buckets))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->comp_list, sizeof(int) * (size_t)h->n_buckets))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->comp_cnt, sizeof(int)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->esc_list, sizeof(int) * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->dirty_list, sizeof(int) * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->dirty_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->esc_cnt, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fraw, es * n))) return fail(rc);
@@ -538,6 +577,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->part, sizeof(double) * 3 * ((n + dem::kThreads - 1) / dem::kThreads)))) return fail(rc);
     for (int i = 0; i < 2; ++i) {
         if ((rc = dev_alloc(h, &h->kin[i], es * 4 * n))) return fail(rc);
+        if ((rc = dev_alloc(h, &h->kvel[i], es * 2 * n))) return fail(rc);
         if ((rc = dev_alloc(h, &h->sp_rot[i], es * n))) return fail(rc);
         if ((rc = dev_alloc(h, &h->sp_avel[i], es * n))) return fail(rc);
     }
@@ -561,7 +601,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->sprow, es * 6))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bar, sizeof(unsigned) * 2))) return fail(rc);
     if ((rc = dev_alloc(h, &h->status, sizeof(int)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->stats, sizeof(long long) * 4))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->stats, sizeof(long long) * 8))) return fail(rc);
     ce = cudaMallocHost(&h->host_status, sizeof(int));
     if (ce != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "cudaMallocHost: %s", cudaGetErrorString(ce)));
 
@@ -572,6 +612,12 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     } while (0)
     CREATE_TRY(cudaMemcpy(h->boff, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     CREATE_TRY(cudaMemcpy(h->bslot, slots.data(), sizeof(int2) * slots.size(), cudaMemcpyHostToDevice));
+    {
+        std::vector<int> owner(slots.size(), 0);
+        for (int e = 0; e < n; ++e)
+            for (int sl = off[e]; sl < off[e + 1]; ++sl) owner[sl] = e;
+        CREATE_TRY(cudaMemcpy(h->slot_owner, owner.data(), sizeof(int) * owner.size(), cudaMemcpyHostToDevice));
+    }
     if (h->dtype == DEM_F32) {
         std::vector<float> v(n);
         for (int e = 0; e < n; ++e) v[e] = std::nextafter((float)vr[e], INFINITY);
@@ -581,7 +627,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     }
     if ((rc = reset_broad_phase(h, 0))) return fail(rc);
     CREATE_TRY(cudaMemset(h->status, 0, sizeof(int)));
-    CREATE_TRY(cudaMemset(h->stats, 0, sizeof(long long) * 4));
+    CREATE_TRY(cudaMemset(h->stats, 0, sizeof(long long) * 8));
     CREATE_TRY(cudaMemset(h->bar, 0, sizeof(unsigned) * 2));
     if (nb) {
         int n_slots = 2 * nb;
@@ -651,6 +697,8 @@ int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out, cons
     if (!h) return DEM_ERR_INVALID;
     int rc;
     if (K < 1) return set_err(h, DEM_ERR_INVALID, "K must be >= 1");
+    if ((long long)K * dem::phases_per_frame(h->P.n_ice_steps) > (long long)INT_MAX / 2)
+        return set_err(h, DEM_ERR_INVALID, "K = %d frames is too many for one call", (int)K);
     if ((rc = check_state(h, in, "input"))) return rc;
     if ((rc = check_state(h, out, "output"))) return rc;
     if ((rc = check_ship(h, ship_in, "input"))) return rc;
@@ -680,9 +728,15 @@ int dem_sync_status(DemHandle* h, void* stream) {
         int rc = reset_broad_phase(h, st);
         if (rc) return rc;
         CUDA_TRY(h, cudaStreamSynchronize(st));
-        if (v == DEM_ERR_CAPACITY)
-            return set_err(h, DEM_ERR_CAPACITY, "neighbour or grid-bucket capacity exceeded (max_neighbors=%d, bucket_capacity=%d)",
-                           h->P.max_neighbors, h->P.bucket_capacity);
+        if (v == DEM_ERR_CAPACITY) {
+            long long flags = 0;
+            CUDA_TRY(h, cudaMemcpy(&flags, h->stats + 5, sizeof(flags), cudaMemcpyDeviceToHost));
+            CUDA_TRY(h, cudaMemset(h->stats + 5, 0, sizeof(flags)));
+            h->capacity_flags = (int)flags;
+            return set_err(h, DEM_ERR_CAPACITY, "%s%s%s capacity exceeded (max_neighbors=%d, bucket_capacity=%d)",
+                           (flags & 2) ? "neighbour-list" : "", (flags & 3) == 3 ? " and " : "",
+                           (flags & 1) ? "grid-bucket" : "", h->P.max_neighbors, h->P.bucket_capacity);
+        }
         if (v == DEM_ERR_TIMEOUT) return set_err(h, DEM_ERR_TIMEOUT, "grid barrier wait exceeded its limit");
         return set_err(h, v, "device status %d", v);
     }
@@ -716,7 +770,7 @@ int dem_set_launch_mode(DemHandle* h, int32_t mode) {
 int dem_get_info(DemHandle* h, DemInfo* info) {
     if (!h || !info) return DEM_ERR_INVALID;
     CUDA_TRY(h, cudaSetDevice(h->device));
-    long long st[4] = {0, 0, 0, 0};
+    long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     CUDA_TRY(h, cudaMemcpy(st, h->stats, sizeof(st), cudaMemcpyDeviceToHost));
     info->grid_blocks = h->grid_blocks;
     info->threads_per_block = dem::kThreads;
@@ -725,6 +779,9 @@ int dem_get_info(DemHandle* h, DemInfo* info) {
     info->max_bucket_count = (int)st[2];
     info->hash_buckets = h->n_buckets;
     info->cell_size = 2.0 * h->r_max + h->P.skin;
+    info->escaped_total = st[3];
+    info->rebuilt_lists_total = st[4];
+    info->capacity_flags = h->capacity_flags;
     return DEM_OK;
 }
 

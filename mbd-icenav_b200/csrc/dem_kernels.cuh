@@ -40,6 +40,13 @@ constexpr int kMaxEdgeSamples = 16;
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s per barrier wait
 constexpr int kMaxPhaseTimes = 4096;
 
+// Phases of one frame: cull, near contact, contact forces, reduce, then per
+// substep escape round, all-lists rebuild and force, and last fracture.
+__host__ __device__ constexpr int phases_per_frame(int k_sub) { return 5 + 3 * k_sub; }
+#ifndef DEM_MIN_BLOCKS
+#define DEM_MIN_BLOCKS 2  // resident CTAs per SM the register allocation targets
+#endif
+
 // Per-frame record of one bond slot (see phase_reduce): partner index with the
 // slot's role in the sign bit, rest length, stiffness E*mean(h)*factor, and
 // (1 - damage), or -1 when the bond adds no force this frame (broken, or its
@@ -92,8 +99,10 @@ struct KArgs {
     int* ncnt;          // (n) neighbour count
     int* nbr;           // (max_nb * n) neighbour lists, slot-major
     T* pos_ref;         // (n,2) reference positions (NaN before the first build)
-    uint8_t* esc;       // (n) moved more than 0.45 skin from its reference
-    uint8_t* dirty;     // (n) neighbour list must be rebuilt
+    unsigned* dirty;    // (n) stamp of the round whose list rebuild the element needs
+    int* bflag;         // (n_buckets) bucket queued for compaction
+    int* comp_list;     // (n_buckets) buckets to compact at the next frame start
+    int* comp_cnt;      // (1) queued buckets
     unsigned* esc_cnt;  // (k_sub + 2) escaped elements found before substep s
     // per-frame scratch
     int* near_list;     // (n) elements whose bounding circle reaches the hull
@@ -105,7 +114,13 @@ struct KArgs {
     int* fcoll;         // (nf) floe touched by the ship this frame
     unsigned long long* fmax;  // (nf) max force magnitude per floe (ordered bits)
     double* part;       // (nchunks * 3) per-chunk sums: soi_x, soi_y, moment
-    T* kin[2];          // (n,4) {x, y, vx, vy} of the substep being read / written
+    T* kin[2];          // (n,4) {x, y, radius, 0} of the substep being read / written
+    T* kvel[2];         // (n,2) {vx, vy} of the substep being read / written
+    int* esc_list;      // (n) escaped elements of the current detection
+    int* dirty_list;    // (n) elements whose list is rebuilt
+    int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
+    unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
+    const int* slot_owner;  // (2 nb) element that owns each bond slot
     T *sp_rot[2], *sp_avel[2];  // substep ping-pong of own-element angles
     void* slotrec;      // (2 nb) SlotRec<T>: per-frame bond slot records
     const T* r3;        // (n) radius^3 (dtype pow, once at create)
@@ -123,8 +138,17 @@ struct KArgs {
     uint8_t* h_intact;
     unsigned* bar;        // [count, generation]
     int* status;
-    long long* stats;     // [rebuilds, max_nb_count, max_bucket_count]
+    long long* stats;     // [rounds, max list, max bucket, re-referenced, lists rebuilt, overflow flags]
 };
+
+template <typename T> struct vec4_of;
+template <> struct vec4_of<float> { typedef float4 type; };
+template <> struct vec4_of<double> { typedef double4 type; };
+
+template <typename T>
+__device__ __forceinline__ typename vec4_of<T>::type ld4(const T* p, int i) {
+    return reinterpret_cast<const typename vec4_of<T>::type*>(p)[i];
+}
 
 // ─── per-frame pointer bundle ───────────────────────────────────────────────
 template <typename T>
@@ -256,151 +280,214 @@ __device__ __forceinline__ void grid_put(const KArgs<T>& a, int e, T px, T py) {
         a.bitems[(size_t)b * a.bucket_cap + slot] = e;
     } else {
         atomicMax(a.status, DEM_ERR_CAPACITY);
+        atomicOr((unsigned long long*)&a.stats[5], 1ull);  // a grid bucket overflowed
     }
     if (slot + 1 > a.bucket_cap / 2) atomicMax((unsigned long long*)&a.stats[2], (unsigned long long)(slot + 1));
 }
 
-// Visit every element o != e whose reference lies within r_e + r_o + skin of
-// ref_e (a conservative superset: the test is done in double with a margin).
-// An element can sit twice in one bucket (a stale and a current entry when its
-// old and new cells hash together); callers that collect must deduplicate.
+// Warp-cooperative neighbourhood scan: the 9 stencil buckets' entries are
+// spread over the lanes; `fn(o)` runs on the lane that found o.  Every element
+// within r_e + r_o + skin of ref_e (double test with a margin) is visited; an
+// element can be visited twice (stale + current entry in one bucket).
 template <typename T, typename Fn>
-__device__ __forceinline__ void for_each_near(const KArgs<T>& a, int e, Fn fn) {
-    int2 c = a.ecell[e];
+__device__ __forceinline__ void warp_near_at(const KArgs<T>& a, int e, T px, T py, int2 c, Fn fn) {
+    const int lane = threadIdx.x & 31;
     if (c.x == INT_MIN) return;
-    const T px = a.pos_ref[2 * e], py = a.pos_ref[2 * e + 1];
     const double re = (double)a.radii[e] + (double)a.skin;
-    for (int dy = -1; dy <= 1; ++dy) {
-        for (int dx = -1; dx <= 1; ++dx) {
-            int2 cc = make_int2(c.x + dx, c.y + dy);
-            int b = bucket_of(cc, a.n_buckets);
-            int m = min(a.bcnt[b], a.bucket_cap);
-            const int* it = a.bitems + (size_t)b * a.bucket_cap;
-            for (int k0 = 0; k0 < m; k0 += 2) {
-                int ob[2];
-                int2 oc[2];
-                T ox[2], oy[2], orr[2];
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    ob[j] = (k0 + j < m) ? it[k0 + j] : -1;
-                    if (ob[j] >= 0) {
-                        oc[j] = a.ecell[ob[j]];
-                        ox[j] = a.pos_ref[2 * ob[j]];
-                        oy[j] = a.pos_ref[2 * ob[j] + 1];
-                        orr[j] = a.radii[ob[j]];
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    int o = ob[j];
-                    if (o < 0 || o == e) continue;
-                    if (oc[j].x != cc.x || oc[j].y != cc.y) continue;  // stale entry or hash collision
-                    double ddx = (double)ox[j] - (double)px, ddy = (double)oy[j] - (double)py;
-                    double lim = (re + (double)orr[j]) * (1.0 + 1e-5) + 1e-6;
-                    if (ddx * ddx + ddy * ddy < lim * lim) fn(o);
-                }
+    // lanes 0..8 own one stencil bucket each; warp prefix of their fills
+    int b = 0, m = 0;
+    if (lane < 9) {
+        const int2 cc = make_int2(c.x + (lane % 3) - 1, c.y + (lane / 3) - 1);
+        b = bucket_of(cc, a.n_buckets);
+        m = min(a.bcnt[b], a.bucket_cap);
+    }
+    int incl = m;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - m;
+    // uniform trip count: every lane executes every shuffle
+    for (int t0 = 0; t0 < total; t0 += 32) {
+        const int t = t0 + lane;
+        // bucket j holding entry t: the last stencil lane whose prefix start <= t
+        int q = 0, qb = 0, qe = 0;
+        for (int j = 0; j < 9; ++j) {
+            const int ej = __shfl_sync(0xffffffffu, excl, j);
+            const int bj = __shfl_sync(0xffffffffu, b, j);
+            if (t >= ej) {
+                q = j;
+                qb = bj;
+                qe = ej;
             }
         }
+        if (t >= total) continue;
+        // entries are written after their slot is claimed: a concurrent insertion
+        // can show an old value (-1 or a valid stale index), never an invalid one
+        const int o = ((volatile const int*)a.bitems)[(size_t)qb * a.bucket_cap + (t - qe)];
+        if (o < 0 || o >= a.n || o == e) continue;
+        const int2 cc = make_int2(c.x + (q % 3) - 1, c.y + (q / 3) - 1);
+        const int2 oc = a.ecell[o];
+        if (oc.x != cc.x || oc.y != cc.y) continue;  // stale entry or hash collision
+        const double ddx = (double)a.pos_ref[2 * o] - (double)px, ddy = (double)a.pos_ref[2 * o + 1] - (double)py;
+        const double lim = (re + (double)a.radii[o]) * (1.0 + 1e-5) + 1e-6;
+        if (ddx * ddx + ddy * ddy < lim * lim) fn(o);
     }
 }
 
-// Build element e's list sorted so that indices above e come first (ascending),
-// then indices below e (ascending) — the order in which the reference's
-// scatter-adds reach e: pairs (e, j>e) through pair_i, then pairs (i<e, e)
-// through pair_j (jax_simulation.py:152-162).
+template <typename T, typename Fn>
+__device__ __forceinline__ void warp_near(const KArgs<T>& a, int e, Fn fn) {
+    warp_near_at(a, e, a.pos_ref[2 * e], a.pos_ref[2 * e + 1], a.ecell[e], fn);
+}
+
+// Append `flag`-set lanes' values to list[atomicAdd(cnt)] with one atomic per warp.
+__device__ __forceinline__ void warp_append(int* list, int* cnt, bool flag, int v) {
+    const unsigned am = __activemask();
+    const unsigned bal = __ballot_sync(am, flag);
+    if (!bal) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(am) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(cnt, __popc(bal));
+    base = __shfl_sync(am, base, leader);
+    if (flag) list[base + __popc(bal & ((1u << lane) - 1u))] = v;
+}
+
+// Build element e's list (one warp): candidates are gathered in shared memory,
+// sorted and deduplicated, then stored so that indices above e come first
+// (ascending), then indices below e (ascending) — the order in which the
+// reference's scatter-adds reach e: pairs (e, j>e) through pair_i, then pairs
+// (i<e, e) through pair_j (jax_simulation.py:152-162).
 template <typename T>
-__device__ void build_neighbors(const KArgs<T>& a, int e) {
-    int cnt = 0;
-    int loc[kMaxNbLocal];
-    const int cap = a.max_nb;
-    for_each_near(a, e, [&](int o) {
-        for (int i = 0; i < min(cnt, cap); ++i)
-            if (loc[i] == o) return;  // duplicate entry of one element
-        if (cnt < cap) loc[cnt] = o;
-        ++cnt;
+__device__ void warp_build(const KArgs<T>& a, int e, int* sbuf, int* scnt) {
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) *scnt = 0;
+    __syncwarp();
+    const int cap = 2 * kMaxNbLocal;
+    warp_near(a, e, [&](int o) {
+        const int slot = atomicAdd(scnt, 1);
+        if (slot < cap) sbuf[slot] = o;
     });
-    if (cnt > cap) atomicMax(a.status, DEM_ERR_CAPACITY);
-    if (cnt > 16) atomicMax((unsigned long long*)&a.stats[1], (unsigned long long)cnt);
-    int m = min(cnt, cap);
-    for (int i = 1; i < m; ++i) {
-        int v = loc[i];
-        int j = i - 1;
-        while (j >= 0 && loc[j] > v) {
-            loc[j + 1] = loc[j];
-            --j;
+    __syncwarp();
+    int cnt = min(*scnt, cap);
+    if (lane == 0) {
+        // sort + dedup (short lists)
+        for (int i = 1; i < cnt; ++i) {
+            const int v = sbuf[i];
+            int j = i - 1;
+            while (j >= 0 && sbuf[j] > v) {
+                sbuf[j + 1] = sbuf[j];
+                --j;
+            }
+            sbuf[j + 1] = v;
         }
-        loc[j + 1] = v;
+        int w = 0;
+        for (int i = 0; i < cnt; ++i)
+            if (w == 0 || sbuf[w - 1] != sbuf[i]) sbuf[w++] = sbuf[i];
+        if (*scnt > cap || w > a.max_nb) {
+            atomicMax(a.status, DEM_ERR_CAPACITY);
+            atomicOr((unsigned long long*)&a.stats[5], 2ull);  // a neighbour list overflowed
+        }
+        if (w > 16) atomicMax((unsigned long long*)&a.stats[1], (unsigned long long)w);
+        *scnt = min(w, a.max_nb);
     }
+    __syncwarp();
+    const int m = *scnt;
     int split = 0;
-    while (split < m && loc[split] < e) ++split;
-    int w = 0;
-    for (int i = split; i < m; ++i) a.nbr[(size_t)(w++) * a.n + e] = loc[i];
-    for (int i = 0; i < split; ++i) a.nbr[(size_t)(w++) * a.n + e] = loc[i];
-    a.ncnt[e] = m;
+    for (int i = 0; i < m; ++i) split += (sbuf[i] < e) ? 1 : 0;
+    for (int i = lane; i < m; i += 32) {
+        const int src = (i < m - split) ? split + i : i - (m - split);
+        a.nbr[(size_t)i * a.n + e] = sbuf[src];
+    }
+    if (lane == 0) a.ncnt[e] = m;
+    __syncwarp();
 }
 
-// R1: escaped elements take their current position as reference and are
-// appended to the bucket of their new home cell.
+// Queue bucket b for compaction at the next frame start.
 template <typename T>
-__device__ void phase_reref(const KArgs<T>& a, const T* kin) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    for (int e = gtid; e < a.n; e += gsz) {
-        if (!a.esc[e]) continue;
+__device__ __forceinline__ void queue_bucket(const KArgs<T>& a, int b) {
+    if (atomicExch(&a.bflag[b], 1) == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = b;
+}
+
+// Stamp o dirty for this round; the first stamper lists it.
+template <typename T>
+__device__ __forceinline__ void mark_dirty(const KArgs<T>& a, int o, int s, unsigned round) {
+    if (atomicExch(&a.dirty[o], round) != round) a.dirty_list[atomicAdd(&a.dirty_cnt[s], 1)] = o;
+}
+
+// One rebuild round before substep s, one warp per escaped element: the
+// element takes its current position as reference and is appended to its new
+// home bucket; it and every element within reach of its new reference need a
+// new list (skipped when most elements escaped: every list is then rebuilt).
+// Runs concurrently with insertions by other warps: marking only needs the
+// references of elements that did not escape, which do not move.
+template <typename T>
+__device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int s, unsigned round, bool all) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int q = warp; q < (int)cnt; q += nwarps) {
+        const int e = a.esc_list[q];
         const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-        a.pos_ref[2 * e] = px;
-        a.pos_ref[2 * e + 1] = py;
-        grid_put(a, e, px, py);
+        if (lane == 0) {
+            const int2 old = a.ecell[e];
+            if (old.x != INT_MIN) queue_bucket(a, bucket_of(old, a.n_buckets));
+            a.pos_ref[2 * e] = px;
+            a.pos_ref[2 * e + 1] = py;
+            grid_put(a, e, px, py);
+            const int2 nw = a.ecell[e];
+            if (nw.x != INT_MIN) queue_bucket(a, bucket_of(nw, a.n_buckets));
+        }
+        if (all) continue;
+        const bool fin = jfinite(px) && jfinite(py);
+        const int2 c = fin ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+        warp_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
+        if (lane == 0) mark_dirty(a, e, s, round);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&a.stats[0], 1ull);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd((unsigned long long*)&a.stats[0], 1ull);
+        atomicAdd((unsigned long long*)&a.stats[3], (unsigned long long)cnt);
+    }
 }
 
-// R2: an escaped element and every element within reach of its new reference
-// need a new list.
+// Rebuild every list (when most elements escaped at once).
 template <typename T>
-__device__ void phase_mark(const KArgs<T>& a) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    for (int e = gtid; e < a.n; e += gsz) {
-        if (!a.esc[e]) continue;
-        a.dirty[e] = 1;
-        for_each_near(a, e, [&](int o) { a.dirty[o] = 1; });
-    }
+__device__ void phase_build_all(const KArgs<T>& a) {
+    __shared__ int sbuf[kThreads / 32][2 * kMaxNbLocal];
+    __shared__ int scnt[kThreads / 32];
+    const int wl = threadIdx.x >> 5;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int e = warp; e < a.n; e += nwarps) warp_build(a, e, sbuf[wl], &scnt[wl]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)a.n);
 }
 
-// R3: rebuild the marked lists (all of them when most elements escaped).
-template <typename T>
-__device__ void phase_build(const KArgs<T>& a, bool all) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    for (int e = gtid; e < a.n; e += gsz) {
-        if (all || a.dirty[e]) build_neighbors(a, e);
-        a.dirty[e] = 0;
-        a.esc[e] = 0;
-    }
-}
-
-// Drop stale and duplicate bucket entries (run while nothing reads the grid).
+// Drop stale and duplicate entries of the queued buckets (run while nothing
+// reads or writes the grid).
 template <typename T>
 __device__ void compact_buckets(const KArgs<T>& a) {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
-    for (int b = gtid; b < a.n_buckets; b += gsz) {
-        int m = a.bcnt[b];
-        if (m == 0) continue;
-        m = min(m, a.bucket_cap);
+    const int nq = *((volatile int*)a.comp_cnt);
+    for (int i = gtid; i < nq; i += gsz) {
+        const int b = a.comp_list[i];
+        const int m = min(a.bcnt[b], a.bucket_cap);
         int* it = a.bitems + (size_t)b * a.bucket_cap;
         int w = 0;
         for (int k = 0; k < m; ++k) {
-            int o = it[k];
-            int2 c = a.ecell[o];
+            const int o = it[k];
+            if (o < 0 || o >= a.n) continue;
+            const int2 c = a.ecell[o];
             if (c.x == INT_MIN || bucket_of(c, a.n_buckets) != b) continue;
             bool dup = false;
             for (int q = 0; q < w; ++q)
                 if (it[q] == o) dup = true;
             if (!dup) it[w++] = o;
         }
+        for (int k = w; k < m; ++k) it[k] = -1;
         a.bcnt[b] = w;
+        a.bflag[b] = 0;
     }
 }
 
@@ -497,12 +584,13 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
     const int gsz = gridDim.x * blockDim.x;
     const T sx = F.ship_src.eta[0], sy = F.ship_src.eta[1];
     const T reach = a.hull_r * T(1.0001) + T(1e-3);
+    // nothing reads the grid in this phase: drop stale entries queued last frame
+    compact_buckets(a);
     // per-floe scratch of this frame (read last by the previous frame's fracture)
     for (int fl = gtid; fl < a.nf; fl += gsz) {
         a.fcoll[fl] = 0;
         a.fmax[fl] = 0ull;
     }
-    int nesc = 0;
     for (int e = gtid; e < a.n; e += gsz) {
         typename vec2_of<T>::type p = ld2(F.src.pos, e);
         const T ddx = p.x - sx, ddy = p.y - sy;
@@ -519,12 +607,9 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
             a.cnx[e] = T(0);
             a.cny[e] = T(0);
         }
-        if (escaped(a, e, p.x, p.y)) {
-            a.esc[e] = 1;
-            ++nesc;
-        }
+        a.crack[e] = 0;  // set by phase_reduce for elements touching a broken bond
+        warp_append(a.esc_list, (int*)&a.esc_cnt[0], escaped(a, e, p.x, p.y), e);
     }
-    cta_count_add(&a.esc_cnt[0], nesc);
 }
 
 // ─── P_NEAR: one warp per near element (jax_geometry.py:515-594) ────────────
@@ -690,7 +775,10 @@ __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
     const T inv_rise = T(1.0 / P.rise_time_const);
     const T dt = T(P.dt);
     const T rho_g = T(P.water_density * 9.81);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *a.near_cnt = 0;  // P_NEAR is done with it
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *a.near_cnt = 0;   // P_NEAR is done with it
+        *a.comp_cnt = 0;   // P_CULL compacted the queue
+    }
     for (int chunk = blockIdx.x; chunk < a.nchunks; chunk += gridDim.x) {
         int e = chunk * kThreads + threadIdx.x;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -921,255 +1009,318 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     }
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
-    SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
     for (int e = gtid; e < a.n; e += gsz) {
         // activation (jax_simulation.py:498-509)
         const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
         F.dst.active[e] = ae ? 1 : 0;
         // packed kinematics read by substep 0
         const V2 p = ld2(F.src.pos, e), v = ld2(F.src.vel, e);
-        T* k0 = a.kin[0] + 4 * (size_t)e;
-        k0[0] = p.x;
-        k0[1] = p.y;
-        k0[2] = v.x;
-        k0[3] = v.y;
-        // bond slot records for this frame; crack front = touches a broken bond
-        uint8_t ck = 0;
-        const int s0 = a.boff[e], s1 = a.boff[e + 1];
-        for (int sl = s0; sl < s1; ++sl) {
-            const int2 ent = a.bslot[sl];
-            const int b = ent.x & 0x7fffffff;
-            const int o = ent.y;
-            const bool in = F.src.intact[b] != 0;
-            ck |= (uint8_t)!in;
-            const bool ao = F.src.active[o] || a.fcoll[a.floe_of[o]];
-            SlotRec<T> r;
-            r.o = (ent.x < 0) ? (int)((unsigned)o | 0x80000000u) : o;
-            r.rest = a.slot_rest[sl];
-            r.stiff = a.slot_stiff[sl];
-            r.omd = (in && ao == ae) ? T(1) - F.src.dmg[b] : T(-1);
-            rec[sl] = r;
-        }
-        a.crack[e] = ck;
+        typename vec4_of<T>::type k4;
+        k4.x = p.x;
+        k4.y = p.y;
+        k4.z = a.radii[e];
+        k4.w = T(0);
+        reinterpret_cast<typename vec4_of<T>::type*>(a.kin[0])[e] = k4;
+        st2(a.kvel[0], e, v.x, v.y);
+    }
+    // bond slot records for this frame, one thread per slot; crack front =
+    // element touches a bond that is broken at frame start
+    SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
+    for (int sl = gtid; sl < 2 * a.nb; sl += gsz) {
+        const int e = a.slot_owner[sl];
+        const int2 ent = a.bslot[sl];
+        const int b = ent.x & 0x7fffffff;
+        const int o = ent.y;
+        const bool in = F.src.intact[b] != 0;
+        if (!in) a.crack[e] = 1;
+        const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
+        const bool ao = F.src.active[o] || a.fcoll[a.floe_of[o]];
+        SlotRec<T> r;
+        r.o = (ent.x < 0) ? (int)((unsigned)o | 0x80000000u) : o;
+        r.rest = a.slot_rest[sl];
+        r.stiff = a.slot_stiff[sl];
+        r.omd = (in && ao == ae) ? T(1) - F.src.dmg[b] : T(-1);
+        rec[sl] = r;
     }
 }
 
 // ─── P_FORCE: one substep (jax_simulation.py:63-268, 363-395) ───────────────
 // One thread per element, gather form: each element sums its own bond and
 // contact terms in the reference's scatter order, so no atomics are needed.
-// Kinematics are packed {x, y, vx, vy} (one 16-byte load per neighbour) and bond
-// slots are 16-byte records; loads of a batch are issued before any is used.
+// Positions are packed with radii as {x, y, r} (one 16-byte load per neighbour,
+// velocities only for overlapping pairs) and bond slots are 16-byte records;
+// the loads of a batch are issued before any of them is used.
 // Contact distances and every predicate are computed unfused (-fmad=false);
 // force values use explicit fma where the reference's products are summed.
 constexpr int kBatch = 4;
 
-template <typename T> struct vec4_of;
-template <> struct vec4_of<float> { typedef float4 type; };
-template <> struct vec4_of<double> { typedef double4 type; };
-
-template <typename T>
-__device__ __forceinline__ typename vec4_of<T>::type ld4(const T* p, int i) {
-    return reinterpret_cast<const typename vec4_of<T>::type*>(p)[i];
-}
 
 __device__ __forceinline__ float jfma(float a, float b, float c) { return fmaf(a, b, c); }
+// correctly rounded reciprocal (force directions; predicates never use it)
+__device__ __forceinline__ float jrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double jrcp(double a) { return __drcp_rn(a); }
 __device__ __forceinline__ double jfma(double a, double b, double c) { return fma(a, b, c); }
 
+// Constants and substep buffers of one force phase.
 template <typename T>
-__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s) {
+struct ForceCtx {
+    const T *kin, *kvin, *rin, *ain;
+    T *kout, *kvout, *rout, *aout;
+    const uint8_t* act;
+    const SlotRec<T>* rec;
+    T hf, hexp, mu, fcap, c_drag, href, lin, c_rot, dti, damp, alo, ahi, vclip, pclip;
+    bool h15, last;
+};
+
+template <typename T>
+__device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<T>& F, int s) {
+    const DemParams& P = a.P;
+    ForceCtx<T> c;
+    const int k = a.k_sub;
+    c.kin = a.kin[s & 1];
+    c.kout = a.kin[(s + 1) & 1];
+    c.kvin = a.kvel[s & 1];
+    c.kvout = a.kvel[(s + 1) & 1];
+    c.rin = (s == 0) ? F.src.rot : a.sp_rot[(s - 1) & 1];
+    c.ain = (s == 0) ? F.src.avel : a.sp_avel[(s - 1) & 1];
+    c.last = (s == k - 1);
+    c.rout = c.last ? F.dst.rot : a.sp_rot[s & 1];
+    c.aout = c.last ? F.dst.avel : a.sp_avel[s & 1];
+    c.act = F.dst.active;
+    c.rec = reinterpret_cast<const SlotRec<T>*>(a.slotrec);
+    c.hf = T(P.hertz_factor);
+    c.hexp = T(P.hertz_exponent);
+    c.h15 = (P.hertz_exponent == 1.5);
+    c.mu = T(P.ice_ice_friction);
+    c.fcap = T(P.friction_cap);
+    c.c_drag = T(0.5 * P.water_density * P.c_d_drag);
+    c.href = T(P.drag_ref_thickness);
+    c.lin = T(P.linear_drag_factor);
+    c.c_rot = T(-0.5 * P.drag_coefficient_moment * P.water_density);
+    c.dti = T(P.dt_ice);
+    c.damp = T(P.angular_damping);
+    c.alo = T(P.angular_cap_lo);
+    c.ahi = T(P.angular_cap_hi);
+    c.vclip = T(P.velocity_clip);
+    c.pclip = T(P.position_clip);
+    return c;
+}
+
+// Forces, torque and the semi-implicit update of element e for one substep;
+// returns whether e escaped its reference ball.
+template <typename T>
+__device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
+                                              int e) {
     typedef typename vec2_of<T>::type V2;
     typedef typename vec4_of<T>::type V4;
-    const DemParams& P = a.P;
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    const int k = a.k_sub;
-    const T* kin = a.kin[s & 1];
-    T* kout = a.kin[(s + 1) & 1];
-    const T* rin = (s == 0) ? F.src.rot : a.sp_rot[(s - 1) & 1];
-    const T* ain = (s == 0) ? F.src.avel : a.sp_avel[(s - 1) & 1];
-    const bool last = (s == k - 1);
-    T* rout = last ? F.dst.rot : a.sp_rot[s & 1];
-    T* aout = last ? F.dst.avel : a.sp_avel[s & 1];
-    const uint8_t* act = F.dst.active;
-    const SlotRec<T>* rec = reinterpret_cast<const SlotRec<T>*>(a.slotrec);
-    const T hf = T(P.hertz_factor), hexp = T(P.hertz_exponent);
-    const bool h15 = (P.hertz_exponent == 1.5);
-    const T mu = T(P.ice_ice_friction), fcap = T(P.friction_cap);
-    const T c_drag = T(0.5 * P.water_density * P.c_d_drag);
-    const T href = T(P.drag_ref_thickness);
-    const T lin = T(P.linear_drag_factor);
-    const T c_rot = T(-0.5 * P.drag_coefficient_moment * P.water_density);
-    const T dti = T(P.dt_ice);
-    const T damp = T(P.angular_damping), alo = T(P.angular_cap_lo), ahi = T(P.angular_cap_hi);
-    const T vclip = T(P.velocity_clip), pclip = T(P.position_clip);
-    const bool check_escape = !last;
-    int nesc = 0;
-    for (int e = gtid; e < a.n; e += gsz) {
-        const V4 ke = ld4(kin, e);
-        const bool ae = act[e] != 0;
-        // bond forces (jax_simulation.py:63-108): slots with e == bond_i first, then e == bond_j
-        T fbx = T(0), fby = T(0), mb = T(0);
-        const int s0 = a.boff[e], s1 = a.boff[e + 1];
-        for (int base = s0; base < s1; base += kBatch) {
-            SlotRec<T> r[kBatch];
-            V4 ko[kBatch];
+    const T *kin = cx.kin, *kvin = cx.kvin;
+    const uint8_t* act = cx.act;
+    const SlotRec<T>* rec = cx.rec;
+    const T hf = cx.hf, hexp = cx.hexp, mu = cx.mu, fcap = cx.fcap, c_drag = cx.c_drag, href = cx.href;
+    const T lin = cx.lin, c_rot = cx.c_rot, dti = cx.dti, damp = cx.damp, alo = cx.alo, ahi = cx.ahi;
+    const T vclip = cx.vclip, pclip = cx.pclip;
+    const bool h15 = cx.h15, last = cx.last;
+    const V4 ke = ld4(kin, e);  // x, y, radius
+    const V2 ve = ld2(kvin, e);
+    const bool ae = act[e] != 0;
+    // bond forces (jax_simulation.py:63-108): slots with e == bond_i first, then e == bond_j
+    T fbx = T(0), fby = T(0), mb = T(0);
+    const int s0 = a.boff[e], s1 = a.boff[e + 1];
+    for (int base = s0; base < s1; base += kBatch) {
+        SlotRec<T> r[kBatch];
+        V4 ko[kBatch];
 #pragma unroll
-            for (int j = 0; j < kBatch; ++j) {
-                if (base + j < s1) {
-                    r[j] = rec[base + j];
-                    ko[j] = ld4(kin, r[j].o & 0x7fffffff);
-                } else {
-                    r[j].omd = T(-1);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < kBatch; ++j) {
-                if (r[j].omd < T(0)) continue;  // broken, or active/frozen endpoints
-                const bool role_j = r[j].o < 0;
-                const T dx = role_j ? ke.x - ko[j].x : ko[j].x - ke.x;
-                const T dy = role_j ? ke.y - ko[j].y : ko[j].y - ke.y;
-                const T dist = jsqrt(dx * dx + dy * dy);
-                const T inv = T(1) / jmax(dist, T(1e-10));
-                const T fmag = r[j].stiff * (dist - r[j].rest) * r[j].omd;
-                const T fx = (dx * inv) * fmag, fy = (dy * inv) * fmag;
-                const T cr = T(0.5) * jfma(dx, fy, -(dy * fx));
-                if (!role_j) {
-                    fbx += fx;
-                    fby += fy;
-                    mb += cr;
-                } else {
-                    fbx -= fx;
-                    fby -= fy;
-                    mb -= cr;
-                }
+        for (int j = 0; j < kBatch; ++j) {
+            if (base + j < s1) {
+                r[j] = rec[base + j];
+                ko[j] = ld4(kin, r[j].o & 0x7fffffff);
+            } else {
+                r[j].omd = T(-1);
             }
         }
-        // ice-ice contact (jax_simulation.py:111-164)
-        T fix = T(0), fiy = T(0), mi = T(0);
-        const T re = a.radii[e];
-        const int nc = a.ncnt[e];
-        for (int base = 0; base < nc; base += kBatch) {
-            int idx[kBatch];
-            V4 ko[kBatch];
-            T ro[kBatch];
 #pragma unroll
-            for (int j = 0; j < kBatch; ++j) idx[j] = (base + j < nc) ? a.nbr[(size_t)(base + j) * a.n + e] : -1;
-#pragma unroll
-            for (int j = 0; j < kBatch; ++j) {
-                if (idx[j] >= 0) {
-                    ko[j] = ld4(kin, idx[j]);
-                    ro[j] = a.radii[idx[j]];
-                }
+        for (int j = 0; j < kBatch; ++j) {
+            if (r[j].omd < T(0)) continue;  // broken, or active/frozen endpoints
+            const bool role_j = r[j].o < 0;
+            const T dx = role_j ? ke.x - ko[j].x : ko[j].x - ke.x;
+            const T dy = role_j ? ke.y - ko[j].y : ko[j].y - ke.y;
+            const T dist = jsqrt(dx * dx + dy * dy);
+            const T inv = jrcp(jmax(dist, T(1e-10)));
+            const T fmag = r[j].stiff * (dist - r[j].rest) * r[j].omd;
+            const T fx = (dx * inv) * fmag, fy = (dy * inv) * fmag;
+            const T cr = T(0.5) * jfma(dx, fy, -(dy * fx));
+            if (!role_j) {
+                fbx += fx;
+                fby += fy;
+                mb += cr;
+            } else {
+                fbx -= fx;
+                fby -= fy;
+                mb -= cr;
             }
-#pragma unroll
-            for (int j = 0; j < kBatch; ++j) {
-                const int o = idx[j];
-                if (o < 0) continue;
-                const bool e_is_i = e < o;
-                const T dx = e_is_i ? ko[j].x - ke.x : ke.x - ko[j].x;
-                const T dy = e_is_i ? ko[j].y - ke.y : ke.y - ko[j].y;
-                // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
-                const T dist = jsqrt(dx * dx + dy * dy);
-                const T min_dist = e_is_i ? re + ro[j] : ro[j] + re;
-                T overlap = jmax(min_dist - dist, T(0));
-                if (!(dist > T(1e-6))) overlap = T(0);
-                if (!(overlap > T(0))) continue;  // non-overlapping pairs add exact zeros
-                const T inv = T(1) / jmax(dist, T(1e-10));
-                const T ux = dx * inv, uy = dy * inv;
-                const T fn = hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, hexp));
-                const T fnx = ux * fn, fny = uy * fn;
-                const T vrx = e_is_i ? ko[j].z - ke.z : ke.z - ko[j].z;
-                const T vry = e_is_i ? ko[j].w - ke.w : ke.w - ko[j].w;
-                const T vdot = jfma(vrx, ux, vry * uy);
-                const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
-                const T vtm = jsqrt(vtx * vtx + vty * vty);
-                T ftx = T(0), fty = T(0);
-                if (vtm > T(1e-6)) {
-                    const T ftm = jmin(mu * fn, fcap) / vtm;
-                    ftx = -vtx * ftm;
-                    fty = -vty * ftm;
-                }
-                const T oix = -fnx - ftx, oiy = -fny - fty;
-                const T cr = -jfma(dx, oiy, -(dy * oix));
-                if (e_is_i) {
-                    fix += ftx - fnx;
-                    fiy += fty - fny;
-                    mi += T(0.5) * cr;
-                } else {
-                    fix += fnx - ftx;
-                    fiy += fny - fty;
-                    mi -= T(0.5) * cr;
-                }
-            }
-        }
-        // drag (jax_simulation.py:167-192)
-        const T h = a.thick[e], A = a.areas[e];
-        const T a_drag = A * (h / href);
-        const V2 w = ld2(F.vw, e);
-        const T vrx = ke.z - w.x, vry = ke.w - w.y;
-        const T vm = jsqrt(vrx * vrx + vry * vry);
-        T fdx, fdy;
-        if (vm > T(1e-6)) {
-            const T q = c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
-            fdx = vrx * q;
-            fdy = vry * q;
-        } else {
-            const T cl = c_drag * a_drag * lin;
-            fdx = cl * vrx;
-            fdy = cl * vry;
-        }
-        // rotational drag (jax_simulation.py:195-212)
-        const T av = ain[e];
-        const T sub = F.dst.sub[e];
-        const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
-        const T md = c_rot * a.r3[e] * av * fabs(av) * a_sub;
-        const V2 so = ld2(a.soi, e);
-        const T Fx = ((fbx + fix) - fdx) + so.x;
-        const T Fy = ((fby + fiy) - fdy) + so.y;
-        const T Mz = (mb + mi) + md;
-        // semi-implicit Euler (jax_simulation.py:215-268)
-        const T m = a.mass[e];
-        T nvx = jclip(ke.z + (Fx / m) * dti, -vclip, vclip);
-        T nvy = jclip(ke.w + (Fy / m) * dti, -vclip, vclip);
-        T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
-        const T alpha = Mz / a.inertia[e];
-        T nav = jclip(av * damp + alpha * dti, alo, ahi);
-        const T rot = rin[e];
-        T nrot = rot + nav * dti;
-        if (!jfinite(nvx)) nvx = T(0);
-        if (!jfinite(nvy)) nvy = T(0);
-        if (!jfinite(npx)) npx = ke.x;
-        if (!jfinite(npy)) npy = ke.y;
-        npx = jclip(npx, -pclip, pclip);
-        npy = jclip(npy, -pclip, pclip);
-        if (!ae) {
-            nvx = ke.z;
-            nvy = ke.w;
-            npx = ke.x;
-            npy = ke.y;
-            nav = av;
-            nrot = rot;
-        }
-        if (last) {
-            st2(F.dst.pos, e, npx, npy);
-            st2(F.dst.vel, e, nvx, nvy);
-        } else {
-            T* ko = kout + 4 * (size_t)e;
-            typename vec4_of<T>::type v4;
-            v4.x = npx;
-            v4.y = npy;
-            v4.z = nvx;
-            v4.w = nvy;
-            reinterpret_cast<typename vec4_of<T>::type*>(ko)[0] = v4;
-        }
-        rout[e] = nrot;
-        aout[e] = nav;
-        if (check_escape && escaped(a, e, npx, npy)) {
-            a.esc[e] = 1;
-            ++nesc;
         }
     }
-    if (check_escape) cta_count_add(&a.esc_cnt[s + 1], nesc);
+    // ice-ice contact (jax_simulation.py:111-164).  Pass 1 evaluates the exact
+    // contact predicate for every candidate and records the overlapping ones
+    // in a bit mask; pass 2 computes forces for those only, in list order, so
+    // a warp runs the force math max(#overlaps) times, not max(#candidates).
+    T fix = T(0), fiy = T(0), mi = T(0);
+    const T re = ke.z;
+    const int nc = a.ncnt[e];
+    unsigned long long ovm = 0ull;  // max_neighbors <= 64
+    for (int base = 0; base < nc; base += kBatch) {
+        int idx[kBatch];
+        V4 ko[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) idx[j] = (base + j < nc) ? a.nbr[(size_t)(base + j) * a.n + e] : -1;
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j)
+            if (idx[j] >= 0) ko[j] = ld4(kin, idx[j]);
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+            const int o = idx[j];
+            if (o < 0) continue;
+            const bool e_is_i = e < o;
+            const T dx = e_is_i ? ko[j].x - ke.x : ke.x - ko[j].x;
+            const T dy = e_is_i ? ko[j].y - ke.y : ke.y - ko[j].y;
+            // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
+            const T dist = jsqrt(dx * dx + dy * dy);
+            const T min_dist = e_is_i ? re + ko[j].z : ko[j].z + re;
+            const T overlap = jmax(min_dist - dist, T(0));
+            if ((dist > T(1e-6)) && (overlap > T(0))) ovm |= 1ull << (base + j);
+        }
+    }
+    while (ovm) {
+        const int q = __ffsll((long long)ovm) - 1;
+        ovm &= ovm - 1ull;
+        const int o = a.nbr[(size_t)q * a.n + e];
+        const V4 ko = ld4(kin, o);
+        const V2 vo = ld2(kvin, o);
+        const bool e_is_i = e < o;
+        const T dx = e_is_i ? ko.x - ke.x : ke.x - ko.x;
+        const T dy = e_is_i ? ko.y - ke.y : ke.y - ko.y;
+        const T dist = jsqrt(dx * dx + dy * dy);
+        const T min_dist = e_is_i ? re + ko.z : ko.z + re;
+        const T overlap = min_dist - dist;
+        const T inv = jrcp(dist);  // dist > 1e-6 here
+        const T ux = dx * inv, uy = dy * inv;
+        const T fn = hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, hexp));
+        const T fnx = ux * fn, fny = uy * fn;
+        const T vrx = e_is_i ? vo.x - ve.x : ve.x - vo.x;
+        const T vry = e_is_i ? vo.y - ve.y : ve.y - vo.y;
+        const T vdot = jfma(vrx, ux, vry * uy);
+        const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
+        const T vtm = jsqrt(vtx * vtx + vty * vty);
+        T ftx = T(0), fty = T(0);
+        if (vtm > T(1e-6)) {
+            const T ftm = jmin(mu * fn, fcap) * jrcp(vtm);
+            ftx = -vtx * ftm;
+            fty = -vty * ftm;
+        }
+        const T oix = -fnx - ftx, oiy = -fny - fty;
+        const T cr = -jfma(dx, oiy, -(dy * oix));
+        if (e_is_i) {
+            fix += ftx - fnx;
+            fiy += fty - fny;
+            mi += T(0.5) * cr;
+        } else {
+            fix += fnx - ftx;
+            fiy += fny - fty;
+            mi -= T(0.5) * cr;
+        }
+    }
+    // drag (jax_simulation.py:167-192)
+    const T h = a.thick[e], A = a.areas[e];
+    const T a_drag = A * (h / href);
+    const V2 w = ld2(F.vw, e);
+    const T vrx = ve.x - w.x, vry = ve.y - w.y;
+    const T vm = jsqrt(vrx * vrx + vry * vry);
+    T fdx, fdy;
+    if (vm > T(1e-6)) {
+        const T q = c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
+        fdx = vrx * q;
+        fdy = vry * q;
+    } else {
+        const T cl = c_drag * a_drag * lin;
+        fdx = cl * vrx;
+        fdy = cl * vry;
+    }
+    // rotational drag (jax_simulation.py:195-212)
+    const T av = cx.ain[e];
+    const T sub = F.dst.sub[e];
+    const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
+    const T md = c_rot * a.r3[e] * av * fabs(av) * a_sub;
+    const V2 so = ld2(a.soi, e);
+    const T Fx = ((fbx + fix) - fdx) + so.x;
+    const T Fy = ((fby + fiy) - fdy) + so.y;
+    const T Mz = (mb + mi) + md;
+    // semi-implicit Euler (jax_simulation.py:215-268)
+    const T m = a.mass[e];
+    T nvx = jclip(ve.x + (Fx / m) * dti, -vclip, vclip);
+    T nvy = jclip(ve.y + (Fy / m) * dti, -vclip, vclip);
+    T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
+    const T alpha = Mz / a.inertia[e];
+    T nav = jclip(av * damp + alpha * dti, alo, ahi);
+    const T rot = cx.rin[e];
+    T nrot = rot + nav * dti;
+    if (!jfinite(nvx)) nvx = T(0);
+    if (!jfinite(nvy)) nvy = T(0);
+    if (!jfinite(npx)) npx = ke.x;
+    if (!jfinite(npy)) npy = ke.y;
+    npx = jclip(npx, -pclip, pclip);
+    npy = jclip(npy, -pclip, pclip);
+    if (!ae) {
+        nvx = ve.x;
+        nvy = ve.y;
+        npx = ke.x;
+        npy = ke.y;
+        nav = av;
+        nrot = rot;
+    }
+    if (last) {
+        st2(F.dst.pos, e, npx, npy);
+        st2(F.dst.vel, e, nvx, nvy);
+    } else {
+        typename vec4_of<T>::type v4;
+        v4.x = npx;
+        v4.y = npy;
+        v4.z = re;
+        v4.w = T(0);
+        reinterpret_cast<typename vec4_of<T>::type*>(cx.kout)[e] = v4;
+        st2(cx.kvout, e, nvx, nvy);
+    }
+    cx.rout[e] = nrot;
+    cx.aout[e] = nav;
+    return !last && escaped(a, e, npx, npy);
+}
+
+template <typename T>
+__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigned round, bool has_dirty) {
+    const ForceCtx<T> cx = force_ctx(a, F, s);
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    int* esc_ctr = (int*)&a.esc_cnt[s + 1];
+    if (has_dirty) {
+        // elements whose list this round invalidated: one warp rebuilds the list,
+        // then lane 0 computes the element (the main loop below skips them)
+        __shared__ int sbuf[kThreads / 32][2 * kMaxNbLocal];
+        __shared__ int scnt[kThreads / 32];
+        const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int warp = gtid >> 5, nwarps = gsz >> 5;
+        const int nd = *((volatile int*)&a.dirty_cnt[s]);
+        if (gtid == 0) atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)nd);
+        for (int q = warp; q < nd; q += nwarps) {
+            const int e = a.dirty_list[q];
+            warp_build(a, e, sbuf[wl], &scnt[wl]);
+            if (lane == 0 && force_element(a, F, cx, e)) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+            __syncwarp();
+        }
+    }
+    for (int e = gtid; e < a.n; e += gsz) {
+        if (has_dirty && a.dirty[e] == round) continue;
+        const bool esc = force_element(a, F, cx, e);
+        if (!cx.last) warp_append(a.esc_list, esc_ctr, esc, e);
+    }
 }
 
 // ─── bond damage (jax_bond_fracture.py:133-208) ─────────────────────────────
@@ -1314,21 +1465,26 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
     for (int fl = gtid; fl < a.nf; fl += gsz) F.dst.elig[fl] = new_elig(a, F, fl, scale) ? 1 : 0;
     if (a.d_fmag)
         for (int e = gtid; e < a.n; e += gsz) a.d_fmag[e] = a.fraw[e] * scale;
-    for (int i = gtid; i < a.k_sub + 2; i += gsz) a.esc_cnt[i] = 0u;
+    for (int i = gtid; i < a.k_sub + 2; i += gsz) {
+        a.esc_cnt[i] = 0u;
+        a.dirty_cnt[i] = 0;
+    }
 }
 
 // ─── the kernel ─────────────────────────────────────────────────────────────
-// Phase numbering inside a frame: 0 cull, 1 near-element contact, 2 contact
-// forces, 3 reduce + vessel, then for substep s: 4+4s re-reference, 5+4s mark,
-// 6+4s list build, 7+4s force; last: 4+4k fracture.  The three list phases run
-// only when elements escaped (esc_cnt[s] > 0), a decision every CTA takes from
-// the same word after a barrier.
+// Phase numbering inside a frame: 0 cull (+ grid compaction), 1 near-element
+// contact, 2 contact forces, 3 reduce + vessel, then for substep s: 4+3s
+// escape round (re-reference + mark), 5+3s rebuild of every list (only when
+// most elements escaped), 6+3s force (rebuilding marked lists first); last:
+// 4+3k fracture.  Whether a list phase runs is decided by every CTA from the
+// same word after a barrier, so skipped phases skip their barrier too.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2) dem_frames_kernel(KArgs<T> a, int ph_lo, int ph_hi) {
+__global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(const __grid_constant__ KArgs<T> a, int ph_lo, int ph_hi) {
     extern __shared__ unsigned char smem_raw[];
     T* hullw = reinterpret_cast<T*>(smem_raw);
     const int k = a.k_sub;
-    const int per_frame = 5 + 4 * k;
+    const int per_frame = phases_per_frame(k);
+    if (ph_hi > a.K * per_frame) ph_hi = a.K * per_frame;  // uniform over the grid
     const bool persistent = (a.mode == DEM_LAUNCH_PERSISTENT);
     if (persistent && a.ptimes && blockIdx.x == 0 && threadIdx.x == 0) a.ptimes[1] = globaltimer_ns();
     for (int ph = ph_lo; ph < ph_hi; ++ph) {
@@ -1346,22 +1502,20 @@ __global__ void __launch_bounds__(kThreads, 2) dem_frames_kernel(KArgs<T> a, int
         } else if (p == per_frame - 1) {
             phase_fracture(a, F, T(*((volatile double*)&a.fscal[0])));
         } else {
-            const int s = (p - 4) / 4;
-            const int sub = (p - 4) % 4;
+            const int s = (p - 4) / 3;
+            const int sub = (p - 4) % 3;
             const unsigned cnt = *((volatile unsigned*)&a.esc_cnt[s]);
-            if (sub < 3) {
-                const bool all = (unsigned long long)cnt * 8ull > (unsigned long long)a.n;
-                if (cnt == 0u || (sub == 1 && all)) continue;  // uniform: no barrier either
-                if (sub == 0) {
-                    phase_reref(a, a.kin[s & 1]);
-                } else if (sub == 1) {
-                    phase_mark(a);
-                } else {
-                    phase_build(a, all);
-                }
+            const bool all = (unsigned long long)cnt * 8ull > (unsigned long long)a.n;
+            // stamp of this rebuild round, unique since the dirty stamps were last cleared
+            const unsigned round = a.round_base + (unsigned)(f * k + s) + 1u;
+            if (sub == 0) {
+                if (cnt == 0u) continue;  // uniform: no barrier either
+                phase_escape(a, a.kin[s & 1], cnt, s, round, all);
+            } else if (sub == 1) {
+                if (cnt == 0u || !all) continue;
+                phase_build_all(a);
             } else {
-                if (cnt != 0u) compact_buckets(a);  // nothing reads the grid in this phase
-                phase_force(a, F, s);
+                phase_force(a, F, s, round, cnt != 0u && !all);
             }
         }
         if (persistent && ph + 1 < ph_hi) {

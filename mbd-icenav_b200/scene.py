@@ -413,6 +413,40 @@ def make_large_field(seed: int = 0, n_frames: int = 1000, cell_area: float = 6.2
                    (0.0, side, 0.0, side), extra={"floes": len(floes), "concentration": covered})
 
 
+def morton_order(points: np.ndarray, cell: float) -> np.ndarray:
+    """Permutation sorting points along a Z-order (Morton) curve of square cells."""
+    q = np.floor((points - points.min(axis=0)) / cell).astype(np.int64)
+    q = np.clip(q, 0, (1 << 20) - 1)
+
+    def spread(v):
+        v = (v | (v << 16)) & 0x0000FFFF0000FFFF
+        v = (v | (v << 8)) & 0x00FF00FF00FF00FF
+        v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0F
+        v = (v | (v << 2)) & 0x3333333333333333
+        v = (v | (v << 1)) & 0x5555555555555555
+        return v
+
+    code = spread(q[:, 0]) | (spread(q[:, 1]) << 1)
+    return np.argsort(code, kind="stable")
+
+
+def spatially_sorted(field: IceField, cell: float = 4.0) -> IceField:
+    """The same field with its elements renumbered in Morton order of their centroids.
+
+    Element order does not change the physics (bond and pair lists are
+    renumbered with it); it decides memory locality of the per-element gathers.
+    """
+    perm = morton_order(field.centroids, cell)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    bonds = [(int(min(inv[i], inv[j])), int(max(inv[i], inv[j]))) for i, j in field.bonds]
+    bonds.sort()
+    import dataclasses
+    return dataclasses.replace(field, polygons=[field.polygons[k] for k in perm],
+                               centroids=field.centroids[perm], bonds=bonds,
+                               thicknesses=field.thicknesses[perm], parent_ids=field.parent_ids[perm])
+
+
 def make_field(name: str, seed: int = 0, **kw) -> IceField:
     return {"small": make_small_field, "medium": make_medium_field,
             "large": make_large_field}[name](seed=seed, **kw)

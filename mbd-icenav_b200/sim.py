@@ -292,14 +292,26 @@ class FrameStep:
             rc = self.lib.dem_sync_status(self._h, self._stream())
             if rc == _abi.DEM_OK:
                 return
-            if rc == _abi.DEM_ERR_CAPACITY and attempt < retries:
-                # inputs are untouched: grow the scratch and run the same call again
-                P = self.params
-                P.max_neighbors = min(64, int(P.max_neighbors * 1.5) + 1)
-                P.bucket_capacity = int(P.bucket_capacity * 2)
-                self._check(self.lib.dem_set_capacity(self._h, P.max_neighbors, P.bucket_capacity))
-                continue
+            if rc == _abi.DEM_ERR_CAPACITY and attempt < retries and self.grow_capacity():
+                continue  # inputs are untouched: run the same call again
             raise _abi.DemError(rc, self._error())
+
+    def grow_capacity(self) -> bool:
+        """After ``DEM_ERR_CAPACITY``: enlarge what overflowed (neighbour lists up
+        to 64 entries, grid buckets without limit) and reset the broad phase.
+        Returns False when nothing can grow any more."""
+        flags = self.info()["capacity_flags"] or 3
+        P = self.params
+        nb, bc = P.max_neighbors, P.bucket_capacity
+        if flags & 2:
+            nb = min(64, int(nb * 1.5) + 1)
+        if flags & 1:
+            bc = int(bc * 2)
+        if (nb, bc) == (P.max_neighbors, P.bucket_capacity):
+            return False
+        P.max_neighbors, P.bucket_capacity = nb, bc
+        self._check(self.lib.dem_set_capacity(self._h, nb, bc))
+        return True
 
     # ── the reference-facing calls ────────────────────────────────────────────
     def __call__(self, state: IceState, ship_state: ShipState, setpoint, setpoint_next, v_water,

@@ -181,7 +181,9 @@ class Oracle:
             self._all_j = np.concatenate([np.arange(i + 1, n) for i in range(n)]) if n else np.zeros(0, int)
         # max vertex radius per element, for the ship-contact cull
         self.vert_r = np.sqrt((np.asarray(s.local_polys_padded, np.float64) ** 2).sum(-1)).max(-1) if self.n else np.zeros(0)
-        self.hull_r = float(np.sqrt((np.asarray(ship_dyn.ship_hull_local, np.float64) ** 2).sum(-1)).max())
+        # ship reach: outline points (pass 2) and the analytic hull box corners (pass 1)
+        self.hull_r = max(float(np.sqrt((np.asarray(ship_dyn.ship_hull_local, np.float64) ** 2).sum(-1)).max()),
+                          math.hypot(params.half_len, params.half_beam))
 
     # ── broad phase ─────────────────────────────────────────────────────────
     def candidate_pairs(self, pos):

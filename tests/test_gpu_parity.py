@@ -133,3 +133,37 @@ def test_f32_drift_1000_substeps_vs_f64_oracle(golden64):
     assert max(drift) < 5e-3, drift
     print("max position drift (m) over 1000 substeps:", max(drift))
     fs.close()
+
+
+def test_contact_in_hull_box_corner_is_not_culled():
+    """A vertex inside the analytic hull's stern corner, farther from the ship
+    centre than any outline point, still makes contact (pass 1 of
+    jax_geometry.py:515-594); the reach bound must cover the hull box corners."""
+    from mbd_icenav_b200 import sim
+    from mbd_icenav_b200.config import SimulationConfig
+    from mbd_icenav_b200.state import (build_static_arrays, initial_ice_state_arrays,
+                                       ship_dynamics_arrays)
+    from mbd_icenav_b200.vessel import ShipProperties, SupplyVessel, pointed_hull_outline
+    from oracle.dem_oracle import OShip, OState, Oracle, params_from_config
+    cfg = SimulationConfig()
+    tri = np.array([[29.9, 5.9], [31.9, 6.2], [30.6, 7.9]])
+    cent = tri.mean(axis=0, keepdims=True)
+    props = ShipProperties(length=60.0, beam=12.0, draft=4.0)
+    hull = pointed_hull_outline(60.0, 12.0)
+    assert np.hypot(*tri[0]) > np.hypot(hull[:, 0], hull[:, 1]).max()
+    sa = build_static_arrays([tri], cent, [], np.ones(1), None, cfg)
+    sd = ship_dynamics_arrays(props, cfg, 60.0, 12.0, hull)
+    sv = SupplyVessel(mass=props.mass, length=60.0)
+    o = Oracle(sa, sd, params_from_config(cfg, 60.0, 12.0, 1, 0.05, 0.05, False, 1.0), sv.B)
+    st0 = OState(*initial_ice_state_arrays(1, cent, 0, np.zeros(1, np.int32)))
+    sh0 = OShip(np.zeros(3), np.zeros(3), np.zeros(6), np.zeros(3))
+    _, _, od = o.frame_step(st0, sh0, np.zeros(3), np.zeros(3), np.zeros((1, 2)), st0.dpdem_floe_eligible)
+    assert od["pen_max"][0] > 0
+    fs = sim.make_frame_step(sa, cfg, sd, 60.0, 12.0, 1, 0.05, 0.05, False, sv.B, 1.0,
+                             device=torch.device("cuda", 0), dtype=torch.float64)
+    st, sh = to_gpu_state(st0, sh0, torch.float64)
+    z = torch.zeros(3, dtype=torch.float64, device="cuda")
+    _, _, diag = fs(st, sh, z, z, torch.zeros((1, 2), dtype=torch.float64, device="cuda"),
+                    st.dpdem_floe_eligible)
+    np.testing.assert_allclose(diag["pen_max"].cpu().numpy(), od["pen_max"], rtol=1e-12)
+    fs.close()
