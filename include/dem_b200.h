@@ -229,6 +229,38 @@ int dem_destroy(DemHandle* h);
 /* Library version string, e.g. "dem_b200 0.1 sm_100a". */
 const char* dem_version(void);
 
+/* Largest n accepted by dem_ship_contact_noalloc. */
+#define DEM_CONTACT_NOALLOC_MAX_ELEMENTS 262144
+
+/* Ship–ice contact detection that allocates nothing.  No counterpart in the
+ * reference: it is the contact test that dem_frame_step runs at the start of
+ * every frame (diag.pen_max), offered without a handle for callers that cannot
+ * call cudaMalloc — a host whose caching allocator already owns all of the
+ * GPU's memory, or a fixed-rate navigation loop that cannot take cudaMalloc's
+ * device-wide synchronisation and unbounded latency in its cycle.
+ *
+ * For each element (positions (n,2), rotations (n,), local_polys_padded
+ * (n,max_v,2), poly_mask (n,max_v), all DEVICE arrays of `dtype`) against the
+ * ship at ship_eta (3,) with outline ship_hull_local (n_hull,2) and analytic
+ * hull half_len x half_beam: pen_max (n,) gets the deepest penetration and, if
+ * not NULL, normals (n,2) its unit normal (zeros where there is no contact).
+ * Runs on the CURRENT device and on `stream` (a cudaStream_t; NULL = default).
+ *
+ * Scratch: one static device array of 1 MiB + 256 bytes per device (held by
+ * every device that loads the library until the process exits), hence the
+ * limit n <= DEM_CONTACT_NOALLOC_MAX_ELEMENTS; larger n returns
+ * DEM_ERR_CAPACITY before any work.  The first call on a device looks up that
+ * array's device address (once per device): make that first call before any
+ * stream capture on the device.  Every call on a device shares the array, so
+ * calls that overlap on the GPU (other streams, other host threads) race on
+ * it: serialise them.  Returns DEM_ERR_INVALID for bad arguments and
+ * DEM_ERR_CUDA if a launch fails. */
+int dem_ship_contact_noalloc(int32_t dtype, int32_t n, int32_t max_v, const void* local_polys_padded,
+                             const uint8_t* poly_mask, const void* positions, const void* rotations,
+                             int32_t n_hull, const void* ship_hull_local, double half_len, double half_beam,
+                             int32_t n_edge_samples, const void* ship_eta, void* pen_max, void* normals,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -826,3 +827,276 @@ int dem_destroy(DemHandle* h) {
 }
 
 }  // extern "C"
+
+// ════════════════════════════════════════════════════════════════════════════
+// dem_ship_contact_noalloc: the frame step's ship-contact test with its
+// near-element list in a static device array instead of handle scratch.
+// ════════════════════════════════════════════════════════════════════════════
+namespace {
+
+constexpr int kNoAllocMax = DEM_CONTACT_NOALLOC_MAX_ELEMENTS;
+// bytes [0, 4): near-element count; from byte 256: the near-element list
+constexpr size_t kNoAllocListOffset = 256;
+constexpr size_t kNoAllocBytes = kNoAllocListOffset + sizeof(int) * (size_t)kNoAllocMax;
+static __device__ __align__(256) unsigned char g_contact_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+    unsigned char* scratch = nullptr;  // device address of g_contact_scratch
+    int sm_count = 0;
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+template <typename T>
+struct ContactArgs {
+    int n, V, S, E;
+    const T* polys;
+    const uint8_t* pmask;
+    const T* pos;
+    const T* rot;
+    const T* hull;
+    const T* eta;
+    double half_len, half_beam;
+    T t_samp[dem::kMaxEdgeSamples];
+    T* pen;
+    T* nrm;
+    int* near_cnt;
+    int* near_list;
+};
+
+// Elements whose bounding circle reaches the ship go to the near list; the
+// rest get pen = 0 and a zero normal, which is what all of their point tests
+// return (every query point lies within the element's vertex radius of its
+// centroid, every hull point within the hull reach of the ship).
+template <typename T>
+__global__ void __launch_bounds__(dem::kThreads) noalloc_cull_kernel(const __grid_constant__ ContactArgs<T> c) {
+    __shared__ double s_part[dem::kThreads / 32];
+    double r = 0.0;
+    for (int i = threadIdx.x; i < c.S; i += blockDim.x)
+        r = fmax(r, hypot((double)c.hull[2 * i], (double)c.hull[2 * i + 1]));
+    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = r;
+    __syncthreads();
+    double reach = hypot(c.half_len, c.half_beam);  // corners of the analytic hull box
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) reach = fmax(reach, s_part[w]);
+    reach = reach * (1.0 + 1e-5) + 1e-3;
+    const double sx = (double)c.eta[0], sy = (double)c.eta[1];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < c.n; e += gridDim.x * blockDim.x) {
+        const T* lp = c.polys + (size_t)e * c.V * 2;
+        double vr = 0.0;
+        for (int k = 0; k < c.V; ++k) vr = fmax(vr, hypot((double)lp[2 * k], (double)lp[2 * k + 1]));
+        const double lim = reach + vr * (1.0 + 1e-5) + 1e-4;
+        const double dx = (double)c.pos[2 * e] - sx, dy = (double)c.pos[2 * e + 1] - sy;
+        // NaN positions stay on the exact path (the comparison is false)
+        if (!(dx * dx + dy * dy > lim * lim * 1.0001)) {
+            c.near_list[atomicAdd(c.near_cnt, 1)] = e;
+        } else {
+            c.pen[e] = T(0);
+            if (c.nrm) {
+                c.nrm[2 * e] = T(0);
+                c.nrm[2 * e + 1] = T(0);
+            }
+        }
+    }
+}
+
+// One warp per near element: pass 1 (the element's vertices and edge samples
+// against the analytic hull), pass 2 (hull outline points inside the
+// element's polygon), element-wise deepest with the reference's first-index
+// ties (jax_geometry.py:515-594).
+template <typename T>
+__global__ void __launch_bounds__(dem::kThreads) noalloc_near_kernel(const __grid_constant__ ContactArgs<T> c) {
+    extern __shared__ double noalloc_smem[];
+    T* hullw = reinterpret_cast<T*>(noalloc_smem);
+    dem::HullPose<T> H;
+    H.sx = c.eta[0];
+    H.sy = c.eta[1];
+    const T spsi = c.eta[2];
+    dem::jsincos(-spsi, &H.s_neg, &H.c_neg);
+    dem::jsincos(spsi, &H.s_h, &H.c_h);
+    H.hl = T(c.half_len);
+    H.hb = T(c.half_beam);
+    H.hb005 = T(c.half_beam * 0.05);
+    for (int i = threadIdx.x; i < c.S; i += blockDim.x) {
+        const T lx = c.hull[2 * i], ly = c.hull[2 * i + 1];
+        hullw[2 * i] = lx * H.c_h + ly * (-H.s_h) + H.sx;
+        hullw[2 * i + 1] = lx * H.s_h + ly * H.c_h + H.sy;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nnear = *((volatile int*)c.near_cnt);
+    const int V = c.V, E = c.E, P1 = V * (1 + E);
+    for (int q = warp; q < nnear; q += nwarps) {
+        const int e = c.near_list[q];
+        const T px = c.pos[2 * e], py = c.pos[2 * e + 1];
+        T cs, sn;
+        dem::jsincos(c.rot[e], &sn, &cs);
+        const T* lp = c.polys + (size_t)e * V * 2;
+        const uint8_t* mk = c.pmask + (size_t)e * V;
+        auto wv = [&](int k, T& x, T& y) {
+            const T lx = lp[2 * k], ly = lp[2 * k + 1];
+            x = cs * lx - sn * ly + px;
+            y = sn * lx + cs * ly + py;
+        };
+        dem::Best<T> b1 = {T(0), T(0), T(0), INT_MAX};
+        for (int pt = lane; pt < P1; pt += 32) {
+            const int k = pt / (1 + E), j = pt % (1 + E);
+            T qx, qy;
+            wv(k, qx, qy);
+            if (j > 0) {
+                T x1, y1;
+                wv((k + 1 == V) ? 0 : k + 1, x1, y1);
+                const T t = c.t_samp[j - 1];
+                const T omt = T(1) - t;
+                qx = qx * omt + x1 * t;
+                qy = qy * omt + y1 * t;
+            }
+            T p, nx, ny;
+            dem::hull_point(H, qx, qy, p, nx, ny);
+            if (!mk[k]) p = T(0);
+            dem::better(b1, p, nx, ny, pt);
+        }
+        b1 = dem::warp_best(b1);
+        T wx[dem::kMaxV], wy[dem::kMaxV], mx[dem::kMaxV], my[dem::kMaxV], mc[dem::kMaxV];
+        for (int k = 0; k < V; ++k) {
+            wv(k, wx[k], wy[k]);
+            const bool m = mk[k] != 0;
+            mx[k] = m ? wx[k] : T(0);
+            my[k] = m ? wy[k] : T(0);
+            mc[k] = m ? T(1) : T(0);
+        }
+        const T n_real = dem::jmax(dem::np_pairwise_sum(mc, V), T(1));
+        const T cxc = dem::np_pairwise_sum(mx, V) / n_real;
+        const T cyc = dem::np_pairwise_sum(my, V) / n_real;
+        dem::Best<T> b2 = {T(0), T(0), T(0), INT_MAX};
+        for (int si = lane; si < c.S; si += 32) {
+            const T hx = hullw[2 * si], hy = hullw[2 * si + 1];
+            int crossings = 0;
+            T dmin = T(0);
+            int kbest = 0;
+            for (int k = 0; k < V; ++k) {
+                const int k1 = (k + 1 == V) ? 0 : k + 1;
+                const T xi = wx[k], yi = wy[k], xj = wx[k1], yj = wy[k1];
+                const bool cond_y = (yi > hy) != (yj > hy);
+                const T x_int = (xj - xi) * (hy - yi) / (yj - yi + T(1e-10)) + xi;
+                if (cond_y && (hx < x_int)) ++crossings;
+                const T vx = xj - xi, vy = yj - yi;
+                const T c1 = (hx - xi) * vx + (hy - yi) * vy;
+                const T c2 = vx * vx + vy * vy + T(1e-20);
+                const T t = dem::jclip(c1 / c2, T(0), T(1));
+                const T ddx = hx - (xi + t * vx), ddy = hy - (yi + t * vy);
+                const T d = dem::jsqrt(ddx * ddx + ddy * ddy + T(1e-20));
+                if (k == 0 || d < dmin) {
+                    dmin = d;
+                    kbest = k;
+                }
+            }
+            T p = T(0), nx = T(0), ny = T(0);
+            if ((crossings % 2) == 1) {
+                const int k = kbest, k1 = (k + 1 == V) ? 0 : k + 1;
+                const T ex = wx[k1] - wx[k], ey = wy[k1] - wy[k];
+                T nxe = ey, nye = -ex;
+                const T nlen = dem::jsqrt(nxe * nxe + nye * nye + T(1e-20));
+                nxe = nxe / nlen;
+                nye = nye / nlen;
+                const T midx = (wx[k] + wx[k1]) / T(2), midy = (wy[k] + wy[k1]) / T(2);
+                if ((midx - cxc) * nxe + (midy - cyc) * nye < T(0)) {
+                    nxe = -nxe;
+                    nye = -nye;
+                }
+                p = dmin;
+                nx = nxe;
+                ny = nye;
+            }
+            dem::better(b2, p, nx, ny, si);
+        }
+        b2 = dem::warp_best(b2);
+        if (lane == 0) {
+            const bool use2 = (b2.p > T(0)) && (b2.p > b1.p);
+            c.pen[e] = use2 ? b2.p : b1.p;
+            if (c.nrm) {
+                c.nrm[2 * e] = use2 ? b2.nx : b1.nx;
+                c.nrm[2 * e + 1] = use2 ? b2.ny : b1.ny;
+            }
+        }
+    }
+}
+
+template <typename T>
+int noalloc_contact(const NoAllocDevice& d, ContactArgs<T>& c, const double* t_samp, cudaStream_t st) {
+    for (int i = 0; i < dem::kMaxEdgeSamples; ++i) c.t_samp[i] = (T)t_samp[i];
+    // the count must start at zero; the list keeps the previous call's entries
+    // but only the first `count` are read
+    if (cudaMemsetAsync(c.near_cnt, 0, sizeof(int), st) != cudaSuccess) return DEM_ERR_CUDA;
+    const int blocks = (int)std::min<long long>(((long long)c.n + dem::kThreads - 1) / dem::kThreads,
+                                                (long long)d.sm_count * 8);
+    noalloc_cull_kernel<T><<<blocks, dem::kThreads, 0, st>>>(c);
+    if (cudaGetLastError() != cudaSuccess) return DEM_ERR_CUDA;
+    const size_t smem = (size_t)c.S * 2 * sizeof(T) + 16;
+    noalloc_near_kernel<T><<<d.sm_count * 4, dem::kThreads, smem, st>>>(c);
+    if (cudaGetLastError() != cudaSuccess) return DEM_ERR_CUDA;
+    return DEM_OK;
+}
+
+}  // namespace
+
+extern "C" int dem_ship_contact_noalloc(int32_t dtype, int32_t n, int32_t max_v, const void* local_polys_padded,
+                                        const uint8_t* poly_mask, const void* positions, const void* rotations,
+                                        int32_t n_hull, const void* ship_hull_local, double half_len,
+                                        double half_beam, int32_t n_edge_samples, const void* ship_eta,
+                                        void* pen_max, void* normals, void* stream) {
+    if (dtype != DEM_F32 && dtype != DEM_F64) return DEM_ERR_INVALID;
+    if (n < 0) return DEM_ERR_INVALID;
+    if (n > kNoAllocMax) return DEM_ERR_CAPACITY;  // the static scratch holds at most kNoAllocMax elements
+    if (max_v < 1 || max_v > dem::kMaxV || n_hull < 0 || n_hull > dem::kMaxHull || n_edge_samples < 0 ||
+        n_edge_samples > dem::kMaxEdgeSamples)
+        return DEM_ERR_INVALID;
+    if (!local_polys_padded || !poly_mask || !positions || !rotations || !ship_eta || !pen_max ||
+        (n_hull > 0 && !ship_hull_local))
+        return DEM_ERR_INVALID;
+    if (n == 0) return DEM_OK;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DEM_ERR_CUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return DEM_ERR_INVALID;
+    NoAllocDevice d;
+    {
+        // once per device, with that device current: the address of this
+        // device's copy of the static scratch array
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        NoAllocDevice& slot = g_noalloc_dev[dev];
+        if (!slot.scratch) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_contact_scratch) != cudaSuccess || !p) return DEM_ERR_CUDA;
+            int sm = 0;
+            if (cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sm < 1)
+                return DEM_ERR_CUDA;
+            slot.sm_count = sm;
+            slot.scratch = static_cast<unsigned char*>(p);
+        }
+        d = slot;
+    }
+    double t_samp[dem::kMaxEdgeSamples] = {0};
+    np_linspace(1.0 / (n_edge_samples + 1), (double)n_edge_samples / (n_edge_samples + 1), n_edge_samples, t_samp);
+    cudaStream_t st = (cudaStream_t)stream;
+    int* near_cnt = reinterpret_cast<int*>(d.scratch);
+    int* near_list = reinterpret_cast<int*>(d.scratch + kNoAllocListOffset);
+    if (dtype == DEM_F32) {
+        ContactArgs<float> c{};
+        c.n = n, c.V = max_v, c.S = n_hull, c.E = n_edge_samples;
+        c.polys = (const float*)local_polys_padded, c.pmask = poly_mask, c.pos = (const float*)positions;
+        c.rot = (const float*)rotations, c.hull = (const float*)ship_hull_local, c.eta = (const float*)ship_eta;
+        c.half_len = half_len, c.half_beam = half_beam;
+        c.pen = (float*)pen_max, c.nrm = (float*)normals, c.near_cnt = near_cnt, c.near_list = near_list;
+        return noalloc_contact<float>(d, c, t_samp, st);
+    }
+    ContactArgs<double> c{};
+    c.n = n, c.V = max_v, c.S = n_hull, c.E = n_edge_samples;
+    c.polys = (const double*)local_polys_padded, c.pmask = poly_mask, c.pos = (const double*)positions;
+    c.rot = (const double*)rotations, c.hull = (const double*)ship_hull_local, c.eta = (const double*)ship_eta;
+    c.half_len = half_len, c.half_beam = half_beam;
+    c.pen = (double*)pen_max, c.nrm = (double*)normals, c.near_cnt = near_cnt, c.near_list = near_list;
+    return noalloc_contact<double>(d, c, t_samp, st);
+}
