@@ -176,7 +176,7 @@ class ClockSampler:
                 "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def build_stepper(field, dtype_name: str, device, bucket_capacity: int = 64):
+def build_stepper(field, dtype_name: str, device, bucket_capacity: int = 64, skin: float = 0.3):
     import numpy as np
     import torch
     from mbd_icenav_b200 import sim
@@ -192,7 +192,8 @@ def build_stepper(field, dtype_name: str, device, bucket_capacity: int = 64):
                                     field.hull_local, dtype=dt, device=device)
     sv = SupplyVessel(mass=field.ship_props.mass, length=field.ship_length)
     fs = sim.make_frame_step(static, cfg, sdyn, field.ship_length, field.ship_beam, N_SUB, DT, DT / N_SUB,
-                             False, sv.B, sv.T_n, device=device, dtype=dt, bucket_capacity=bucket_capacity)
+                             False, sv.B, sv.T_n, device=device, dtype=dt, bucket_capacity=bucket_capacity,
+                             skin=skin)
     st = to_device(initial_ice_state_arrays(field.n, field.centroids, len(field.bonds), field.parent_ids), dt, device)
     eta0 = field.trajectory[START_FRAME]
     sh = to_device(initial_ship_state_arrays(eta0[:2], float(eta0[2])), dt, device)
@@ -210,7 +211,7 @@ def run_ours(args, rank: int, world: int):
     if args.order == "morton":
         from mbd_icenav_b200 import scene
         field = scene.spatially_sorted(field)
-    fs, st, sh, static = build_stepper(field, args.dtype, device, args.bucket_capacity)
+    fs, st, sh, static = build_stepper(field, args.dtype, device, args.bucket_capacity, args.skin)
     if args.launch == "phased":
         from mbd_icenav_b200 import _abi
         fs.set_launch_mode(_abi.DEM_LAUNCH_PHASED)
@@ -329,7 +330,8 @@ def run_ours(args, rank: int, world: int):
                    "neighbor_rebuild_rounds": info["neighbor_rebuilds"],
                    "elements_reref_total": info["escaped_total"],
                    "lists_rebuilt_total": info["rebuilt_lists_total"],
-                   "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity},
+                   "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity,
+                   "skin_m": fs.params.skin},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} copy bandwidth",
                      "algorithmic_bytes_per_launch": bpf,
@@ -488,6 +490,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch", choices=["persistent", "phased"], default="persistent")
+    ap.add_argument("--skin", type=float, default=0.3, help="Verlet skin of the neighbour lists [m]")
     ap.add_argument("--bucket-capacity", type=int, default=64,
                     help="grid-bucket capacity at start (grown automatically on overflow)")
     ap.add_argument("--order", choices=["floe", "morton"], default="floe",

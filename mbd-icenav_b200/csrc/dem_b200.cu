@@ -90,6 +90,7 @@ struct DemHandle {
     uint8_t* t_elig = nullptr;
     void* slotrec = nullptr;
     void* r3 = nullptr;
+    void* econ = nullptr;
     double* fscal = nullptr;
     unsigned long long* ptimes = nullptr;
     bool profiling = false;
@@ -335,6 +336,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     }
     a.slotrec = h->slotrec;
     a.r3 = (const T*)h->r3;
+    a.econ = (const T*)h->econ;
     a.fscal = h->fscal;
     a.ptimes = h->profiling ? h->ptimes : nullptr;
     a.in = ice_ptrs<T>(in);
@@ -597,6 +599,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->ship_tmp, es * 30))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slotrec, (es == 4 ? 16 : 32) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->r3, es * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->econ, es * 4 * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fscal, sizeof(double) * 4))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ptimes, sizeof(unsigned long long) * (2 + 2 * dem::kMaxPhaseTimes)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->sprow, es * 6))) return fail(rc);
@@ -652,6 +655,15 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
             dem::cube_kernel<float><<<blocks, 256>>>((const float*)s->radii, n, (float*)h->r3);
         else
             dem::cube_kernel<double><<<blocks, 256>>>((const double*)s->radii, n, (double*)h->r3);
+        CREATE_TRY(cudaGetLastError());
+        if (h->dtype == DEM_F32)
+            dem::econ_kernel<float><<<blocks, 256>>>((const float*)s->masses, (const float*)s->inertia,
+                                                     (const float*)s->thicknesses, (const float*)s->areas, n,
+                                                     (float*)h->econ);
+        else
+            dem::econ_kernel<double><<<blocks, 256>>>((const double*)s->masses, (const double*)s->inertia,
+                                                      (const double*)s->thicknesses, (const double*)s->areas, n,
+                                                      (double*)h->econ);
         CREATE_TRY(cudaGetLastError());
     }
     h->smem = (size_t)h->nh * 2 * es + 16;

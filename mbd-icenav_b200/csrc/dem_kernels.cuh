@@ -114,7 +114,7 @@ struct KArgs {
     int* fcoll;         // (nf) floe touched by the ship this frame
     unsigned long long* fmax;  // (nf) max force magnitude per floe (ordered bits)
     double* part;       // (nchunks * 3) per-chunk sums: soi_x, soi_y, moment
-    T* kin[2];          // (n,4) {x, y, radius, 0} of the substep being read / written
+    T* kin[2];          // (n,4) {x, y, radius, radius^3} of the substep being read / written
     T* kvel[2];         // (n,2) {vx, vy} of the substep being read / written
     int* esc_list;      // (n) escaped elements of the current detection
     int* dirty_list;    // (n) elements whose list is rebuilt
@@ -124,6 +124,7 @@ struct KArgs {
     T *sp_rot[2], *sp_avel[2];  // substep ping-pong of own-element angles
     void* slotrec;      // (2 nb) SlotRec<T>: per-frame bond slot records
     const T* r3;        // (n) radius^3 (dtype pow, once at create)
+    const T* econ;      // (n,4) {mass, inertia, thickness, area}, packed once at create
     double* fscal;      // (4) frame scalars: thrust scale, F_x, F_y, M
     unsigned long long* ptimes;  // (2 * kMaxPhaseTimes) [phase, globaltimer ns] or null
     // call arguments
@@ -180,36 +181,31 @@ __device__ __forceinline__ Frame<T> make_frame(const KArgs<T>& a, int f) {
 }
 
 // ─── grid barrier (bounded) ──────────────────────────────────────────────────
-// Returns false (and records DEM_ERR_TIMEOUT) if the wait exceeds its limit or
-// another CTA already recorded a timeout; callers then return.
+// Returns false (and records DEM_ERR_TIMEOUT) if the wait exceeds its limit;
+// callers then return.
 template <typename T>
 __device__ bool grid_barrier(const KArgs<T>& a) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned* count = a.bar;
-        unsigned* gen = a.bar + 1;
-        unsigned g = ld_acquire_u32(gen);
+        // CTA 0 adds 2^31 - (gridDim.x - 1), every other CTA adds 1: the arrivals
+        // of one barrier sum to 2^31, so bit 31 of the word flips exactly when the
+        // last CTA arrives, and the word needs no reset between barriers
+        const unsigned inc = (blockIdx.x == 0) ? 0x80000000u - (gridDim.x - 1u) : 1u;
         __threadfence();
-        unsigned arrived = atomicAdd(count, 1u) + 1u;
+        const unsigned old = atomicAdd(a.bar, inc);
         int ok = 1;
-        if (arrived == gridDim.x) {
-            atomicExch(count, 0u);
-            __threadfence();
-            st_release_u32(gen, g + 1u);
-        } else {
-            unsigned long long t0 = globaltimer_ns();
-            while (ld_acquire_u32(gen) == g) {
-                __nanosleep(40);
-                if (globaltimer_ns() - t0 > kBarrierLimitNs) {
-                    atomicMax(a.status, DEM_ERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
+        const unsigned long long t0 = globaltimer_ns();
+        while (((ld_acquire_u32(a.bar) ^ old) & 0x80000000u) == 0u) {
+            if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                // a CTA that gives up returns; every other CTA's wait then ends
+                // at its own limit, so the launch always finishes
+                atomicMax(a.status, DEM_ERR_TIMEOUT);
+                ok = 0;
+                break;
             }
         }
         __threadfence();
-        if (*((volatile int*)a.status) == DEM_ERR_TIMEOUT) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
@@ -336,6 +332,45 @@ __device__ __forceinline__ void warp_near_at(const KArgs<T>& a, int e, T px, T p
     }
 }
 
+// The same neighbourhood scan by a whole CTA (every thread must call it with
+// the same e): the stencil entries are spread over all threads, so the scan
+// takes one or two dependent load rounds instead of the warp's several.
+template <typename T, typename Fn>
+__device__ __forceinline__ void block_near_at(const KArgs<T>& a, int e, T px, T py, int2 c, Fn fn) {
+    __shared__ int s_b[9];
+    __shared__ int s_start[10];
+    if (c.x == INT_MIN) return;  // depends on e only: uniform over the CTA
+    if (threadIdx.x < 9) {
+        const int2 cc = make_int2(c.x + ((int)threadIdx.x % 3) - 1, c.y + ((int)threadIdx.x / 3) - 1);
+        const int b = bucket_of(cc, a.n_buckets);
+        s_b[threadIdx.x] = b;
+        s_start[threadIdx.x + 1] = min(a.bcnt[b], a.bucket_cap);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_start[0] = 0;
+        for (int j = 0; j < 9; ++j) s_start[j + 1] += s_start[j];
+    }
+    __syncthreads();
+    const int total = s_start[9];
+    const double re = (double)a.radii[e] + (double)a.skin;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int q = 0;
+        while (q < 8 && t >= s_start[q + 1]) ++q;
+        // entries are written after their slot is claimed: a concurrent insertion
+        // can show an old value (-1 or a valid stale index), never an invalid one
+        const int o = ((volatile const int*)a.bitems)[(size_t)s_b[q] * a.bucket_cap + (t - s_start[q])];
+        if (o < 0 || o >= a.n || o == e) continue;
+        const int2 cc = make_int2(c.x + (q % 3) - 1, c.y + (q / 3) - 1);
+        const int2 oc = a.ecell[o];
+        if (oc.x != cc.x || oc.y != cc.y) continue;  // stale entry or hash collision
+        const double ddx = (double)a.pos_ref[2 * o] - (double)px, ddy = (double)a.pos_ref[2 * o + 1] - (double)py;
+        const double lim = (re + (double)a.radii[o]) * (1.0 + 1e-5) + 1e-6;
+        if (ddx * ddx + ddy * ddy < lim * lim) fn(o);
+    }
+    __syncthreads();  // s_b / s_start are reused by the next call
+}
+
 template <typename T, typename Fn>
 __device__ __forceinline__ void warp_near(const KArgs<T>& a, int e, Fn fn) {
     warp_near_at(a, e, a.pos_ref[2 * e], a.pos_ref[2 * e + 1], a.ecell[e], fn);
@@ -370,35 +405,53 @@ __device__ void warp_build(const KArgs<T>& a, int e, int* sbuf, int* scnt) {
         if (slot < cap) sbuf[slot] = o;
     });
     __syncwarp();
-    int cnt = min(*scnt, cap);
+    const int found = *scnt;
+    const int cnt = min(found, cap);
+    // drop repeats (a stale and a current entry of one element), in parallel:
+    // entry i stays if no earlier entry holds the same index
+    constexpr int kPer = (2 * kMaxNbLocal + 31) / 32;
+    int v[kPer];
+    bool keep[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int i = lane + 32 * k;
+        v[k] = (i < cnt) ? sbuf[i] : -1;
+        keep[k] = i < cnt;
+        for (int j = 0; keep[k] && j < i; ++j)
+            if (sbuf[j] == v[k]) keep[k] = false;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+        if (lane + 32 * k < cnt && !keep[k]) sbuf[lane + 32 * k] = -1;
+    __syncwarp();
+    int nk = 0, nlow = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        nk += keep[k] ? 1 : 0;
+        nlow += (keep[k] && v[k] < e) ? 1 : 0;
+    }
+    const int w = __reduce_add_sync(0xffffffffu, nk);
+    const int split = __reduce_add_sync(0xffffffffu, nlow);  // kept indices below e
     if (lane == 0) {
-        // sort + dedup (short lists)
-        for (int i = 1; i < cnt; ++i) {
-            const int v = sbuf[i];
-            int j = i - 1;
-            while (j >= 0 && sbuf[j] > v) {
-                sbuf[j + 1] = sbuf[j];
-                --j;
-            }
-            sbuf[j + 1] = v;
-        }
-        int w = 0;
-        for (int i = 0; i < cnt; ++i)
-            if (w == 0 || sbuf[w - 1] != sbuf[i]) sbuf[w++] = sbuf[i];
-        if (*scnt > cap || w > a.max_nb) {
+        if (found > cap || w > a.max_nb) {
             atomicMax(a.status, DEM_ERR_CAPACITY);
             atomicOr((unsigned long long*)&a.stats[5], 2ull);  // a neighbour list overflowed
         }
         if (w > 16) atomicMax((unsigned long long*)&a.stats[1], (unsigned long long)w);
-        *scnt = min(w, a.max_nb);
     }
-    __syncwarp();
-    const int m = *scnt;
-    int split = 0;
-    for (int i = 0; i < m; ++i) split += (sbuf[i] < e) ? 1 : 0;
-    for (int i = lane; i < m; i += 32) {
-        const int src = (i < m - split) ? split + i : i - (m - split);
-        a.nbr[(size_t)i * a.n + e] = sbuf[src];
+    const int m = min(w, a.max_nb);
+    // slot of a kept index = its rank among the kept ones, indices above e first
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        if (!keep[k]) continue;
+        int r = 0;
+        for (int j = 0; j < cnt; ++j) {
+            const int u = sbuf[j];
+            r += (u >= 0 && u < v[k]) ? 1 : 0;
+        }
+        const int pos = (v[k] > e) ? r - split : (w - split) + r;
+        if (pos < m) a.nbr[(size_t)pos * a.n + e] = v[k];
     }
     if (lane == 0) a.ncnt[e] = m;
     __syncwarp();
@@ -416,21 +469,18 @@ __device__ __forceinline__ void mark_dirty(const KArgs<T>& a, int o, int s, unsi
     if (atomicExch(&a.dirty[o], round) != round) a.dirty_list[atomicAdd(&a.dirty_cnt[s], 1)] = o;
 }
 
-// One rebuild round before substep s, one warp per escaped element: the
+// One rebuild round before substep s, one CTA per escaped element: the
 // element takes its current position as reference and is appended to its new
 // home bucket; it and every element within reach of its new reference need a
 // new list (skipped when most elements escaped: every list is then rebuilt).
-// Runs concurrently with insertions by other warps: marking only needs the
+// Runs concurrently with insertions by other CTAs: marking only needs the
 // references of elements that did not escape, which do not move.
 template <typename T>
 __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int s, unsigned round, bool all) {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int q = warp; q < (int)cnt; q += nwarps) {
+    for (int q = blockIdx.x; q < (int)cnt; q += gridDim.x) {
         const int e = a.esc_list[q];
         const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-        if (lane == 0) {
+        if (threadIdx.x == 0) {
             const int2 old = a.ecell[e];
             if (old.x != INT_MIN) queue_bucket(a, bucket_of(old, a.n_buckets));
             a.pos_ref[2 * e] = px;
@@ -442,8 +492,8 @@ __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int 
         if (all) continue;
         const bool fin = jfinite(px) && jfinite(py);
         const int2 c = fin ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
-        warp_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
-        if (lane == 0) mark_dirty(a, e, s, round);
+        block_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
+        if (threadIdx.x == 0) mark_dirty(a, e, s, round);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd((unsigned long long*)&a.stats[0], 1ull);
@@ -1019,7 +1069,7 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
         k4.x = p.x;
         k4.y = p.y;
         k4.z = a.radii[e];
-        k4.w = T(0);
+        k4.w = a.r3[e];
         reinterpret_cast<typename vec4_of<T>::type*>(a.kin[0])[e] = k4;
         st2(a.kvel[0], e, v.x, v.y);
     }
@@ -1052,7 +1102,10 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
 // the loads of a batch are issued before any of them is used.
 // Contact distances and every predicate are computed unfused (-fmad=false);
 // force values use explicit fma where the reference's products are summed.
-constexpr int kBatch = 4;
+#ifndef DEM_KBATCH
+#define DEM_KBATCH 2
+#endif
+constexpr int kBatch = DEM_KBATCH;  // bond slots / contact candidates whose loads are issued together
 
 
 __device__ __forceinline__ float jfma(float a, float b, float c) { return fmaf(a, b, c); }
@@ -1108,42 +1161,72 @@ __device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<
 
 // Forces, torque and the semi-implicit update of element e for one substep;
 // returns whether e escaped its reference ball.
+//
+// Latency layout: every load that depends only on e is issued first; then one
+// loop walks the bond slots and the contact candidates together, kBatch of
+// each per iteration, issuing the slot records and candidate indices of a
+// batch at once, then all partner gathers at once.  Bond and contact sums keep
+// separate accumulators, each in the reference's order (bond slots with
+// e == bond_i first, then e == bond_j; candidates above e ascending, then
+// below e ascending), so the interleaving does not change any rounding.
 template <typename T>
 __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
                                               int e) {
     typedef typename vec2_of<T>::type V2;
     typedef typename vec4_of<T>::type V4;
     const T *kin = cx.kin, *kvin = cx.kvin;
-    const uint8_t* act = cx.act;
     const SlotRec<T>* rec = cx.rec;
-    const T hf = cx.hf, hexp = cx.hexp, mu = cx.mu, fcap = cx.fcap, c_drag = cx.c_drag, href = cx.href;
-    const T lin = cx.lin, c_rot = cx.c_rot, dti = cx.dti, damp = cx.damp, alo = cx.alo, ahi = cx.ahi;
-    const T vclip = cx.vclip, pclip = cx.pclip;
+    const T hf = cx.hf, hexp = cx.hexp, mu = cx.mu, fcap = cx.fcap;
     const bool h15 = cx.h15, last = cx.last;
-    const V4 ke = ld4(kin, e);  // x, y, radius
+    // loads that depend on e only
+    const V4 ke = ld4(kin, e);  // x, y, radius, radius^3
     const V2 ve = ld2(kvin, e);
-    const bool ae = act[e] != 0;
-    // bond forces (jax_simulation.py:63-108): slots with e == bond_i first, then e == bond_j
-    T fbx = T(0), fby = T(0), mb = T(0);
+    const bool ae = cx.act[e] != 0;
     const int s0 = a.boff[e], s1 = a.boff[e + 1];
-    for (int base = s0; base < s1; base += kBatch) {
+    const int nc = a.ncnt[e];
+    const V4 ec = ld4(a.econ, e);  // mass, inertia, thickness, area
+    const V2 w = ld2(F.vw, e);
+    const T sub = F.dst.sub[e];
+    const V2 so = ld2(a.soi, e);
+    const T av = cx.ain[e];
+    const T rot = cx.rin[e];
+    const T re = ke.z;
+    // bonds (jax_simulation.py:63-108) and ice-ice contacts (:111-164)
+    T fbx = T(0), fby = T(0), mb = T(0);
+    T fix = T(0), fiy = T(0), mi = T(0);
+    const int nbe = s1 - s0;
+    const int iters = max((nbe + kBatch - 1) / kBatch, (nc + kBatch - 1) / kBatch);
+    for (int it = 0; it < iters; ++it) {
+        const int bb = s0 + it * kBatch, cb = it * kBatch;
         SlotRec<T> r[kBatch];
-        V4 ko[kBatch];
+        int idx[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
-            if (base + j < s1) {
-                r[j] = rec[base + j];
-                ko[j] = ld4(kin, r[j].o & 0x7fffffff);
+            if (bb + j < s1) {
+                r[j] = rec[bb + j];
             } else {
+                r[j].o = 0;
                 r[j].omd = T(-1);
+            }
+            idx[j] = (cb + j < nc) ? a.nbr[(size_t)(cb + j) * a.n + e] : -1;
+        }
+        V2 kb[kBatch];
+        V4 ko[kBatch];
+        V2 vo[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+            if (r[j].omd >= T(0)) kb[j] = reinterpret_cast<const V2*>(kin)[2 * (r[j].o & 0x7fffffff)];
+            if (idx[j] >= 0) {
+                ko[j] = ld4(kin, idx[j]);
+                vo[j] = ld2(kvin, idx[j]);
             }
         }
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
-            if (r[j].omd < T(0)) continue;  // broken, or active/frozen endpoints
+            if (r[j].omd < T(0)) continue;  // no slot, broken, or active/frozen endpoints
             const bool role_j = r[j].o < 0;
-            const T dx = role_j ? ke.x - ko[j].x : ko[j].x - ke.x;
-            const T dy = role_j ? ke.y - ko[j].y : ko[j].y - ke.y;
+            const T dx = role_j ? ke.x - kb[j].x : kb[j].x - ke.x;
+            const T dy = role_j ? ke.y - kb[j].y : kb[j].y - ke.y;
             const T dist = jsqrt(dx * dx + dy * dy);
             const T inv = jrcp(jmax(dist, T(1e-10)));
             const T fmag = r[j].stiff * (dist - r[j].rest) * r[j].omd;
@@ -1159,23 +1242,6 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
                 mb -= cr;
             }
         }
-    }
-    // ice-ice contact (jax_simulation.py:111-164).  Pass 1 evaluates the exact
-    // contact predicate for every candidate and records the overlapping ones
-    // in a bit mask; pass 2 computes forces for those only, in list order, so
-    // a warp runs the force math max(#overlaps) times, not max(#candidates).
-    T fix = T(0), fiy = T(0), mi = T(0);
-    const T re = ke.z;
-    const int nc = a.ncnt[e];
-    unsigned long long ovm = 0ull;  // max_neighbors <= 64
-    for (int base = 0; base < nc; base += kBatch) {
-        int idx[kBatch];
-        V4 ko[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) idx[j] = (base + j < nc) ? a.nbr[(size_t)(base + j) * a.n + e] : -1;
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j)
-            if (idx[j] >= 0) ko[j] = ld4(kin, idx[j]);
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
             const int o = idx[j];
@@ -1183,85 +1249,73 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
             const bool e_is_i = e < o;
             const T dx = e_is_i ? ko[j].x - ke.x : ke.x - ko[j].x;
             const T dy = e_is_i ? ko[j].y - ke.y : ke.y - ko[j].y;
-            // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
-            const T dist = jsqrt(dx * dx + dy * dy);
+            const T d2 = dx * dx + dy * dy;
             const T min_dist = e_is_i ? re + ko[j].z : ko[j].z + re;
+            // d2 > (min_dist (1 + 1e-5))^2, all roundings included, puts the rounded
+            // square root above min_dist, where the reference's overlap is exactly
+            // 0: such candidates skip the square root (NaN falls through)
+            const T mdm = min_dist * T(1.00001);
+            if (d2 > mdm * mdm) continue;
+            // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
+            const T dist = jsqrt(d2);
             const T overlap = jmax(min_dist - dist, T(0));
-            if ((dist > T(1e-6)) && (overlap > T(0))) ovm |= 1ull << (base + j);
-        }
-    }
-    while (ovm) {
-        const int q = __ffsll((long long)ovm) - 1;
-        ovm &= ovm - 1ull;
-        const int o = a.nbr[(size_t)q * a.n + e];
-        const V4 ko = ld4(kin, o);
-        const V2 vo = ld2(kvin, o);
-        const bool e_is_i = e < o;
-        const T dx = e_is_i ? ko.x - ke.x : ke.x - ko.x;
-        const T dy = e_is_i ? ko.y - ke.y : ke.y - ko.y;
-        const T dist = jsqrt(dx * dx + dy * dy);
-        const T min_dist = e_is_i ? re + ko.z : ko.z + re;
-        const T overlap = min_dist - dist;
-        const T inv = jrcp(dist);  // dist > 1e-6 here
-        const T ux = dx * inv, uy = dy * inv;
-        const T fn = hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, hexp));
-        const T fnx = ux * fn, fny = uy * fn;
-        const T vrx = e_is_i ? vo.x - ve.x : ve.x - vo.x;
-        const T vry = e_is_i ? vo.y - ve.y : ve.y - vo.y;
-        const T vdot = jfma(vrx, ux, vry * uy);
-        const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
-        const T vtm = jsqrt(vtx * vtx + vty * vty);
-        T ftx = T(0), fty = T(0);
-        if (vtm > T(1e-6)) {
-            const T ftm = jmin(mu * fn, fcap) * jrcp(vtm);
-            ftx = -vtx * ftm;
-            fty = -vty * ftm;
-        }
-        const T oix = -fnx - ftx, oiy = -fny - fty;
-        const T cr = -jfma(dx, oiy, -(dy * oix));
-        if (e_is_i) {
-            fix += ftx - fnx;
-            fiy += fty - fny;
-            mi += T(0.5) * cr;
-        } else {
-            fix += fnx - ftx;
-            fiy += fny - fty;
-            mi -= T(0.5) * cr;
+            if (!((dist > T(1e-6)) && (overlap > T(0)))) continue;
+            const T inv = jrcp(dist);
+            const T ux = dx * inv, uy = dy * inv;
+            const T fn = hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, hexp));
+            const T fnx = ux * fn, fny = uy * fn;
+            const T vrx = e_is_i ? vo[j].x - ve.x : ve.x - vo[j].x;
+            const T vry = e_is_i ? vo[j].y - ve.y : ve.y - vo[j].y;
+            const T vdot = jfma(vrx, ux, vry * uy);
+            const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
+            const T vtm = jsqrt(vtx * vtx + vty * vty);
+            T ftx = T(0), fty = T(0);
+            if (vtm > T(1e-6)) {
+                const T ftm = jmin(mu * fn, fcap) * jrcp(vtm);
+                ftx = -vtx * ftm;
+                fty = -vty * ftm;
+            }
+            const T oix = -fnx - ftx, oiy = -fny - fty;
+            const T cr = -jfma(dx, oiy, -(dy * oix));
+            if (e_is_i) {
+                fix += ftx - fnx;
+                fiy += fty - fny;
+                mi += T(0.5) * cr;
+            } else {
+                fix += fnx - ftx;
+                fiy += fny - fty;
+                mi -= T(0.5) * cr;
+            }
         }
     }
     // drag (jax_simulation.py:167-192)
-    const T h = a.thick[e], A = a.areas[e];
-    const T a_drag = A * (h / href);
-    const V2 w = ld2(F.vw, e);
+    const T m = ec.x, inertia = ec.y, h = ec.z, A = ec.w;
+    const T a_drag = A * (h / cx.href);
     const T vrx = ve.x - w.x, vry = ve.y - w.y;
     const T vm = jsqrt(vrx * vrx + vry * vry);
     T fdx, fdy;
     if (vm > T(1e-6)) {
-        const T q = c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
+        const T q = cx.c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
         fdx = vrx * q;
         fdy = vry * q;
     } else {
-        const T cl = c_drag * a_drag * lin;
+        const T cl = cx.c_drag * a_drag * cx.lin;
         fdx = cl * vrx;
         fdy = cl * vry;
     }
     // rotational drag (jax_simulation.py:195-212)
-    const T av = cx.ain[e];
-    const T sub = F.dst.sub[e];
     const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
-    const T md = c_rot * a.r3[e] * av * fabs(av) * a_sub;
-    const V2 so = ld2(a.soi, e);
+    const T md = cx.c_rot * ke.w * av * fabs(av) * a_sub;
     const T Fx = ((fbx + fix) - fdx) + so.x;
     const T Fy = ((fby + fiy) - fdy) + so.y;
     const T Mz = (mb + mi) + md;
     // semi-implicit Euler (jax_simulation.py:215-268)
-    const T m = a.mass[e];
+    const T dti = cx.dti, vclip = cx.vclip, pclip = cx.pclip;
     T nvx = jclip(ve.x + (Fx / m) * dti, -vclip, vclip);
     T nvy = jclip(ve.y + (Fy / m) * dti, -vclip, vclip);
     T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
-    const T alpha = Mz / a.inertia[e];
-    T nav = jclip(av * damp + alpha * dti, alo, ahi);
-    const T rot = cx.rin[e];
+    const T alpha = Mz / inertia;
+    T nav = jclip(av * cx.damp + alpha * dti, cx.alo, cx.ahi);
     T nrot = rot + nav * dti;
     if (!jfinite(nvx)) nvx = T(0);
     if (!jfinite(nvy)) nvy = T(0);
@@ -1281,12 +1335,12 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
         st2(F.dst.pos, e, npx, npy);
         st2(F.dst.vel, e, nvx, nvy);
     } else {
-        typename vec4_of<T>::type v4;
+        V4 v4;
         v4.x = npx;
         v4.y = npy;
         v4.z = re;
-        v4.w = T(0);
-        reinterpret_cast<typename vec4_of<T>::type*>(cx.kout)[e] = v4;
+        v4.w = ke.w;
+        reinterpret_cast<V4*>(cx.kout)[e] = v4;
         st2(cx.kvout, e, nvx, nvy);
     }
     cx.rout[e] = nrot;
@@ -1530,6 +1584,17 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
             }
         }
     }
+}
+
+// per-element constants packed for one vector load per substep
+template <typename T>
+__global__ void econ_kernel(const T* mass, const T* inertia, const T* thick, const T* area, int n, T* out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    out[4 * (size_t)e + 0] = mass[e];
+    out[4 * (size_t)e + 1] = inertia[e];
+    out[4 * (size_t)e + 2] = thick[e];
+    out[4 * (size_t)e + 3] = area[e];
 }
 
 // r^3 per element in the dtype (radii ** 3, jax_simulation.py:205)
