@@ -43,6 +43,15 @@ constexpr int kMaxPhaseTimes = 4096;
 // Phases of one frame: cull, near contact, contact forces, reduce, then per
 // substep escape round, all-lists rebuild and force, and last fracture.
 __host__ __device__ constexpr int phases_per_frame(int k_sub) { return 5 + 3 * k_sub; }
+// work items per thread and step whose loads are issued together in the
+// per-frame bond-record build and in the fracture update (more than one adds
+// registers that the force loop then spills)
+#ifndef DEM_SLOT_BATCH
+#define DEM_SLOT_BATCH 1
+#endif
+#ifndef DEM_FRACTURE_BATCH
+#define DEM_FRACTURE_BATCH 1
+#endif
 #ifndef DEM_MIN_BLOCKS
 #define DEM_MIN_BLOCKS 2  // resident CTAs per SM the register allocation targets
 #endif
@@ -469,31 +478,52 @@ __device__ __forceinline__ void mark_dirty(const KArgs<T>& a, int o, int s, unsi
     if (atomicExch(&a.dirty[o], round) != round) a.dirty_list[atomicAdd(&a.dirty_cnt[s], 1)] = o;
 }
 
-// One rebuild round before substep s, one CTA per escaped element: the
-// element takes its current position as reference and is appended to its new
-// home bucket; it and every element within reach of its new reference need a
-// new list (skipped when most elements escaped: every list is then rebuilt).
-// Runs concurrently with insertions by other CTAs: marking only needs the
-// references of elements that did not escape, which do not move.
+// One rebuild round before substep s.  Work items 0..cnt-1 (one CTA each)
+// stamp dirty every element within reach of an escaped element's new
+// reference, and the element itself; items cnt..2cnt-1 (one thread each)
+// re-reference the escaped element and append it to its new home bucket.  The
+// two run concurrently: marking only needs the new position (from the packed
+// kinematics) and the references of elements that did not escape, which do
+// not move.  Marking is skipped when most elements escaped (every list is
+// then rebuilt).
 template <typename T>
 __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int s, unsigned round, bool all) {
-    for (int q = blockIdx.x; q < (int)cnt; q += gridDim.x) {
-        const int e = a.esc_list[q];
+    const int items = all ? (int)cnt : 2 * (int)cnt;
+    for (int q = blockIdx.x; q < items; q += gridDim.x) {
+        const bool reref = all || q >= (int)cnt;
+        const int e = a.esc_list[reref && !all ? q - (int)cnt : q];
         const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-        if (threadIdx.x == 0) {
-            const int2 old = a.ecell[e];
-            if (old.x != INT_MIN) queue_bucket(a, bucket_of(old, a.n_buckets));
-            a.pos_ref[2 * e] = px;
-            a.pos_ref[2 * e + 1] = py;
-            grid_put(a, e, px, py);
-            const int2 nw = a.ecell[e];
-            if (nw.x != INT_MIN) queue_bucket(a, bucket_of(nw, a.n_buckets));
-        }
-        if (all) continue;
         const bool fin = jfinite(px) && jfinite(py);
         const int2 c = fin ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
-        block_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
-        if (threadIdx.x == 0) mark_dirty(a, e, s, round);
+        if (!reref) {
+            block_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
+            if (threadIdx.x == 0) mark_dirty(a, e, s, round);
+            continue;
+        }
+        if (threadIdx.x != 0) continue;
+        // old and new buckets are queued for compaction at the next frame
+        // start; the independent atomics of each level are issued together
+        const int2 old = a.ecell[e];
+        a.pos_ref[2 * e] = px;
+        a.pos_ref[2 * e + 1] = py;
+        a.ecell[e] = c;
+        const int bo = (old.x != INT_MIN) ? bucket_of(old, a.n_buckets) : -1;
+        const int bn = (c.x != INT_MIN) ? bucket_of(c, a.n_buckets) : -1;
+        const int slot = (bn >= 0) ? atomicAdd(&a.bcnt[bn], 1) : 0;
+        const int fo = (bo >= 0) ? atomicExch(&a.bflag[bo], 1) : 1;
+        const int fn = (bn >= 0 && bn != bo) ? atomicExch(&a.bflag[bn], 1) : 1;
+        if (bn >= 0) {
+            if (slot < a.bucket_cap) {
+                a.bitems[(size_t)bn * a.bucket_cap + slot] = e;
+            } else {
+                atomicMax(a.status, DEM_ERR_CAPACITY);
+                atomicOr((unsigned long long*)&a.stats[5], 1ull);  // a grid bucket overflowed
+            }
+            if (slot + 1 > a.bucket_cap / 2)
+                atomicMax((unsigned long long*)&a.stats[2], (unsigned long long)(slot + 1));
+        }
+        if (fo == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = bo;
+        if (fn == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = bn;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd((unsigned long long*)&a.stats[0], 1ull);
@@ -517,27 +547,44 @@ __device__ void phase_build_all(const KArgs<T>& a) {
 // reads or writes the grid).
 template <typename T>
 __device__ void compact_buckets(const KArgs<T>& a) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
+    // one warp per queued bucket: lanes test 32 entries at a time; an entry
+    // stays if it is current (its home cell hashes here) and no earlier entry
+    // holds the same element; kept entries move to the front in their order
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nq = *((volatile int*)a.comp_cnt);
-    for (int i = gtid; i < nq; i += gsz) {
+    for (int i = warp; i < nq; i += nwarps) {
         const int b = a.comp_list[i];
         const int m = min(a.bcnt[b], a.bucket_cap);
         int* it = a.bitems + (size_t)b * a.bucket_cap;
         int w = 0;
-        for (int k = 0; k < m; ++k) {
-            const int o = it[k];
-            if (o < 0 || o >= a.n) continue;
-            const int2 c = a.ecell[o];
-            if (c.x == INT_MIN || bucket_of(c, a.n_buckets) != b) continue;
-            bool dup = false;
-            for (int q = 0; q < w; ++q)
-                if (it[q] == o) dup = true;
-            if (!dup) it[w++] = o;
+        for (int k0 = 0; k0 < m; k0 += 32) {
+            const int k = k0 + lane;
+            const int o = (k < m) ? it[k] : -1;
+            bool keep = false;
+            if (o >= 0 && o < a.n) {
+                const int2 c = a.ecell[o];
+                keep = c.x != INT_MIN && bucket_of(c, a.n_buckets) == b;
+            }
+            for (int q = 0; keep && q < w; ++q)  // kept in earlier chunks
+                if (it[q] == o) keep = false;
+            for (int j = 0; j < 32; ++j) {       // earlier lanes of this chunk
+                const int oj = __shfl_sync(0xffffffffu, o, j);
+                const bool kj = __shfl_sync(0xffffffffu, keep, j);
+                if (j < lane && kj && oj == o) keep = false;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            __syncwarp();  // every lane has read its entry before any is overwritten
+            if (keep) it[w + __popc(bal & ((1u << lane) - 1u))] = o;
+            w += __popc(bal);
+            __syncwarp();
         }
-        for (int k = w; k < m; ++k) it[k] = -1;
-        a.bcnt[b] = w;
-        a.bflag[b] = 0;
+        for (int k = w + lane; k < m; k += 32) it[k] = -1;
+        if (lane == 0) {
+            a.bcnt[b] = w;
+            a.bflag[b] = 0;
+        }
     }
 }
 
@@ -1057,8 +1104,12 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             }
         }
     }
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
+    // CTA 0 runs the vessel step above; the other CTAs share the element and
+    // slot work (all CTAs when the grid has one)
+    const int c0 = (gridDim.x > 1) ? 1 : 0;
+    if ((int)blockIdx.x < c0) return;
+    const int gtid = (blockIdx.x - c0) * blockDim.x + threadIdx.x;
+    const int gsz = (gridDim.x - c0) * blockDim.x;
     for (int e = gtid; e < a.n; e += gsz) {
         // activation (jax_simulation.py:498-509)
         const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
@@ -1073,24 +1124,53 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
         reinterpret_cast<typename vec4_of<T>::type*>(a.kin[0])[e] = k4;
         st2(a.kvel[0], e, v.x, v.y);
     }
-    // bond slot records for this frame, one thread per slot; crack front =
-    // element touches a bond that is broken at frame start
+    // bond slot records for this frame; crack front = element touches a bond
+    // that is broken at frame start.  Four slots per thread and step, their
+    // loads issued level by level (slot -> endpoints -> floe flags).
     SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
-    for (int sl = gtid; sl < 2 * a.nb; sl += gsz) {
-        const int e = a.slot_owner[sl];
-        const int2 ent = a.bslot[sl];
-        const int b = ent.x & 0x7fffffff;
-        const int o = ent.y;
-        const bool in = F.src.intact[b] != 0;
-        if (!in) a.crack[e] = 1;
-        const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
-        const bool ao = F.src.active[o] || a.fcoll[a.floe_of[o]];
-        SlotRec<T> r;
-        r.o = (ent.x < 0) ? (int)((unsigned)o | 0x80000000u) : o;
-        r.rest = a.slot_rest[sl];
-        r.stiff = a.slot_stiff[sl];
-        r.omd = (in && ao == ae) ? T(1) - F.src.dmg[b] : T(-1);
-        rec[sl] = r;
+    const int nsl = 2 * a.nb;
+    constexpr int kS = DEM_SLOT_BATCH;
+    for (int base = gtid; base < nsl; base += kS * gsz) {
+        int sl[kS], e[kS];
+        int2 ent[kS];
+#pragma unroll
+        for (int k = 0; k < kS; ++k) {
+            sl[k] = base + k * gsz;
+            if (sl[k] < nsl) {
+                e[k] = a.slot_owner[sl[k]];
+                ent[k] = a.bslot[sl[k]];
+            }
+        }
+        bool in[kS], sae[kS], sao[kS];
+        int fe[kS], fo[kS];
+        T dmg[kS], rest[kS], stiff[kS];
+#pragma unroll
+        for (int k = 0; k < kS; ++k) {
+            if (sl[k] >= nsl) continue;
+            const int b = ent[k].x & 0x7fffffff, o = ent[k].y;
+            in[k] = F.src.intact[b] != 0;
+            sae[k] = F.src.active[e[k]] != 0;
+            sao[k] = F.src.active[o] != 0;
+            fe[k] = a.floe_of[e[k]];
+            fo[k] = a.floe_of[o];
+            dmg[k] = F.src.dmg[b];
+            rest[k] = a.slot_rest[sl[k]];
+            stiff[k] = a.slot_stiff[sl[k]];
+        }
+#pragma unroll
+        for (int k = 0; k < kS; ++k) {
+            if (sl[k] >= nsl) continue;
+            if (!in[k]) a.crack[e[k]] = 1;
+            const bool ae = sae[k] || a.fcoll[fe[k]];
+            const bool ao = sao[k] || a.fcoll[fo[k]];
+            const int o = ent[k].y;
+            SlotRec<T> r;
+            r.o = (ent[k].x < 0) ? (int)((unsigned)o | 0x80000000u) : o;
+            r.rest = rest[k];
+            r.stiff = stiff[k];
+            r.omd = (in[k] && ao == ae) ? T(1) - dmg[k] : T(-1);
+            rec[sl[k]] = r;
+        }
     }
 }
 
@@ -1454,59 +1534,103 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
     const T esc = T(P.effective_strength_collision);
     const T dti = T(P.dt_ice);
     const T kn = a.k_n, ks = a.k_s;
-    for (int b = gtid; b < a.nb; b += gsz) {
-        int i = a.bi[b], j = a.bj[b];
-        typename vec2_of<T>::type pi_ = ld2(F.dst.pos, i), pj = ld2(F.dst.pos, j);
-        T dx = pj.x - pi_.x, dy = pj.y - pi_.y;
-        T dist = jsqrt(dx * dx + dy * dy);
-        T dsafe = jmax(dist, T(1e-10));
-        T bx = dx / dsafe, by = dy / dsafe;
-        bool both_act = F.dst.active[i] && F.dst.active[j];
-        bool floe_ok = new_elig(a, F, a.floe_of[i], scale) && new_elig(a, F, a.floe_of[j], scale);
-        bool breakable = (a.thick[i] <= mft) && (a.thick[j] <= mft);
-        T fmi = a.fraw[i] * scale, fmj = a.fraw[j] * scale;
-        bool near = (fmi > T(0)) || (fmj > T(0));
-        bool at_crack = a.crack[i] || a.crack[j];
-        bool dpdem_ok = both_act && floe_ok && (near || at_crack) && breakable;
-        typename vec2_of<T>::type vi = ld2(F.dst.vel, i), vj = ld2(F.dst.vel, j);
-        T vrx = vj.x - vi.x, vry = vj.y - vi.y;
-        T vn = vrx * bx + vry * by;
-        T vtx = vrx - vn * bx, vty = vry - vn * by;
-        T ds_incr = jsqrt(vtx * vtx + vty * vty) * dti;
-        bool ds_gate = near && both_act && floe_ok && breakable;
-        T new_ds = F.src.ds[b] + (ds_gate ? ds_incr : T(0));
-        T rest = a.rest[b];
-        T L0 = jmax(rest, T(1e-10));
-        T delta_n = dist - rest;
-        T dn_d = near ? delta_n : T(0);
-        T cur_d = F.src.dmg[b];
-        T sn = (kn * (dn_d / L0)) * (T(1) - cur_d);
-        T st = (ks * (new_ds / L0)) * (T(1) - cur_d);
-        bool intact = F.src.intact[b] != 0;
-        T od = cur_d, omax = F.src.dmmax[b], o0 = F.src.dm0[b];
-        bool fin = intact;
-        if (dpdem_ok) {
-            // the damage law's result is only selected for DPDEM-eligible bonds
-            // (jnp.where at jax_simulation.py:620-623); elsewhere the old state stays
-            T nd, nmax, n0;
-            bool nint;
-            bond_damage<T>(P, delta_n, new_ds, sn, st, a.sbar[b], cur_d, omax, o0, intact, nd, nmax, n0, nint);
-            od = nd;
-            omax = nmax;
-            o0 = n0;
-            if (breakable) fin = nint;
+    // two bonds per thread and step: every load of both (bond -> endpoints ->
+    // floe flags) is issued before any store
+    typedef typename vec2_of<T>::type V2;
+    constexpr int kB = DEM_FRACTURE_BATCH;
+    for (int base = gtid; base < a.nb; base += kB * gsz) {
+        int bb[kB], ii[kB], jj[kB];
+        bool ok[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            bb[k] = base + k * gsz;
+            ok[k] = bb[k] < a.nb;
+            ii[k] = ok[k] ? a.bi[bb[k]] : 0;
+            jj[k] = ok[k] ? a.bj[bb[k]] : 0;
         }
-        // direct collision breaking (jax_simulation.py:629-637)
-        bool coll_on = (fmi > T(0)) || (fmj > T(0));
-        T coll_f = jmax(fmi, fmj);
-        bool brk = intact && coll_on && (coll_f > a.bstr[b] * esc) && breakable;
-        fin = fin && !brk;
-        F.dst.dmg[b] = od;
-        F.dst.dmmax[b] = omax;
-        F.dst.dm0[b] = o0;
-        F.dst.ds[b] = new_ds;
-        F.dst.intact[b] = fin ? 1 : 0;
-        if (a.h_intact) a.h_intact[(size_t)F.f * a.nb + b] = fin ? 1 : 0;
+        V2 pi[kB], pj[kB], vi[kB], vj[kB];
+        bool both_act[kB], breakable[kB], at_crack[kB], intact[kB];
+        int fli[kB], flj[kB];
+        T fmi[kB], fmj[kB], ds0[kB], rest[kB], cur_d[kB], dmmax0[kB], dm00[kB], sbar[kB], bstr[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            if (!ok[k]) continue;
+            const int i = ii[k], j = jj[k], b = bb[k];
+            pi[k] = ld2(F.dst.pos, i);
+            pj[k] = ld2(F.dst.pos, j);
+            vi[k] = ld2(F.dst.vel, i);
+            vj[k] = ld2(F.dst.vel, j);
+            both_act[k] = F.dst.active[i] && F.dst.active[j];
+            fli[k] = a.floe_of[i];
+            flj[k] = a.floe_of[j];
+            breakable[k] = (a.thick[i] <= mft) && (a.thick[j] <= mft);
+            fmi[k] = a.fraw[i] * scale;
+            fmj[k] = a.fraw[j] * scale;
+            at_crack[k] = a.crack[i] || a.crack[j];
+            ds0[k] = F.src.ds[b];
+            rest[k] = a.rest[b];
+            cur_d[k] = F.src.dmg[b];
+            intact[k] = F.src.intact[b] != 0;
+            dmmax0[k] = F.src.dmmax[b];
+            dm00[k] = F.src.dm0[b];
+            sbar[k] = a.sbar[b];
+            bstr[k] = a.bstr[b];
+        }
+        bool floe_ok[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            if (!ok[k]) continue;
+            const bool ei = new_elig(a, F, fli[k], scale);
+            const bool ej = new_elig(a, F, flj[k], scale);
+            floe_ok[k] = ei && ej;
+        }
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            if (!ok[k]) continue;
+            const int b = bb[k];
+            T dx = pj[k].x - pi[k].x, dy = pj[k].y - pi[k].y;
+            T dist = jsqrt(dx * dx + dy * dy);
+            T dsafe = jmax(dist, T(1e-10));
+            T bx = dx / dsafe, by = dy / dsafe;
+            bool near = (fmi[k] > T(0)) || (fmj[k] > T(0));
+            bool dpdem_ok = both_act[k] && floe_ok[k] && (near || at_crack[k]) && breakable[k];
+            T vrx = vj[k].x - vi[k].x, vry = vj[k].y - vi[k].y;
+            T vn = vrx * bx + vry * by;
+            T vtx = vrx - vn * bx, vty = vry - vn * by;
+            T ds_incr = jsqrt(vtx * vtx + vty * vty) * dti;
+            bool ds_gate = near && both_act[k] && floe_ok[k] && breakable[k];
+            T new_ds = ds0[k] + (ds_gate ? ds_incr : T(0));
+            T L0 = jmax(rest[k], T(1e-10));
+            T delta_n = dist - rest[k];
+            T dn_d = near ? delta_n : T(0);
+            T sn = (kn * (dn_d / L0)) * (T(1) - cur_d[k]);
+            T st = (ks * (new_ds / L0)) * (T(1) - cur_d[k]);
+            T od = cur_d[k], omax = dmmax0[k], o0 = dm00[k];
+            bool fin = intact[k];
+            if (dpdem_ok) {
+                // the damage law's result is only selected for DPDEM-eligible bonds
+                // (jnp.where at jax_simulation.py:620-623); elsewhere the old state stays
+                T nd, nmax, n0;
+                bool nint;
+                bond_damage<T>(P, delta_n, new_ds, sn, st, sbar[k], cur_d[k], omax, o0, intact[k], nd, nmax, n0,
+                               nint);
+                od = nd;
+                omax = nmax;
+                o0 = n0;
+                if (breakable[k]) fin = nint;
+            }
+            // direct collision breaking (jax_simulation.py:629-637)
+            bool coll_on = (fmi[k] > T(0)) || (fmj[k] > T(0));
+            T coll_f = jmax(fmi[k], fmj[k]);
+            bool brk = intact[k] && coll_on && (coll_f > bstr[k] * esc) && breakable[k];
+            fin = fin && !brk;
+            F.dst.dmg[b] = od;
+            F.dst.dmmax[b] = omax;
+            F.dst.dm0[b] = o0;
+            F.dst.ds[b] = new_ds;
+            F.dst.intact[b] = fin ? 1 : 0;
+            if (a.h_intact) a.h_intact[(size_t)F.f * a.nb + b] = fin ? 1 : 0;
+        }
     }
     for (int e = gtid; e < a.n; e += gsz) {
         if (a.h_pos) {
