@@ -200,6 +200,28 @@ def build_stepper(field, dtype_name: str, device, bucket_capacity: int = 64, ski
     return fs, st, sh, static
 
 
+def max_over_ranks(seconds: float, world: int, device) -> float:
+    """The slowest rank's time: every rank calls this with its own timed seconds."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def retry_verdict(rc: int, grown: bool, world: int, device) -> int:
+    """One decision for all ranks after a timed region: 0 = every rank clean,
+    1 = some rank grew its capacity (all ranks time the region again),
+    2 = some rank failed for good (all ranks stop)."""
+    import torch
+    import torch.distributed as dist
+    v = torch.tensor([0.0 if rc == 0 else (1.0 if grown else 2.0)], device=device)
+    if world > 1:
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    return int(v.item())
+
+
 def run_ours(args, rank: int, world: int):
     import numpy as np
     import torch
@@ -253,21 +275,16 @@ def run_ours(args, rank: int, world: int):
         rc = fs.lib.dem_sync_status(fs._h, fs._stream())
         msg = fs._error() if rc != 0 else ""
         grown = rc == _abi_mod().DEM_ERR_CAPACITY and attempt < 3 and fs.grow_capacity()
-        verdict = torch.tensor([0.0 if rc == 0 else (1.0 if grown else 2.0)], device=device)
-        if world > 1:
-            dist.all_reduce(verdict, op=dist.ReduceOp.MAX)
-        if float(verdict.item()) == 0.0:
+        verdict = retry_verdict(rc, grown, world, device)
+        if verdict == 0:
             break
-        if float(verdict.item()) == 2.0:
+        if verdict == 2:
             raise RuntimeError(f"device status {rc}: {msg}" if rc else "device error on another rank")
     if world > 1:
         dist.barrier()
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_s = sum(frame_ms) / 1e3
-    t = torch.tensor([total_s], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_max = float(t.item())
+    total_max = max_over_ranks(total_s, world, device)
     value = world * n * N_SUB * K / total_max
 
     # end to end through the public API with host buffers
@@ -297,10 +314,7 @@ def run_ours(args, rank: int, world: int):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_s = e0.elapsed_time(e1) / 1e3
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * N_SUB * E / float(t.item())
+    e2e_value = world * n * N_SUB * E / max_over_ranks(e2e_s, world, device)
     rc = fs.lib.dem_sync_status(fs._h, fs._stream())
     if rc != 0:
         raise RuntimeError(f"device status {rc}: {fs._error()}")

@@ -221,6 +221,14 @@ int dem_set_profiling(DemHandle* h, int32_t on);
  * no entry. */
 int dem_get_phase_times(DemHandle* h, int64_t* pairs, int32_t max_pairs, int32_t* count, int64_t* start_ns);
 
+/* Failure-detection test hook (no reference counterpart): in the next
+ * persistent call on this handle, the last CTA leaves instead of arriving at
+ * the grid barrier that follows phase `phase`.  Every other CTA's wait then
+ * ends at its time limit (2 s), the call's status becomes DEM_ERR_TIMEOUT and
+ * dem_sync_status resets the broad phase, so the handle stays usable.
+ * One-shot; DEM_ERR_INVALID in phased mode or for phase < 0. */
+int dem_debug_fail_barrier(DemHandle* h, int32_t phase);
+
 /* Copy the last error message (NUL-terminated) into buf. */
 int dem_get_error(DemHandle* h, char* buf, size_t len);
 

@@ -101,7 +101,7 @@ class DemInfo(C.Structure):
 
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
            "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_set_profiling",
-           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version")
+           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier")
 
 _LIB = None
 
@@ -135,6 +135,7 @@ def load_library(path: str = None):
     lib.dem_get_phase_times.argtypes = [H, C.POINTER(C.c_int64), _i, C.POINTER(_i), C.POINTER(C.c_int64)]
     lib.dem_get_error.argtypes = [H, C.c_char_p, C.c_size_t]
     lib.dem_destroy.argtypes = [H]
+    lib.dem_debug_fail_barrier.argtypes = [H, _i]
     lib.dem_version.restype = C.c_char_p
     for name in EXPORTS:
         if name != "dem_version":

@@ -50,6 +50,7 @@ struct DemHandle {
     int* nbr = nullptr;
     void* pos_ref = nullptr;
     unsigned* dirty = nullptr;
+    int fail_phase = -1;      // one-shot barrier fault for the next persistent call (test hook)
     int capacity_flags = 0;   // what overflowed at the last DEM_ERR_CAPACITY (1 bucket, 2 list)
     unsigned round_base = 0;  // dirty stamps issued so far (since the last clear)
     int* bflag = nullptr;
@@ -401,6 +402,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
             h->round_base = 0;
         }
         a.round_base = h->round_base;
+        a.fail_phase = (h->mode == DEM_LAUNCH_PERSISTENT) ? h->fail_phase : -1;
+        h->fail_phase = -1;
         h->round_base += need;
     }
     CUDA_TRY(h, cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * 2, stream));
@@ -818,6 +821,14 @@ int dem_get_phase_times(DemHandle* h, int64_t* pairs, int32_t max_pairs, int32_t
     }
     *count = c;
     if (start_ns) *start_ns = (int64_t)buf[1];
+    return DEM_OK;
+}
+
+int dem_debug_fail_barrier(DemHandle* h, int32_t phase) {
+    if (!h || phase < 0) return DEM_ERR_INVALID;
+    if (h->mode != DEM_LAUNCH_PERSISTENT)
+        return set_err(h, DEM_ERR_INVALID, "barrier faults apply to persistent launches only");
+    h->fail_phase = phase;
     return DEM_OK;
 }
 

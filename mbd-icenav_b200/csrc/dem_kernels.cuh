@@ -129,6 +129,7 @@ struct KArgs {
     int* dirty_list;    // (n) elements whose list is rebuilt
     int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
+    int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
     const int* slot_owner;  // (2 nb) element that owns each bond slot
     T *sp_rot[2], *sp_avel[2];  // substep ping-pong of own-element angles
     void* slotrec;      // (2 nb) SlotRec<T>: per-frame bond slot records
@@ -1697,6 +1698,9 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
             }
         }
         if (persistent && ph + 1 < ph_hi) {
+            // failure-detection test: one CTA leaves, every other CTA's barrier
+            // wait ends at its time limit with DEM_ERR_TIMEOUT
+            if (ph == a.fail_phase && blockIdx.x == gridDim.x - 1) return;
             if (!grid_barrier(a)) return;
             if (a.ptimes && blockIdx.x == 0 && threadIdx.x == 0) {
                 // phase end times (debug/profiling): entry i = [phase, globaltimer]

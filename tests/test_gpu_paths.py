@@ -1,0 +1,73 @@
+"""GPU path equivalence and recovery, through the C ABI.
+
+* A 100-frame scan equals the same frames run as three chunked scans, bit for
+  bit, and follows the reference's own trajectory (the path-equivalence checks
+  of the reference's tests, test_jax_full_scan.py:233-295 and
+  test_jax_chunked_replan.py:68-160, which compare per-frame, full-scan and
+  chunked runs).
+* A handle created with neighbour-list and grid-bucket capacities far too
+  small reports DEM_ERR_CAPACITY; the wrapper grows what overflowed and re-runs
+  the call, and the result equals that of a handle sized right from the start.
+"""
+import numpy as np
+import pytest
+
+from helpers import frame_inputs, gpu_frame_step, initial_state, rel_err, to_gpu_state
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _scan_inputs(g, prefix, f0, f1, dtype):
+    d = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.asarray(a, np.float64)).to(d, dtype)
+    rows = np.stack([np.concatenate(frame_inputs(g, prefix, f)[:2]) for f in range(f0, f1)])
+    vw = np.stack([frame_inputs(g, prefix, f)[2] for f in range(f0, f1)])
+    vws = np.stack([frame_inputs(g, prefix, f)[3] for f in range(f0, f1)])
+    return t(rows), t(vw), t(vws)
+
+
+def test_chunked_scans_equal_one_scan_and_follow_the_reference(golden64):
+    g = golden64
+    prefix = "small"
+    fs = gpu_frame_step(g, prefix, torch.float64)
+    o_st, o_sh = initial_state(g, prefix, np.float64)
+    st0, sh0 = to_gpu_state(o_st, o_sh, torch.float64)
+    K = 100  # the ship meets the floes near frame 80
+    full_st, full_sh, full_h = fs.scan_segment(st0, sh0, *_scan_inputs(g, prefix, 0, K, torch.float64))
+    st, sh, hists = st0, sh0, []
+    for f0, f1 in ((0, 40), (40, 75), (75, K)):
+        st, sh, h = fs.scan_segment(st, sh, *_scan_inputs(g, prefix, f0, f1, torch.float64))
+        hists.append(h)
+    for a, b in zip(full_st, st):
+        assert torch.equal(a, b)
+    for a, b in zip(full_sh, sh):
+        assert torch.equal(a, b)
+    for i, full in enumerate(full_h):
+        assert torch.equal(full, torch.cat([h[i] for h in hists]))
+    pos = full_h[0].cpu().numpy()
+    assert rel_err(pos, g[f"{prefix}_pos"][:K], 1e-6) < 1e-6
+    np.testing.assert_array_equal(full_h[2].cpu().numpy(), g[f"{prefix}_intact"][:K])
+    fs.close()
+
+
+def test_capacity_overflow_is_retried_with_identical_results(golden32):
+    g = golden32
+    prefix = "window"
+    o_st, o_sh = initial_state(g, prefix, np.float32)
+    inputs = _scan_inputs(g, prefix, 0, 3, torch.float32)
+    ref = gpu_frame_step(g, prefix, torch.float32)
+    st, sh = to_gpu_state(o_st, o_sh, torch.float32)
+    r_st, r_sh, r_h = ref.scan_segment(st, sh, *inputs)
+    tight = gpu_frame_step(g, prefix, torch.float32, max_neighbors=6, bucket_capacity=6)
+    st, sh = to_gpu_state(o_st, o_sh, torch.float32)
+    t_st, t_sh, t_h = tight.scan_segment(st, sh, *inputs)
+    info = tight.info()
+    assert info["capacity_flags"] != 0  # something overflowed and was grown
+    assert tight.params.max_neighbors > 6 or tight.params.bucket_capacity > 6
+    for a, b in zip(r_st + r_sh, t_st + t_sh):
+        assert torch.equal(a, b)
+    for a, b in zip(r_h, t_h):
+        assert torch.equal(a, b)
+    ref.close()
+    tight.close()
