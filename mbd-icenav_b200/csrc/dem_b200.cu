@@ -337,6 +337,24 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     }
     a.slotrec = h->slotrec;
     a.r3 = (const T*)h->r3;
+    {
+        const DemParams& P = h->P;
+        a.fc.hf = (T)P.hertz_factor;
+        a.fc.hexp = (T)P.hertz_exponent;
+        a.fc.h15 = (P.hertz_exponent == 1.5) ? 1 : 0;
+        a.fc.mu = (T)P.ice_ice_friction;
+        a.fc.fcap = (T)P.friction_cap;
+        a.fc.c_drag = (T)(0.5 * P.water_density * P.c_d_drag);
+        a.fc.href = (T)P.drag_ref_thickness;
+        a.fc.lin = (T)P.linear_drag_factor;
+        a.fc.c_rot = (T)(-0.5 * P.drag_coefficient_moment * P.water_density);
+        a.fc.dti = (T)P.dt_ice;
+        a.fc.damp = (T)P.angular_damping;
+        a.fc.alo = (T)P.angular_cap_lo;
+        a.fc.ahi = (T)P.angular_cap_hi;
+        a.fc.vclip = (T)P.velocity_clip;
+        a.fc.pclip = (T)P.position_clip;
+    }
     a.econ = (const T*)h->econ;
     a.fscal = h->fscal;
     a.ptimes = h->profiling ? h->ptimes : nullptr;

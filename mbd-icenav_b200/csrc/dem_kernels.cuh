@@ -83,6 +83,14 @@ struct ShipPtrs {
     T *eta, *nu, *na, *ei;
 };
 
+// Force-phase constants in the kernel's dtype, converted once on the host and
+// read from the kernel parameter (constant bank) rather than held in registers.
+template <typename T>
+struct ForceConst {
+    T hf, hexp, mu, fcap, c_drag, href, lin, c_rot, dti, damp, alo, ahi, vclip, pclip;
+    int h15;  // hertz_exponent == 1.5: overlap * sqrt(overlap) instead of pow
+};
+
 template <typename T>
 struct KArgs {
     DemParams P;
@@ -130,6 +138,7 @@ struct KArgs {
     int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
     int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
+    ForceConst<T> fc;     // force-phase constants
     const int* slot_owner;  // (2 nb) element that owns each bond slot
     T *sp_rot[2], *sp_avel[2];  // substep ping-pong of own-element angles
     void* slotrec;      // (2 nb) SlotRec<T>: per-frame bond slot records
@@ -1202,13 +1211,11 @@ struct ForceCtx {
     T *kout, *kvout, *rout, *aout;
     const uint8_t* act;
     const SlotRec<T>* rec;
-    T hf, hexp, mu, fcap, c_drag, href, lin, c_rot, dti, damp, alo, ahi, vclip, pclip;
-    bool h15, last;
+    bool last;
 };
 
 template <typename T>
 __device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<T>& F, int s) {
-    const DemParams& P = a.P;
     ForceCtx<T> c;
     const int k = a.k_sub;
     c.kin = a.kin[s & 1];
@@ -1222,21 +1229,6 @@ __device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<
     c.aout = c.last ? F.dst.avel : a.sp_avel[s & 1];
     c.act = F.dst.active;
     c.rec = reinterpret_cast<const SlotRec<T>*>(a.slotrec);
-    c.hf = T(P.hertz_factor);
-    c.hexp = T(P.hertz_exponent);
-    c.h15 = (P.hertz_exponent == 1.5);
-    c.mu = T(P.ice_ice_friction);
-    c.fcap = T(P.friction_cap);
-    c.c_drag = T(0.5 * P.water_density * P.c_d_drag);
-    c.href = T(P.drag_ref_thickness);
-    c.lin = T(P.linear_drag_factor);
-    c.c_rot = T(-0.5 * P.drag_coefficient_moment * P.water_density);
-    c.dti = T(P.dt_ice);
-    c.damp = T(P.angular_damping);
-    c.alo = T(P.angular_cap_lo);
-    c.ahi = T(P.angular_cap_hi);
-    c.vclip = T(P.velocity_clip);
-    c.pclip = T(P.position_clip);
     return c;
 }
 
@@ -1257,8 +1249,8 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
     typedef typename vec4_of<T>::type V4;
     const T *kin = cx.kin, *kvin = cx.kvin;
     const SlotRec<T>* rec = cx.rec;
-    const T hf = cx.hf, hexp = cx.hexp, mu = cx.mu, fcap = cx.fcap;
-    const bool h15 = cx.h15, last = cx.last;
+    const T hf = a.fc.hf, hexp = a.fc.hexp, mu = a.fc.mu, fcap = a.fc.fcap;
+    const bool h15 = a.fc.h15 != 0, last = cx.last;
     // loads that depend on e only
     const V4 ke = ld4(kin, e);  // x, y, radius, radius^3
     const V2 ve = ld2(kvin, e);
@@ -1371,32 +1363,32 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
     }
     // drag (jax_simulation.py:167-192)
     const T m = ec.x, inertia = ec.y, h = ec.z, A = ec.w;
-    const T a_drag = A * (h / cx.href);
+    const T a_drag = A * (h / a.fc.href);
     const T vrx = ve.x - w.x, vry = ve.y - w.y;
     const T vm = jsqrt(vrx * vrx + vry * vry);
     T fdx, fdy;
     if (vm > T(1e-6)) {
-        const T q = cx.c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
+        const T q = a.fc.c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
         fdx = vrx * q;
         fdy = vry * q;
     } else {
-        const T cl = cx.c_drag * a_drag * cx.lin;
+        const T cl = a.fc.c_drag * a_drag * a.fc.lin;
         fdx = cl * vrx;
         fdy = cl * vry;
     }
     // rotational drag (jax_simulation.py:195-212)
     const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
-    const T md = cx.c_rot * ke.w * av * fabs(av) * a_sub;
+    const T md = a.fc.c_rot * ke.w * av * fabs(av) * a_sub;
     const T Fx = ((fbx + fix) - fdx) + so.x;
     const T Fy = ((fby + fiy) - fdy) + so.y;
     const T Mz = (mb + mi) + md;
     // semi-implicit Euler (jax_simulation.py:215-268)
-    const T dti = cx.dti, vclip = cx.vclip, pclip = cx.pclip;
+    const T dti = a.fc.dti, vclip = a.fc.vclip, pclip = a.fc.pclip;
     T nvx = jclip(ve.x + (Fx / m) * dti, -vclip, vclip);
     T nvy = jclip(ve.y + (Fy / m) * dti, -vclip, vclip);
     T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
     const T alpha = Mz / inertia;
-    T nav = jclip(av * cx.damp + alpha * dti, cx.alo, cx.ahi);
+    T nav = jclip(av * a.fc.damp + alpha * dti, a.fc.alo, a.fc.ahi);
     T nrot = rot + nav * dti;
     if (!jfinite(nvx)) nvx = T(0);
     if (!jfinite(nvy)) nvy = T(0);
@@ -1435,14 +1427,14 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
     int* esc_ctr = (int*)&a.esc_cnt[s + 1];
+    const int warp = gtid >> 5, nwarps = gsz >> 5, lane = threadIdx.x & 31;
+    const int nd = has_dirty ? *((volatile int*)&a.dirty_cnt[s]) : 0;
     if (has_dirty) {
         // elements whose list this round invalidated: one warp rebuilds the list,
         // then lane 0 computes the element (the main loop below skips them)
         __shared__ int sbuf[kThreads / 32][2 * kMaxNbLocal];
         __shared__ int scnt[kThreads / 32];
-        const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        const int warp = gtid >> 5, nwarps = gsz >> 5;
-        const int nd = *((volatile int*)&a.dirty_cnt[s]);
+        const int wl = threadIdx.x >> 5;
         if (gtid == 0) atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)nd);
         for (int q = warp; q < nd; q += nwarps) {
             const int e = a.dirty_list[q];
@@ -1451,7 +1443,14 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
             __syncwarp();
         }
     }
-    for (int e = gtid; e < a.n; e += gsz) {
+    // The warps that rebuilt a list above take no share of the element loop
+    // (while enough warps remain), so they do not finish the phase last.
+    const int skip = (nd < nwarps / 2) ? nd : 0;
+    if (warp < skip) return;
+    const int w2 = warp - skip, nw2 = nwarps - skip;
+    for (int c = w2; c * 32 < a.n; c += nw2) {
+        const int e = c * 32 + lane;
+        if (e >= a.n) continue;
         if (has_dirty && a.dirty[e] == round) continue;
         const bool esc = force_element(a, F, cx, e);
         if (!cx.last) warp_append(a.esc_list, esc_ctr, esc, e);
