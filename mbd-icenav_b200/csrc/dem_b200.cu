@@ -59,6 +59,7 @@ struct DemHandle {
     int* esc_list = nullptr;
     int* dirty_list = nullptr;
     int* dirty_cnt = nullptr;
+    int* work_cnt = nullptr;
     int* slot_owner = nullptr;
     unsigned* esc_cnt = nullptr;
     int* near_list = nullptr;
@@ -321,6 +322,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.esc_list = h->esc_list;
     a.dirty_list = h->dirty_list;
     a.dirty_cnt = h->dirty_cnt;
+    a.work_cnt = h->work_cnt;
     a.slot_owner = h->slot_owner;
     a.esc_cnt = h->esc_cnt;
     a.soi = (T*)h->soi;
@@ -411,6 +413,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     CUDA_TRY(h, cudaMemsetAsync(h->fmax, 0, sizeof(unsigned long long) * std::max(h->nf, 1), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->esc_cnt, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->dirty_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->work_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
     {
         // every rebuild round of every call gets its own dirty stamp; clear the
         // stamps before the counter would wrap
@@ -591,6 +594,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->esc_list, sizeof(int) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->dirty_list, sizeof(int) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->dirty_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->work_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->esc_cnt, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);

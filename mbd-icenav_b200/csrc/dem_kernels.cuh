@@ -136,6 +136,7 @@ struct KArgs {
     int* esc_list;      // (n) escaped elements of the current detection
     int* dirty_list;    // (n) elements whose list is rebuilt
     int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
+    int* work_cnt;      // (k_sub + 2) element chunks handed out dynamically, per substep
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
     int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
     ForceConst<T> fc;     // force-phase constants
@@ -1447,13 +1448,22 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     // (while enough warps remain), so they do not finish the phase last.
     const int skip = (nd < nwarps / 2) ? nd : 0;
     if (warp < skip) return;
-    const int w2 = warp - skip, nw2 = nwarps - skip;
-    for (int c = w2; c * 32 < a.n; c += nw2) {
+    // Chunks of 32 elements: every warp starts with one chunk of its own, then
+    // takes further chunks from a counter (the next grab is issued before the
+    // current chunk is computed), so uneven chunks do not leave warps idle.
+    const int nchunks = (a.n + 31) >> 5;
+    const int nw2 = nwarps - skip;
+    int c = warp - skip;
+    int* ctr = &a.work_cnt[s];
+    while (c < nchunks) {
+        int next = 0;
+        if (lane == 0) next = nw2 + atomicAdd(ctr, 1);
         const int e = c * 32 + lane;
-        if (e >= a.n) continue;
-        if (has_dirty && a.dirty[e] == round) continue;
-        const bool esc = force_element(a, F, cx, e);
-        if (!cx.last) warp_append(a.esc_list, esc_ctr, esc, e);
+        if (e < a.n && !(has_dirty && a.dirty[e] == round)) {
+            const bool esc = force_element(a, F, cx, e);
+            if (!cx.last) warp_append(a.esc_list, esc_ctr, esc, e);
+        }
+        c = __shfl_sync(0xffffffffu, next, 0);
     }
 }
 
@@ -1646,6 +1656,7 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
     for (int i = gtid; i < a.k_sub + 2; i += gsz) {
         a.esc_cnt[i] = 0u;
         a.dirty_cnt[i] = 0;
+        a.work_cnt[i] = 0;
     }
 }
 
