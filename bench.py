@@ -407,8 +407,7 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5):
             prev = t
     fs.set_profiling(False)
     tot = 0.0
-    # the last phase (fracture) ends the launch and records no time stamp
-    for nm in ("cull", "near", "cforce", "reduce", "escape", "build_all", "force"):
+    for nm in ("cull", "near", "cforce", "reduce", "escape", "build_all", "force", "fracture"):
         v = acc.get(nm, [])
         s = sum(v) / frames
         tot += s

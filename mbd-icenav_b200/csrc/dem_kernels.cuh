@@ -1707,7 +1707,9 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
                 phase_force(a, F, s, round, cnt != 0u && !all);
             }
         }
-        if (persistent && ph + 1 < ph_hi) {
+        // a barrier after every phase but the last; with profiling on, after the
+        // last one too, so that its end time is recorded
+        if (persistent && (ph + 1 < ph_hi || a.ptimes)) {
             // failure-detection test: one CTA leaves, every other CTA's barrier
             // wait ends at its time limit with DEM_ERR_TIMEOUT
             if (ph == a.fail_phase && blockIdx.x == gridDim.x - 1) return;
