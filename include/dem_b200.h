@@ -237,6 +237,31 @@ int dem_destroy(DemHandle* h);
 /* Library version string, e.g. "dem_b200 0.1 sm_100a". */
 const char* dem_version(void);
 
+/* Grid and cost constants of dem_ke_costmap (arguments of build_costmap_jax,
+ * jax_costmap.py:179-203, after its grid geometry, :237-244). */
+typedef struct DemCostmapParams {
+    double x_origin, y_origin;     /* world position of cell (0,0)'s lower-left corner [m] */
+    double resolution;             /* cell size [m]                                      */
+    int32_t rows, cols;
+    double base_cost;              /* open-water cost                                   */
+    double collision_cost;         /* KE cost weight                                    */
+    double obs_cost_buffer_factor; /* extra fractional radius painted per element       */
+    double ship_speed, ship_mass, ke_cost_scale;
+    int32_t dilate_half;           /* square max window of 2h+1 cells; 0 = no dilation  */
+    int32_t has_masses;            /* 0: masses = pi r^2 h 920 (jax_costmap.py:257-259) */
+} DemCostmapParams;
+
+/* Replaces the device work of build_costmap_jax (jax_costmap.py:179-331; with
+ * ice_resistance_weight = 0): the KE collision costmap of the ice elements
+ * (centroids (n,2), radii, thicknesses, masses (n,) of `dtype`; masses may be
+ * NULL when has_masses = 0, thicknesses when it is 1) into grid (rows, cols)
+ * float32, row-major.  tmp (rows, cols) float32 is needed when dilate_half > 0;
+ * flag is one device int32 of scratch.  All pointers are device pointers;
+ * `stream` is a cudaStream_t.  Bit-exact with the reference's float32 grid. */
+int dem_ke_costmap(int32_t dtype, int32_t n, const void* centroids, const void* radii,
+                   const void* thicknesses, const void* masses, const DemCostmapParams* params,
+                   float* grid, float* tmp, int32_t* flag, void* stream);
+
 /* Largest n accepted by dem_ship_contact_noalloc. */
 #define DEM_CONTACT_NOALLOC_MAX_ELEMENTS 262144
 

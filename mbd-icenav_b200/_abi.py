@@ -99,9 +99,16 @@ class DemInfo(C.Structure):
                 ("capacity_flags", _i)]
 
 
+class DemCostmapParams(C.Structure):
+    _fields_ = [("x_origin", _d), ("y_origin", _d), ("resolution", _d), ("rows", _i), ("cols", _i),
+                ("base_cost", _d), ("collision_cost", _d), ("obs_cost_buffer_factor", _d),
+                ("ship_speed", _d), ("ship_mass", _d), ("ke_cost_scale", _d),
+                ("dilate_half", _i), ("has_masses", _i)]
+
+
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
            "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_set_profiling",
-           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier")
+           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap")
 
 _LIB = None
 
@@ -136,6 +143,7 @@ def load_library(path: str = None):
     lib.dem_get_error.argtypes = [H, C.c_char_p, C.c_size_t]
     lib.dem_destroy.argtypes = [H]
     lib.dem_debug_fail_barrier.argtypes = [H, _i]
+    lib.dem_ke_costmap.argtypes = [_i, _i, _vp, _vp, _vp, _vp, C.POINTER(DemCostmapParams), _vp, _vp, _vp, _vp]
     lib.dem_version.restype = C.c_char_p
     for name in EXPORTS:
         if name != "dem_version":

@@ -173,6 +173,17 @@ def _make_jnp():
 
     m.zeros, m.ones, m.arange, m.linspace, m.eye = zeros, ones, arange, linspace, eye
 
+    def full(shape, fill_value, dtype=None):
+        return _w(np.full(shape, fill_value, dtype=_canon(dtype) or _default_float()))
+
+    def meshgrid(*xs, indexing="xy"):
+        return tuple(_w(g) for g in np.meshgrid(*[np.asarray(x) for x in xs], indexing=indexing))
+
+    def pad(x, pad_width, mode="constant", **kw):
+        return _w(np.pad(np.asarray(x), pad_width, mode=mode, **kw))
+
+    m.full, m.meshgrid, m.pad = full, meshgrid, pad
+
     def _wrapfn(fn):
         def g(*a, **k):
             return _w(fn(*a, **k))
@@ -253,8 +264,19 @@ def _make_lax():
             val = body(i, val)
         return val
 
+    def reduce_window(x, init_value, computation, window_dimensions, window_strides, padding):
+        # the max-pool form only: stride 1, VALID padding, computation = lax.max
+        x = np.asarray(x)
+        if tuple(window_strides) != (1,) * x.ndim or padding != "VALID" or computation is not lax.max:
+            raise NotImplementedError("reduce_window: only max, stride 1, VALID")
+        win = np.lib.stride_tricks.sliding_window_view(x, tuple(window_dimensions))
+        out = win.max(axis=tuple(range(x.ndim, 2 * x.ndim)))
+        return _w(np.maximum(out, np.asarray(init_value, dtype=x.dtype)))
+
     lax.scan = scan
     lax.fori_loop = fori_loop
+    lax.max = lambda a, b: _w(np.maximum(a, b))
+    lax.reduce_window = reduce_window
     return lax
 
 
@@ -280,6 +302,15 @@ def install(x64: bool) -> None:
     jax.lax = lax
     jax.config = _Config()
     jax.block_until_ready = lambda x: x
+
+    def vmap(f, in_axes=0, out_axes=0):
+        def g(*args):
+            n = int(np.shape(args[0])[0])
+            outs = [f(*[_w(np.asarray(a)[i]) for a in args]) for i in range(n)]
+            return _w(np.stack([np.asarray(o) for o in outs]))
+        return g
+
+    jax.vmap = vmap
     jax.Array = ShimArray
     sys.modules["jax"] = jax
     sys.modules["jax.numpy"] = jnp
