@@ -117,6 +117,14 @@ typedef struct DemStatic {
     const int32_t* initial_floe_of;   /* (n,) parent floe, 0 <= id < n_floes */
     double k_n, k_s;
     const void* ship_hull_local;      /* (n_hull, 2) ShipDynamicsData.ship_hull_local */
+    /* Independent systems (no reference counterpart): n_systems > 1 splits the
+     * elements into contiguous ranges [system_start[q], system_start[q+1]), each
+     * an ice window with its own ship (same hull), advanced together by
+     * dem_scan_segment / dem_rollout_segment.  Floes and bonds stay inside one
+     * system; elements of different systems never interact.  system_start is a
+     * HOST array of n_systems + 1 offsets from 0 to n.  0 or 1: one system. */
+    int32_t n_systems;
+    const int32_t* system_start;
 } DemStatic;
 
 /* IceState (jax_ice_state.py:31-44). */
@@ -192,7 +200,10 @@ int dem_frame_step(DemHandle* h, const DemIceState* in, DemIceState* out,
 
 /* Replaces JaxSimContext.scan_segment (jax_simulation.py:1308-1335): K frames with
  * setpoints (K,6) rows [sp, sp_next], v_water (K,n,2), v_water_ship (K,2) or NULL.
- * Each frame uses the previous frame's dpdem_floe_eligible (jax_simulation.py:1314). */
+ * Each frame uses the previous frame's dpdem_floe_eligible (jax_simulation.py:1314).
+ * With Q = n_systems > 1: ship states are (Q,3) / (Q,6) arrays, setpoints (K,Q,6),
+ * v_water_ship (K,Q,2), and the history's eta (K,Q,3), J_cumul_incr (K,Q),
+ * F_ice_on_ship (K,Q,2). */
 int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out,
                      const DemShipState* ship_in, DemShipState* ship_out, int32_t K,
                      const void* setpoints_K6, const void* v_water_Kn2,

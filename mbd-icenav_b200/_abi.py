@@ -69,6 +69,7 @@ class DemStatic(C.Structure):
         ("sigma_bar_bond", _vp), ("initial_floe_of", _vp),
         ("k_n", _d), ("k_s", _d),
         ("ship_hull_local", _vp),
+        ("n_systems", _i), ("system_start", C.POINTER(_i)),
     ]
 
 

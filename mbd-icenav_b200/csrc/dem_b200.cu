@@ -96,7 +96,16 @@ struct DemHandle {
     double* fscal = nullptr;
     unsigned long long* ptimes = nullptr;
     bool profiling = false;
-    void* ship_tmp = nullptr;  // 2 x 15
+    void* ship_tmp = nullptr;  // 2 x 15 x nsys
+    // independent systems (ice windows with their own ships)
+    int nsys = 1;
+    int nchunks = 0;
+    int* sys_of = nullptr;
+    int* floe_sys = nullptr;
+    int2* chunk_info = nullptr;
+    int* sys_end = nullptr;
+    int* part_base = nullptr;
+    std::vector<int> sys_start_h;  // (nsys + 1) element offsets
     void* sprow = nullptr;     // (6,) setpoint row of dem_frame_step
     unsigned* bar = nullptr;
     int* status = nullptr;
@@ -272,7 +281,13 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.S = h->nh;
     a.K = K;
     a.k_sub = h->P.n_ice_steps;
-    a.nchunks = (h->n + dem::kThreads - 1) / dem::kThreads;
+    a.nchunks = h->nchunks;
+    a.nsys = h->nsys;
+    a.sys_of = h->sys_of;
+    a.floe_sys = h->floe_sys;
+    a.chunk_info = h->chunk_info;
+    a.sys_end = h->sys_end;
+    a.part_base = h->part_base;
     a.n_buckets = h->n_buckets;
     a.bucket_cap = h->P.bucket_capacity;
     a.max_nb = h->P.max_neighbors;
@@ -380,10 +395,11 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.ship_out = ship_ptrs<T>(ship_out);
     T* st = (T*)h->ship_tmp;
     for (int i = 0; i < 2; ++i) {
-        a.ship_tmp[i].eta = st + 15 * i;
-        a.ship_tmp[i].nu = st + 15 * i + 3;
-        a.ship_tmp[i].na = st + 15 * i + 6;
-        a.ship_tmp[i].ei = st + 15 * i + 12;
+        const int q = h->nsys;  // per buffer: eta (3q), nu (3q), n_actual (6q), e_int (3q)
+        a.ship_tmp[i].eta = st + 15 * q * i;
+        a.ship_tmp[i].nu = st + 15 * q * i + 3 * q;
+        a.ship_tmp[i].na = st + 15 * q * i + 6 * q;
+        a.ship_tmp[i].ei = st + 15 * q * i + 12 * q;
     }
     a.setpoints = (const T*)setpoints;
     a.vw = (const T*)vw;
@@ -524,6 +540,40 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     for (int b = 0; b < nb; ++b)
         if (bi[b] < 0 || bi[b] >= n || bj[b] < 0 || bj[b] >= n || bi[b] == bj[b])
             return fail(set_err(h, DEM_ERR_INVALID, "bond %d=(%d,%d) invalid", b, bi[b], bj[b]));
+    // systems: contiguous element ranges; floes and bonds may not span two
+    h->nsys = s->n_systems > 1 ? s->n_systems : 1;
+    h->sys_start_h.assign(h->nsys + 1, 0);
+    h->sys_start_h[h->nsys] = n;
+    if (h->nsys > 1) {
+        if (!s->system_start) return fail(set_err(h, DEM_ERR_INVALID, "n_systems > 1 needs system_start"));
+        for (int q = 0; q <= h->nsys; ++q) h->sys_start_h[q] = s->system_start[q];
+        if (h->sys_start_h[0] != 0 || h->sys_start_h[h->nsys] != n)
+            return fail(set_err(h, DEM_ERR_INVALID, "system_start must run from 0 to n"));
+        for (int q = 0; q < h->nsys; ++q)
+            if (h->sys_start_h[q + 1] <= h->sys_start_h[q])
+                return fail(set_err(h, DEM_ERR_INVALID, "system %d has no element", q));
+    }
+    std::vector<int> sys_of(n), floe_sys(nf, -1);
+    for (int q = 0; q < h->nsys; ++q)
+        for (int e = h->sys_start_h[q]; e < h->sys_start_h[q + 1]; ++e) sys_of[e] = q;
+    for (int e = 0; e < n; ++e) {
+        if (floe_sys[floe[e]] >= 0 && floe_sys[floe[e]] != sys_of[e])
+            return fail(set_err(h, DEM_ERR_INVALID, "floe %d spans two systems", floe[e]));
+        floe_sys[floe[e]] = sys_of[e];
+    }
+    for (int& v : floe_sys) v = std::max(v, 0);
+    for (int b = 0; b < nb; ++b)
+        if (sys_of[bi[b]] != sys_of[bj[b]]) return fail(set_err(h, DEM_ERR_INVALID, "bond %d spans two systems", b));
+    // force chunks of kThreads elements, aligned to each system's first element
+    std::vector<int2> chunks;
+    std::vector<int> part_base(h->nsys + 1, 0), sys_end(h->nsys);
+    for (int q = 0; q < h->nsys; ++q) {
+        part_base[q] = (int)chunks.size();
+        sys_end[q] = h->sys_start_h[q + 1];
+        for (int e0 = h->sys_start_h[q]; e0 < h->sys_start_h[q + 1]; e0 += dem::kThreads) chunks.push_back(make_int2(q, e0));
+    }
+    part_base[h->nsys] = (int)chunks.size();
+    h->nchunks = (int)chunks.size();
     h->r_max = 0.0;
     for (double r : radii) {
         if (!(r >= 0.0) || !std::isfinite(r)) return fail(set_err(h, DEM_ERR_INVALID, "radii must be finite and >= 0"));
@@ -602,7 +652,12 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->crack, n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fcoll, sizeof(int) * nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fmax, sizeof(unsigned long long) * nf))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->part, sizeof(double) * 3 * ((n + dem::kThreads - 1) / dem::kThreads)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->part, sizeof(double) * 3 * std::max(h->nchunks, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->sys_of, sizeof(int) * n))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->floe_sys, sizeof(int) * nf))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->chunk_info, sizeof(int2) * std::max(h->nchunks, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->sys_end, sizeof(int) * h->nsys))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->part_base, sizeof(int) * (h->nsys + 1)))) return fail(rc);
     for (int i = 0; i < 2; ++i) {
         if ((rc = dev_alloc(h, &h->kin[i], es * 4 * n))) return fail(rc);
         if ((rc = dev_alloc(h, &h->kvel[i], es * 2 * n))) return fail(rc);
@@ -621,11 +676,11 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->t_ds, es * std::max(nb, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->t_active, n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->t_elig, nf))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->ship_tmp, es * 30))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->ship_tmp, es * 30 * h->nsys))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slotrec, (es == 4 ? 16 : 32) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->r3, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->econ, es * 4 * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->fscal, sizeof(double) * 4))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fscal, sizeof(double) * 4 * h->nsys))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ptimes, sizeof(unsigned long long) * (2 + 2 * dem::kMaxPhaseTimes)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->sprow, es * 6))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bar, sizeof(unsigned) * 2))) return fail(rc);
@@ -640,6 +695,11 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
         if (_e != cudaSuccess) return fail(set_err(h, DEM_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e))); \
     } while (0)
     CREATE_TRY(cudaMemcpy(h->boff, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CREATE_TRY(cudaMemcpy(h->sys_of, sys_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CREATE_TRY(cudaMemcpy(h->floe_sys, floe_sys.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
+    CREATE_TRY(cudaMemcpy(h->chunk_info, chunks.data(), sizeof(int2) * chunks.size(), cudaMemcpyHostToDevice));
+    CREATE_TRY(cudaMemcpy(h->sys_end, sys_end.data(), sizeof(int) * h->nsys, cudaMemcpyHostToDevice));
+    CREATE_TRY(cudaMemcpy(h->part_base, part_base.data(), sizeof(int) * (h->nsys + 1), cudaMemcpyHostToDevice));
     CREATE_TRY(cudaMemcpy(h->bslot, slots.data(), sizeof(int2) * slots.size(), cudaMemcpyHostToDevice));
     {
         std::vector<int> owner(slots.size(), 0);
@@ -713,6 +773,8 @@ int dem_frame_step(DemHandle* h, const DemIceState* in, DemIceState* out, const 
     if (out->positions == in->positions || out->velocities == in->velocities || out->rotations == in->rotations ||
         out->angular_vels == in->angular_vels)
         return set_err(h, DEM_ERR_ALIAS, "output element kinematics alias the input");
+    if (h->nsys > 1)
+        return set_err(h, DEM_ERR_INVALID, "a handle with several systems steps through dem_scan_segment");
     CUDA_TRY(h, cudaSetDevice(h->device));
     cudaStream_t st = (cudaStream_t)stream;
     // pack [setpoint, setpoint_next] into the (1,6) row the kernel reads

@@ -95,6 +95,15 @@ template <typename T>
 struct KArgs {
     DemParams P;
     int n, V, nb, nf, S, K, k_sub, nchunks;
+    // independent systems (an ice window with its own ship) advanced together;
+    // 1 for a plain field.  Elements of system s are [sys_start_s, sys_end[s]),
+    // its force chunks [part_base[s], part_base[s + 1]).
+    int nsys;
+    const int* sys_of;        // (n) system of each element (read when nsys > 1)
+    const int* floe_sys;      // (nf) system of each floe (read when nsys > 1)
+    const int2* chunk_info;   // (nchunks) {system, first element} of each chunk of kThreads elements
+    const int* sys_end;       // (nsys) one past each system's last element
+    const int* part_base;     // (nsys + 1) first chunk of each system
     int n_buckets, bucket_cap, max_nb, mode;
     T k_n, k_s, min_bstr, cell, skin, hull_r;
     T t_samp[kMaxEdgeSamples];
@@ -179,8 +188,8 @@ struct Frame {
     ShipPtrs<T> ship_src, ship_dst;
     const uint8_t* elig_in;
     const T* vw;
-    T sp[6];
-    T vws[2];
+    const T* sp;   // (nsys, 6) [setpoint, setpoint_next] of this frame
+    const T* vws;  // (nsys, 2) current at the ships, or NULL (none)
 };
 
 template <typename T>
@@ -194,9 +203,8 @@ __device__ __forceinline__ Frame<T> make_frame(const KArgs<T>& a, int f) {
     F.ship_src = (f == 0) ? a.ship_in : a.ship_tmp[(f - 1) & 1];
     F.elig_in = (f == 0) ? a.elig0 : F.src.elig;
     F.vw = a.vw + (size_t)f * a.n * 2;
-    for (int i = 0; i < 6; ++i) F.sp[i] = a.setpoints[f * 6 + i];
-    F.vws[0] = a.vws ? a.vws[f * 2 + 0] : T(0);
-    F.vws[1] = a.vws ? a.vws[f * 2 + 1] : T(0);
+    F.sp = a.setpoints + (size_t)f * a.nsys * 6;
+    F.vws = a.vws ? a.vws + (size_t)f * a.nsys * 2 : nullptr;
     return F;
 }
 
@@ -343,6 +351,7 @@ __device__ __forceinline__ void warp_near_at(const KArgs<T>& a, int e, T px, T p
         // can show an old value (-1 or a valid stale index), never an invalid one
         const int o = ((volatile const int*)a.bitems)[(size_t)qb * a.bucket_cap + (t - qe)];
         if (o < 0 || o >= a.n || o == e) continue;
+        if (a.nsys > 1 && a.sys_of[o] != a.sys_of[e]) continue;  // systems never interact
         const int2 cc = make_int2(c.x + (q % 3) - 1, c.y + (q / 3) - 1);
         const int2 oc = a.ecell[o];
         if (oc.x != cc.x || oc.y != cc.y) continue;  // stale entry or hash collision
@@ -381,6 +390,7 @@ __device__ __forceinline__ void block_near_at(const KArgs<T>& a, int e, T px, T 
         // can show an old value (-1 or a valid stale index), never an invalid one
         const int o = ((volatile const int*)a.bitems)[(size_t)s_b[q] * a.bucket_cap + (t - s_start[q])];
         if (o < 0 || o >= a.n || o == e) continue;
+        if (a.nsys > 1 && a.sys_of[o] != a.sys_of[e]) continue;  // systems never interact
         const int2 cc = make_int2(c.x + (q % 3) - 1, c.y + (q / 3) - 1);
         const int2 oc = a.ecell[o];
         if (oc.x != cc.x || oc.y != cc.y) continue;  // stale entry or hash collision
@@ -672,11 +682,11 @@ __device__ __forceinline__ void block_sum3(double v0, double v1, double v2, doub
 }
 
 template <typename T>
-__device__ __forceinline__ HullPose<T> hull_pose(const KArgs<T>& a, const Frame<T>& F) {
+__device__ __forceinline__ HullPose<T> hull_pose(const KArgs<T>& a, const T* eta) {
     HullPose<T> H;
-    H.sx = F.ship_src.eta[0];
-    H.sy = F.ship_src.eta[1];
-    const T spsi = F.ship_src.eta[2];
+    H.sx = eta[0];
+    H.sy = eta[1];
+    const T spsi = eta[2];
     jsincos(-spsi, &H.s_neg, &H.c_neg);
     jsincos(spsi, &H.s_h, &H.c_h);
     H.hl = T(a.P.half_len);
@@ -690,7 +700,6 @@ template <typename T>
 __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
-    const T sx = F.ship_src.eta[0], sy = F.ship_src.eta[1];
     const T reach = a.hull_r * T(1.0001) + T(1e-3);
     // nothing reads the grid in this phase: drop stale entries queued last frame
     compact_buckets(a);
@@ -701,7 +710,8 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
     }
     for (int e = gtid; e < a.n; e += gsz) {
         typename vec2_of<T>::type p = ld2(F.src.pos, e);
-        const T ddx = p.x - sx, ddy = p.y - sy;
+        const T* eta = F.ship_src.eta + 3 * (a.nsys > 1 ? a.sys_of[e] : 0);  // this element's ship
+        const T ddx = p.x - eta[0], ddy = p.y - eta[1];
         const T lim = reach + a.vert_r[e];
         // every query point of e lies within vert_r of its centroid and every hull
         // point within hull_r of the ship: farther elements get pen = 0, which is
@@ -755,12 +765,17 @@ __device__ __forceinline__ Best<T> warp_best(Best<T> b) {
 
 template <typename T>
 __device__ void phase_near(const KArgs<T>& a, const Frame<T>& F, T* hullw) {
-    const HullPose<T> H = hull_pose(a, F);
-    // hull outline in world frame: ship_hull_local @ R.T + [x, y] (jax_geometry.py:568-572)
-    for (int i = threadIdx.x; i < a.S; i += blockDim.x) {
-        T lx = a.hull[2 * i], ly = a.hull[2 * i + 1];
-        hullw[2 * i] = lx * H.c_h + ly * (-H.s_h) + H.sx;
-        hullw[2 * i + 1] = lx * H.s_h + ly * H.c_h + H.sy;
+    // hull outline in world frame: ship_hull_local @ R.T + [x, y] (jax_geometry.py:568-572),
+    // staged once per CTA for a single ship; with several ships each element
+    // transforms its own ship's outline point by point (the same expression)
+    const bool one_ship = a.nsys == 1;
+    HullPose<T> H1 = hull_pose(a, F.ship_src.eta);
+    if (one_ship) {
+        for (int i = threadIdx.x; i < a.S; i += blockDim.x) {
+            T lx = a.hull[2 * i], ly = a.hull[2 * i + 1];
+            hullw[2 * i] = lx * H1.c_h + ly * (-H1.s_h) + H1.sx;
+            hullw[2 * i + 1] = lx * H1.s_h + ly * H1.c_h + H1.sy;
+        }
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -772,6 +787,7 @@ __device__ void phase_near(const KArgs<T>& a, const Frame<T>& F, T* hullw) {
     const int P1 = V * (1 + E);
     for (int q = warp; q < nnear; q += nwarps) {
         const int e = a.near_list[q];
+        const HullPose<T> H = one_ship ? H1 : hull_pose(a, F.ship_src.eta + 3 * a.sys_of[e]);
         typename vec2_of<T>::type pe = ld2(F.src.pos, e);
         T c, sn;
         jsincos(F.src.rot[e], &sn, &c);
@@ -817,7 +833,15 @@ __device__ void phase_near(const KArgs<T>& a, const Frame<T>& F, T* hullw) {
         const T cyc = np_pairwise_sum(my, V) / n_real;
         Best<T> b2 = {T(0), T(0), T(0), INT_MAX};
         for (int si = lane; si < a.S; si += 32) {
-            const T hx = hullw[2 * si], hy = hullw[2 * si + 1];
+            T hx, hy;
+            if (one_ship) {
+                hx = hullw[2 * si];
+                hy = hullw[2 * si + 1];
+            } else {
+                const T lx = a.hull[2 * si], ly = a.hull[2 * si + 1];
+                hx = lx * H.c_h + ly * (-H.s_h) + H.sx;
+                hy = lx * H.s_h + ly * H.c_h + H.sy;
+            }
             int crossings = 0;
             T dmin = T(0);
             int kbest = 0;
@@ -874,7 +898,6 @@ __device__ void phase_near(const KArgs<T>& a, const Frame<T>& F, T* hullw) {
 template <typename T>
 __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
     const DemParams& P = a.P;
-    const T sx = F.ship_src.eta[0], sy = F.ship_src.eta[1];
     const T wcf = T(P.w_contact_radius_factor), wcap = T(P.w_contact_cap);
     const T flex = T(P.flexural_strength_base);
     const T pcr = T(P.pen_crit_ref), pct = T(P.pen_crit_thickness_ref);
@@ -888,9 +911,13 @@ __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
         *a.comp_cnt = 0;   // P_CULL compacted the queue
     }
     for (int chunk = blockIdx.x; chunk < a.nchunks; chunk += gridDim.x) {
-        int e = chunk * kThreads + threadIdx.x;
+        // chunks of kThreads elements start at each system's first element, so a
+        // system's sums are grouped as they would be if it were simulated alone
+        const int2 ci = a.chunk_info[chunk];
+        const int e = ci.y + threadIdx.x;
+        const T sx = F.ship_src.eta[3 * ci.x], sy = F.ship_src.eta[3 * ci.x + 1];
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        if (e < a.n) {
+        if (e < a.sys_end[ci.x]) {
             typename vec2_of<T>::type p = ld2(F.src.pos, e);
             const T pen = a.cpen[e], nx = a.cnx[e], ny = a.cny[e];
             const bool has = pen > T(0);
@@ -1041,10 +1068,10 @@ __device__ void ship_step(const DemParams& P, const T* eta, const T* nu, const T
 
 // ─── P_REDUCE ───────────────────────────────────────────────────────────────
 template <typename T>
-__device__ void frame_totals(const KArgs<T>& a, double* tot3) {
-    // every CTA reduces the partials in the same fixed order
+__device__ void frame_totals(const KArgs<T>& a, int sys, double* tot3) {
+    // a CTA reduces one system's partials in a fixed order
     double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-    for (int i = threadIdx.x; i < a.nchunks; i += blockDim.x) {
+    for (int i = a.part_base[sys] + threadIdx.x; i < a.part_base[sys + 1]; i += blockDim.x) {
         v0 += a.part[3 * i];
         v1 += a.part[3 * i + 1];
         v2 += a.part[3 * i + 2];
@@ -1064,10 +1091,11 @@ __device__ __forceinline__ T thrust_scale_of(const KArgs<T>& a, const double* to
 template <typename T>
 __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     typedef typename vec2_of<T>::type V2;
-    if (blockIdx.x == 0) {
+    // one CTA per system: totals, thrust cap and the vessel step
+    for (int sys = blockIdx.x; sys < a.nsys; sys += gridDim.x) {
         __shared__ double tot3[3];
         double r[3];
-        frame_totals(a, r);
+        frame_totals(a, sys, r);
         if (threadIdx.x == 0) {
             tot3[0] = r[0];
             tot3[1] = r[1];
@@ -1078,46 +1106,53 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             const T scale = thrust_scale_of(a, tot3);
             // reaction on the ship (jax_simulation.py:470-478)
             T Fx = -(T(tot3[0]) * scale), Fy = -(T(tot3[1]) * scale), M = T(tot3[2]);
-            a.fscal[0] = (double)scale;
-            a.fscal[1] = (double)Fx;
-            a.fscal[2] = (double)Fy;
-            a.fscal[3] = (double)M;
+            double* fs = a.fscal + 4 * sys;
+            fs[0] = (double)scale;
+            fs[1] = (double)Fx;
+            fs[2] = (double)Fy;
+            fs[3] = (double)M;
             T tau[3] = {Fx, Fy, M};
             T J = jsqrt(Fx * Fx + Fy * Fy) * T(a.P.dt);
-            T sp[3] = {F.sp[0], F.sp[1], F.sp[2]};
-            const T* eta = F.ship_src.eta;
+            const T* spf = F.sp + 6 * sys;
+            T sp[3] = {spf[0], spf[1], spf[2]};
+            const T* eta = F.ship_src.eta + 3 * sys;
             if (a.P.ice_brake_threshold > 0.0) {  // jax_simulation.py:658-669
                 T thr = T(a.P.ice_brake_threshold);
                 T bf = jclip(thr / jmax(fabs(tau[0]), thr), T(0.1), T(1));
-                sp[0] = eta[0] + bf * (F.sp[0] - eta[0]);
-                sp[1] = eta[1] + bf * (F.sp[1] - eta[1]);
+                sp[0] = eta[0] + bf * (spf[0] - eta[0]);
+                sp[1] = eta[1] + bf * (spf[1] - eta[1]);
             }
+            const T vzero[2] = {T(0), T(0)};
+            const T* vws = F.vws ? F.vws + 2 * sys : vzero;
             T eta_o[3], nu_o[3], na_o[6], ei_o[3];
-            ship_step<T>(a.P, eta, F.ship_src.nu, F.ship_src.na, F.ship_src.ei, sp, F.sp + 3, tau, F.vws,
-                         eta_o, nu_o, na_o, ei_o);
+            ship_step<T>(a.P, eta, F.ship_src.nu + 3 * sys, F.ship_src.na + 6 * sys, F.ship_src.ei + 3 * sys, sp,
+                         spf + 3, tau, vws, eta_o, nu_o, na_o, ei_o);
             for (int i = 0; i < 3; ++i) {
-                F.ship_dst.eta[i] = eta_o[i];
-                F.ship_dst.nu[i] = nu_o[i];
-                F.ship_dst.ei[i] = ei_o[i];
+                F.ship_dst.eta[3 * sys + i] = eta_o[i];
+                F.ship_dst.nu[3 * sys + i] = nu_o[i];
+                F.ship_dst.ei[3 * sys + i] = ei_o[i];
             }
-            for (int i = 0; i < 6; ++i) F.ship_dst.na[i] = na_o[i];
+            for (int i = 0; i < 6; ++i) F.ship_dst.na[6 * sys + i] = na_o[i];
             if (a.d_F) {
-                a.d_F[0] = Fx;
-                a.d_F[1] = Fy;
+                a.d_F[2 * sys] = Fx;
+                a.d_F[2 * sys + 1] = Fy;
             }
-            if (a.d_J) a.d_J[0] = J;
+            if (a.d_J) a.d_J[sys] = J;
+            const size_t fs_i = (size_t)F.f * a.nsys + sys;
             if (a.h_eta)
-                for (int i = 0; i < 3; ++i) a.h_eta[F.f * 3 + i] = eta_o[i];
-            if (a.h_J) a.h_J[F.f] = J;
+                for (int i = 0; i < 3; ++i) a.h_eta[fs_i * 3 + i] = eta_o[i];
+            if (a.h_J) a.h_J[fs_i] = J;
             if (a.h_F) {
-                a.h_F[F.f * 2] = Fx;
-                a.h_F[F.f * 2 + 1] = Fy;
+                a.h_F[fs_i * 2] = Fx;
+                a.h_F[fs_i * 2 + 1] = Fy;
             }
         }
+        __syncthreads();  // tot3 is reused by this CTA's next system
     }
-    // CTA 0 runs the vessel step above; the other CTAs share the element and
-    // slot work (all CTAs when the grid has one)
-    const int c0 = (gridDim.x > 1) ? 1 : 0;
+    // With one system, CTA 0 runs the vessel step above and the other CTAs share
+    // the element and slot work (all CTAs when the grid has one); with several
+    // systems every CTA takes part in both.
+    const int c0 = (gridDim.x > 1 && a.nsys == 1) ? 1 : 0;
     if ((int)blockIdx.x < c0) return;
     const int gtid = (blockIdx.x - c0) * blockDim.x + threadIdx.x;
     const int gsz = (gridDim.x - c0) * blockDim.x;
@@ -1535,6 +1570,12 @@ __device__ __forceinline__ bool new_elig(const KArgs<T>& a, const Frame<T>& F, i
 }
 
 // ─── P_FRACTURE (jax_simulation.py:534-653) + history ───────────────────────
+// thrust-cap scale of system `sys` for this frame (one value when nsys == 1)
+template <typename T>
+__device__ __forceinline__ T sys_scale(const KArgs<T>& a, T scale1, int sys) {
+    return a.nsys == 1 ? scale1 : T(*((volatile double*)&a.fscal[4 * sys]));
+}
+
 template <typename T>
 __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
     const DemParams& P = a.P;
@@ -1574,8 +1615,9 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
             fli[k] = a.floe_of[i];
             flj[k] = a.floe_of[j];
             breakable[k] = (a.thick[i] <= mft) && (a.thick[j] <= mft);
-            fmi[k] = a.fraw[i] * scale;
-            fmj[k] = a.fraw[j] * scale;
+            const T sc = sys_scale(a, scale, a.nsys > 1 ? a.sys_of[i] : 0);  // i and j share a system
+            fmi[k] = a.fraw[i] * sc;
+            fmj[k] = a.fraw[j] * sc;
             at_crack[k] = a.crack[i] || a.crack[j];
             ds0[k] = F.src.ds[b];
             rest[k] = a.rest[b];
@@ -1590,8 +1632,9 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
 #pragma unroll
         for (int k = 0; k < kB; ++k) {
             if (!ok[k]) continue;
-            const bool ei = new_elig(a, F, fli[k], scale);
-            const bool ej = new_elig(a, F, flj[k], scale);
+            const T sc = sys_scale(a, scale, a.nsys > 1 ? a.floe_sys[fli[k]] : 0);
+            const bool ei = new_elig(a, F, fli[k], sc);
+            const bool ej = new_elig(a, F, flj[k], sc);
             floe_ok[k] = ei && ej;
         }
 #pragma unroll
@@ -1650,9 +1693,11 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
         if (a.h_rot) a.h_rot[(size_t)F.f * a.n + e] = F.dst.rot[e];
         if (a.h_sub) a.h_sub[(size_t)F.f * a.n + e] = F.dst.sub[e];
     }
-    for (int fl = gtid; fl < a.nf; fl += gsz) F.dst.elig[fl] = new_elig(a, F, fl, scale) ? 1 : 0;
+    for (int fl = gtid; fl < a.nf; fl += gsz)
+        F.dst.elig[fl] = new_elig(a, F, fl, sys_scale(a, scale, a.nsys > 1 ? a.floe_sys[fl] : 0)) ? 1 : 0;
     if (a.d_fmag)
-        for (int e = gtid; e < a.n; e += gsz) a.d_fmag[e] = a.fraw[e] * scale;
+        for (int e = gtid; e < a.n; e += gsz)
+            a.d_fmag[e] = a.fraw[e] * sys_scale(a, scale, a.nsys > 1 ? a.sys_of[e] : 0);
     for (int i = gtid; i < a.k_sub + 2; i += gsz) {
         a.esc_cnt[i] = 0u;
         a.dirty_cnt[i] = 0;

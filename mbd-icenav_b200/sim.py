@@ -126,7 +126,11 @@ class FrameStep:
                  ship_beam: float, n_ice_steps: int, dt: float, dt_ice: float,
                  use_auto_icenav: bool, B_mat, T_n: float, material: IceMaterial = DEFAULT_MATERIAL,
                  skin: float = 0.3, max_neighbors: int = 32, bucket_capacity: int = 32,
-                 device=None, dtype=None, launch_mode: int = _abi.DEM_LAUNCH_PERSISTENT):
+                 device=None, dtype=None, launch_mode: int = _abi.DEM_LAUNCH_PERSISTENT,
+                 system_start=None):
+        """``system_start`` (Q+1 element offsets) splits the field into Q independent
+        systems, each with its own ship; they step together through ``scan_segment``
+        with ship arrays of shape (Q, 3) / (Q, 6) and setpoints of shape (K, Q, 6)."""
         torch = _tm()
         self.lib = _abi.load_library()
         if device is None:
@@ -173,6 +177,12 @@ class FrameStep:
         S.sigma_bar_bond, S.initial_floe_of = _ptr(k["sbar"]), _ptr(k["floe"])
         S.k_n, S.k_s = float(static.k_n), float(static.k_s)
         S.ship_hull_local = _ptr(k["hull"])
+        self.n_systems = 1
+        if system_start is not None and len(system_start) > 2:
+            self.n_systems = len(system_start) - 1
+            self._sys_start = (C.c_int32 * len(system_start))(*[int(v) for v in system_start])
+            S.n_systems = self.n_systems
+            S.system_start = C.cast(self._sys_start, C.POINTER(C.c_int32))
         self.params = build_params(cfg, ship_dyn, ship_length, ship_beam, n_ice_steps, dt, dt_ice,
                                    use_auto_icenav, B_mat, T_n, material, skin, max_neighbors,
                                    bucket_capacity)
@@ -267,7 +277,8 @@ class FrameStep:
 
     def _alloc_ship(self) -> ShipState:
         torch = _tm()
-        e = lambda k: torch.empty(k, dtype=self.dtype, device=self.device)
+        qs = () if self.n_systems == 1 else (self.n_systems,)
+        e = lambda k: torch.empty(qs + (k,), dtype=self.dtype, device=self.device)
         return ShipState(eta=e(3), nu=e(3), n_actual=e(6), e_int=e(3))
 
     @staticmethod
@@ -355,8 +366,10 @@ class FrameStep:
         sp = f(setpoints_K6)
         vw = f(v_water_Kn2)
         K = int(sp.shape[0])
-        if sp.shape != (K, 6) or vw.shape != (K, self.n, 2):
-            raise ValueError("setpoints_K6 must be (K,6) and v_water_Kn2 (K,n,2)")
+        Q = self.n_systems
+        qs = () if Q == 1 else (Q,)
+        if tuple(sp.shape) != (K,) + qs + (6,) or vw.shape != (K, self.n, 2):
+            raise ValueError(f"setpoints_K6 must be {(K,) + qs + (6,)} and v_water_Kn2 (K,n,2)")
         vws = None if v_water_ship_K2 is None else f(v_water_ship_K2)
         out = self._alloc_state()
         sh_out = self._alloc_ship()
@@ -367,10 +380,10 @@ class FrameStep:
             hist = (torch.empty((K, self.n, 2), dtype=d, device=dev),
                     torch.empty((K, self.n), dtype=d, device=dev),
                     torch.empty((K, self.n_bonds), dtype=torch.bool, device=dev),
-                    torch.empty((K, 3), dtype=d, device=dev),
+                    torch.empty((K,) + qs + (3,), dtype=d, device=dev),
                     torch.empty((K, self.n), dtype=d, device=dev),
-                    torch.empty((K,), dtype=d, device=dev),
-                    torch.empty((K, 2), dtype=d, device=dev))
+                    torch.empty((K,) + qs, dtype=d, device=dev),
+                    torch.empty((K,) + qs + (2,), dtype=d, device=dev))
             chist = _abi.DemHistory(*[_ptr(t) for t in hist])
         cin, cout = self._c_state(st), self._c_state(out)
         sin, sout = self._c_ship(sh), self._c_ship(sh_out)
