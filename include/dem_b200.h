@@ -209,6 +209,20 @@ int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out,
                      const void* setpoints_K6, const void* v_water_Kn2,
                      const void* v_water_ship_K2, DemHistory* hist, void* stream);
 
+/* Planner rollouts (no single counterpart in the reference, whose planners roll
+ * the ship out alone, jax_vessel_dynamics.py:87-122): K frames of the frame step
+ * (jax_simulation.py:397-699) in which each system's ship is driven by controls
+ * instead of setpoints: tau = u + tau_ice (body frame) through ship_euler_step_jax
+ * (jax_vessel_dynamics.py:54-84) and the velocity clip (:233-243), as ship_step_jax
+ * (:246-348) with its controller replaced; RPMs and integral error are kept.
+ * controls_KQ3 (K, Q, 3) body-frame [X, Y, N] per frame and system (Q = n_systems,
+ * 1 for a plain field); v_water (K, n, 2); v_water_ship (K, Q, 2) or NULL; the
+ * history is that of dem_scan_segment. */
+int dem_rollout_segment(DemHandle* h, const DemIceState* in, DemIceState* out,
+                        const DemShipState* ship_in, DemShipState* ship_out, int32_t K,
+                        const void* controls_KQ3, const void* v_water_Kn2,
+                        const void* v_water_ship_KQ2, DemHistory* hist, void* stream);
+
 /* Synchronise `stream`, return and clear the device status word (DEM_OK if clean). */
 int dem_sync_status(DemHandle* h, void* stream);
 

@@ -109,7 +109,7 @@ class DemCostmapParams(C.Structure):
 
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
            "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_set_profiling",
-           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap")
+           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap", "dem_rollout_segment")
 
 _LIB = None
 
@@ -135,6 +135,9 @@ def load_library(path: str = None):
     lib.dem_scan_segment.argtypes = [H, C.POINTER(DemIceState), C.POINTER(DemIceState),
                                      C.POINTER(DemShipState), C.POINTER(DemShipState), _i,
                                      _vp, _vp, _vp, C.POINTER(DemHistory), _vp]
+    lib.dem_rollout_segment.argtypes = [H, C.POINTER(DemIceState), C.POINTER(DemIceState),
+                                        C.POINTER(DemShipState), C.POINTER(DemShipState), _i,
+                                        _vp, _vp, _vp, C.POINTER(DemHistory), _vp]
     lib.dem_sync_status.argtypes = [H, _vp]
     lib.dem_set_capacity.argtypes = [H, _i, _i]
     lib.dem_set_launch_mode.argtypes = [H, _i]

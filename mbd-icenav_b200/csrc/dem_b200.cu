@@ -270,9 +270,11 @@ int check_ship(DemHandle* h, const DemShipState* s, const char* what) {
 template <typename T>
 int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipState* ship_in,
            DemShipState* ship_out, int K, const void* setpoints, const void* vw, const void* vws,
-           const uint8_t* elig0, DemDiag* diag, DemHistory* hist, cudaStream_t stream) {
+           const uint8_t* elig0, DemDiag* diag, DemHistory* hist, cudaStream_t stream,
+           const void* u_ctrl = nullptr) {
     KArgs<T> a;
     std::memset(&a, 0, sizeof(a));
+    a.u_ctrl = (const T*)u_ctrl;
     a.P = h->P;
     a.n = h->n;
     a.V = h->V;
@@ -814,6 +816,31 @@ int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out, cons
                              in->dpdem_floe_eligible, nullptr, hist, st);
     return launch<double>(h, in, out, ship_in, ship_out, K, setpoints_K6, v_water_Kn2, v_water_ship_K2,
                           in->dpdem_floe_eligible, nullptr, hist, st);
+}
+
+int dem_rollout_segment(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipState* ship_in,
+                        DemShipState* ship_out, int32_t K, const void* controls_KQ3, const void* v_water_Kn2,
+                        const void* v_water_ship_KQ2, DemHistory* hist, void* stream) {
+    if (!h) return DEM_ERR_INVALID;
+    int rc;
+    if (K < 1) return set_err(h, DEM_ERR_INVALID, "K must be >= 1");
+    if ((long long)K * dem::phases_per_frame(h->P.n_ice_steps) > (long long)INT_MAX / 2)
+        return set_err(h, DEM_ERR_INVALID, "K = %d frames is too many for one call", (int)K);
+    if ((rc = check_state(h, in, "input"))) return rc;
+    if ((rc = check_state(h, out, "output"))) return rc;
+    if ((rc = check_ship(h, ship_in, "input"))) return rc;
+    if ((rc = check_ship(h, ship_out, "output"))) return rc;
+    if (!controls_KQ3 || !v_water_Kn2) return set_err(h, DEM_ERR_INVALID, "controls / v_water is NULL");
+    if (out->positions == in->positions || out->velocities == in->velocities || out->rotations == in->rotations ||
+        out->angular_vels == in->angular_vels)
+        return set_err(h, DEM_ERR_ALIAS, "output element kinematics alias the input");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (h->dtype == DEM_F32)
+        return launch<float>(h, in, out, ship_in, ship_out, K, nullptr, v_water_Kn2, v_water_ship_KQ2,
+                             in->dpdem_floe_eligible, nullptr, hist, st, controls_KQ3);
+    return launch<double>(h, in, out, ship_in, ship_out, K, nullptr, v_water_Kn2, v_water_ship_KQ2,
+                          in->dpdem_floe_eligible, nullptr, hist, st, controls_KQ3);
 }
 
 int dem_sync_status(DemHandle* h, void* stream) {

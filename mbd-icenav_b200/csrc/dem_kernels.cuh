@@ -104,6 +104,7 @@ struct KArgs {
     const int2* chunk_info;   // (nchunks) {system, first element} of each chunk of kThreads elements
     const int* sys_end;       // (nsys) one past each system's last element
     const int* part_base;     // (nsys + 1) first chunk of each system
+    const T* u_ctrl;          // (K, nsys, 3) body-frame ship controls of planner rollouts, or NULL
     int n_buckets, bucket_cap, max_nb, mode;
     T k_n, k_s, min_bstr, cell, skin, hull_r;
     T t_samp[kMaxEdgeSamples];
@@ -203,7 +204,7 @@ __device__ __forceinline__ Frame<T> make_frame(const KArgs<T>& a, int f) {
     F.ship_src = (f == 0) ? a.ship_in : a.ship_tmp[(f - 1) & 1];
     F.elig_in = (f == 0) ? a.elig0 : F.src.elig;
     F.vw = a.vw + (size_t)f * a.n * 2;
-    F.sp = a.setpoints + (size_t)f * a.nsys * 6;
+    F.sp = a.setpoints ? a.setpoints + (size_t)f * a.nsys * 6 : nullptr;
     F.vws = a.vws ? a.vws + (size_t)f * a.nsys * 2 : nullptr;
     return F;
 }
@@ -973,7 +974,7 @@ __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
 template <typename T>
 __device__ void ship_step(const DemParams& P, const T* eta, const T* nu, const T* na, const T* ei,
                           const T* sp, const T* spn, const T* tau_ice, const T* vws, T* eta_o,
-                          T* nu_o, T* na_o, T* ei_o) {
+                          T* nu_o, T* na_o, T* ei_o, const T* u_ctrl = nullptr) {
     const T pi = T(M_PI), two_pi = T(2.0 * M_PI);
     const T dtf = T(P.dt);
     T c = jcos(eta[2]), s = jsin(eta[2]);
@@ -987,62 +988,72 @@ __device__ void ship_step(const DemParams& P, const T* eta, const T* nu, const T
     tib[0] = (c * tau_ice[0] + s * tau_ice[1]) + T(0) * tau_ice[2];
     tib[1] = ((-s) * tau_ice[0] + c * tau_ice[1]) + T(0) * tau_ice[2];
     tib[2] = (T(0) * tau_ice[0] + T(0) * tau_ice[1]) + T(1) * tau_ice[2];
-    T dpsi_d = pymod(spn[2] - sp[2] + pi, two_pi) - pi;
-    T v_d[3] = {(spn[0] - sp[0]) / dtf, (spn[1] - sp[1]) / dtf, dpsi_d / dtf};
-    T nu_d[3];
-    nu_d[0] = (c * v_d[0] + s * v_d[1]) + T(0) * v_d[2];
-    nu_d[1] = ((-s) * v_d[0] + c * v_d[1]) + T(0) * v_d[2];
-    nu_d[2] = (T(0) * v_d[0] + T(0) * v_d[1]) + T(1) * v_d[2];
-    T tau_ff[3];
-    {
-        T DKt[9];
-        for (int i = 0; i < 9; ++i) DKt[i] = T(P.D3[i]) + T(P.Kd[i]);
-        for (int i = 0; i < 3; ++i)
-            tau_ff[i] = (DKt[3 * i] * nu_d[0] + DKt[3 * i + 1] * nu_d[1]) + DKt[3 * i + 2] * nu_d[2];
-    }
-    // dp_control (jax_vessel_dynamics.py:127-184): tau = -(R^T Kp) e - Kd nu - (R^T Ki) e_int
-    T e[3];
-    e[0] = eta[0] - sp[0];
-    e[1] = eta[1] - sp[1];
-    e[2] = pymod(eta[2] - sp[2] + pi, two_pi) - pi;
-    T Rt[9] = {c, s, T(0), -s, c, T(0), T(0), T(0), T(1)};
-    T RKp[9], RKi[9];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-            RKp[3 * i + j] = (Rt[3 * i] * T(P.Kp[j]) + Rt[3 * i + 1] * T(P.Kp[3 + j])) + Rt[3 * i + 2] * T(P.Kp[6 + j]);
-            RKi[3 * i + j] = (Rt[3 * i] * T(P.Ki[j]) + Rt[3 * i + 1] * T(P.Ki[3 + j])) + Rt[3 * i + 2] * T(P.Ki[6 + j]);
-        }
-    T a1[3], a2[3], a3[3];
-    for (int i = 0; i < 3; ++i) {
-        a1[i] = (RKp[3 * i] * e[0] + RKp[3 * i + 1] * e[1]) + RKp[3 * i + 2] * e[2];
-        a2[i] = (T(P.Kd[3 * i]) * nu[0] + T(P.Kd[3 * i + 1]) * nu[1]) + T(P.Kd[3 * i + 2]) * nu[2];
-        a3[i] = (RKi[3 * i] * ei[0] + RKi[3 * i + 1] * ei[1]) + RKi[3 * i + 2] * ei[2];
-    }
-    T tau_c[3];
-    for (int i = 0; i < 3; ++i) {
-        tau_c[i] = (-a1[i] - a2[i]) - a3[i];
-        ei_o[i] = ei[i] + dtf * e[i];
-    }
     T tau_act[3];
-    if (P.use_auto_icenav) {
-        T tc[3] = {tau_c[0] + tau_ff[0], tau_c[1] + tau_ff[1], tau_c[2] + tau_ff[2]};
-        T ncmd[6];
-        for (int i = 0; i < 6; ++i) {
-            T u = (T(P.B_pinv[3 * i]) * tc[0] + T(P.B_pinv[3 * i + 1]) * tc[1]) + T(P.B_pinv[3 * i + 2]) * tc[2];
-            T n_ = jsign(u) * jsqrt(fabs(u) + T(1e-12));
-            ncmd[i] = jclip(n_, -T(P.n_max[i]), T(P.n_max[i]));
-            na_o[i] = na[i] + dtf * (ncmd[i] - na[i]) / T(P.T_n);
-        }
-        T q[6];
-        for (int i = 0; i < 6; ++i) q[i] = fabs(na_o[i]) * na_o[i];
+    if (u_ctrl) {
+        // planner rollouts: the body-frame control replaces the DP controller
+        // and the thrust allocation (RPMs and integral error stay as they are)
         for (int i = 0; i < 3; ++i) {
-            T acc = T(P.B_mat[6 * i]) * q[0];
-            for (int j = 1; j < 6; ++j) acc = acc + T(P.B_mat[6 * i + j]) * q[j];
-            tau_act[i] = acc;
+            tau_act[i] = u_ctrl[i];
+            ei_o[i] = ei[i];
         }
-    } else {
-        for (int i = 0; i < 3; ++i) tau_act[i] = tau_c[i] + tau_ff[i];
         for (int i = 0; i < 6; ++i) na_o[i] = na[i];
+    } else {
+        T dpsi_d = pymod(spn[2] - sp[2] + pi, two_pi) - pi;
+        T v_d[3] = {(spn[0] - sp[0]) / dtf, (spn[1] - sp[1]) / dtf, dpsi_d / dtf};
+        T nu_d[3];
+        nu_d[0] = (c * v_d[0] + s * v_d[1]) + T(0) * v_d[2];
+        nu_d[1] = ((-s) * v_d[0] + c * v_d[1]) + T(0) * v_d[2];
+        nu_d[2] = (T(0) * v_d[0] + T(0) * v_d[1]) + T(1) * v_d[2];
+        T tau_ff[3];
+        {
+            T DKt[9];
+            for (int i = 0; i < 9; ++i) DKt[i] = T(P.D3[i]) + T(P.Kd[i]);
+            for (int i = 0; i < 3; ++i)
+                tau_ff[i] = (DKt[3 * i] * nu_d[0] + DKt[3 * i + 1] * nu_d[1]) + DKt[3 * i + 2] * nu_d[2];
+        }
+        // dp_control (jax_vessel_dynamics.py:127-184): tau = -(R^T Kp) e - Kd nu - (R^T Ki) e_int
+        T e[3];
+        e[0] = eta[0] - sp[0];
+        e[1] = eta[1] - sp[1];
+        e[2] = pymod(eta[2] - sp[2] + pi, two_pi) - pi;
+        T Rt[9] = {c, s, T(0), -s, c, T(0), T(0), T(0), T(1)};
+        T RKp[9], RKi[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                RKp[3 * i + j] = (Rt[3 * i] * T(P.Kp[j]) + Rt[3 * i + 1] * T(P.Kp[3 + j])) + Rt[3 * i + 2] * T(P.Kp[6 + j]);
+                RKi[3 * i + j] = (Rt[3 * i] * T(P.Ki[j]) + Rt[3 * i + 1] * T(P.Ki[3 + j])) + Rt[3 * i + 2] * T(P.Ki[6 + j]);
+            }
+        T a1[3], a2[3], a3[3];
+        for (int i = 0; i < 3; ++i) {
+            a1[i] = (RKp[3 * i] * e[0] + RKp[3 * i + 1] * e[1]) + RKp[3 * i + 2] * e[2];
+            a2[i] = (T(P.Kd[3 * i]) * nu[0] + T(P.Kd[3 * i + 1]) * nu[1]) + T(P.Kd[3 * i + 2]) * nu[2];
+            a3[i] = (RKi[3 * i] * ei[0] + RKi[3 * i + 1] * ei[1]) + RKi[3 * i + 2] * ei[2];
+        }
+        T tau_c[3];
+        for (int i = 0; i < 3; ++i) {
+            tau_c[i] = (-a1[i] - a2[i]) - a3[i];
+            ei_o[i] = ei[i] + dtf * e[i];
+        }
+        if (P.use_auto_icenav) {
+            T tc[3] = {tau_c[0] + tau_ff[0], tau_c[1] + tau_ff[1], tau_c[2] + tau_ff[2]};
+            T ncmd[6];
+            for (int i = 0; i < 6; ++i) {
+                T u = (T(P.B_pinv[3 * i]) * tc[0] + T(P.B_pinv[3 * i + 1]) * tc[1]) + T(P.B_pinv[3 * i + 2]) * tc[2];
+                T n_ = jsign(u) * jsqrt(fabs(u) + T(1e-12));
+                ncmd[i] = jclip(n_, -T(P.n_max[i]), T(P.n_max[i]));
+                na_o[i] = na[i] + dtf * (ncmd[i] - na[i]) / T(P.T_n);
+            }
+            T q[6];
+            for (int i = 0; i < 6; ++i) q[i] = fabs(na_o[i]) * na_o[i];
+            for (int i = 0; i < 3; ++i) {
+                T acc = T(P.B_mat[6 * i]) * q[0];
+                for (int j = 1; j < 6; ++j) acc = acc + T(P.B_mat[6 * i + j]) * q[j];
+                tau_act[i] = acc;
+            }
+        } else {
+            for (int i = 0; i < 3; ++i) tau_act[i] = tau_c[i] + tau_ff[i];
+            for (int i = 0; i < 6; ++i) na_o[i] = na[i];
+        }
     }
     T tau_tot[3] = {tau_act[0] + tib[0], tau_act[1] + tib[1], tau_act[2] + tib[2]};
     // ship_euler_step_jax (jax_vessel_dynamics.py:54-84)
@@ -1113,10 +1124,13 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             fs[3] = (double)M;
             T tau[3] = {Fx, Fy, M};
             T J = jsqrt(Fx * Fx + Fy * Fy) * T(a.P.dt);
-            const T* spf = F.sp + 6 * sys;
+            // rollouts drive the ship by controls (no setpoints, no ice brake)
+            const T* u = a.u_ctrl ? a.u_ctrl + ((size_t)F.f * a.nsys + sys) * 3 : nullptr;
+            const T zero6[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+            const T* spf = u ? zero6 : F.sp + 6 * sys;
             T sp[3] = {spf[0], spf[1], spf[2]};
             const T* eta = F.ship_src.eta + 3 * sys;
-            if (a.P.ice_brake_threshold > 0.0) {  // jax_simulation.py:658-669
+            if (!u && a.P.ice_brake_threshold > 0.0) {  // jax_simulation.py:658-669
                 T thr = T(a.P.ice_brake_threshold);
                 T bf = jclip(thr / jmax(fabs(tau[0]), thr), T(0.1), T(1));
                 sp[0] = eta[0] + bf * (spf[0] - eta[0]);
@@ -1126,7 +1140,7 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             const T* vws = F.vws ? F.vws + 2 * sys : vzero;
             T eta_o[3], nu_o[3], na_o[6], ei_o[3];
             ship_step<T>(a.P, eta, F.ship_src.nu + 3 * sys, F.ship_src.na + 6 * sys, F.ship_src.ei + 3 * sys, sp,
-                         spf + 3, tau, vws, eta_o, nu_o, na_o, ei_o);
+                         spf + 3, tau, vws, eta_o, nu_o, na_o, ei_o, u);
             for (int i = 0; i < 3; ++i) {
                 F.ship_dst.eta[3 * sys + i] = eta_o[i];
                 F.ship_dst.nu[3 * sys + i] = nu_o[i];

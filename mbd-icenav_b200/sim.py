@@ -358,18 +358,31 @@ class FrameStep:
         Returns ``(final_state, final_ship, (positions (K,n,2), rotations (K,n),
         bond_intact (K,n_bonds), eta (K,3), submergence (K,n), J_cumul_incr (K,),
         F_ice_on_ship (K,2)))``; with ``history=False`` the tuple is ``None``.
+        With Q systems the per-ship arrays gain a (Q,) axis after K.
         """
+        return self._segment(self.lib.dem_scan_segment, 6, state, ship_state, setpoints_K6, v_water_Kn2,
+                             v_water_ship_K2, history, check)
+
+    def rollout_segment(self, state: IceState, ship_state: ShipState, controls_K3, v_water_Kn2,
+                        v_water_ship_K2=None, history: bool = True, check: bool = True):
+        """K frames with every ship driven by body-frame controls [X, Y, N] instead of
+        setpoints (``dem_rollout_segment``): ``controls_K3`` is (K, 3), or (K, Q, 3) with
+        Q systems.  Returns what ``scan_segment`` returns."""
+        return self._segment(self.lib.dem_rollout_segment, 3, state, ship_state, controls_K3, v_water_Kn2,
+                             v_water_ship_K2, history, check)
+
+    def _segment(self, fn, row_len, state, ship_state, rows_K, v_water_Kn2, v_water_ship_K2, history, check):
         torch = _tm()
         st = self._ice_in(state)
         sh = self._ship_in(ship_state)
         f = lambda x: _as_tensor(x, self.dtype, self.device)
-        sp = f(setpoints_K6)
+        sp = f(rows_K)
         vw = f(v_water_Kn2)
         K = int(sp.shape[0])
         Q = self.n_systems
         qs = () if Q == 1 else (Q,)
-        if tuple(sp.shape) != (K,) + qs + (6,) or vw.shape != (K, self.n, 2):
-            raise ValueError(f"setpoints_K6 must be {(K,) + qs + (6,)} and v_water_Kn2 (K,n,2)")
+        if tuple(sp.shape) != (K,) + qs + (row_len,) or vw.shape != (K, self.n, 2):
+            raise ValueError(f"per-frame rows must be {(K,) + qs + (row_len,)} and v_water_Kn2 (K,n,2)")
         vws = None if v_water_ship_K2 is None else f(v_water_ship_K2)
         out = self._alloc_state()
         sh_out = self._alloc_ship()
@@ -387,9 +400,8 @@ class FrameStep:
             chist = _abi.DemHistory(*[_ptr(t) for t in hist])
         cin, cout = self._c_state(st), self._c_state(out)
         sin, sout = self._c_ship(sh), self._c_ship(sh_out)
-        self._run(self.lib.dem_scan_segment, C.byref(cin), C.byref(cout), C.byref(sin), C.byref(sout),
-                  K, _ptr(sp), _ptr(vw), _ptr(vws), C.byref(chist) if chist is not None else None,
-                  self._stream(), check=check)
+        self._run(fn, C.byref(cin), C.byref(cout), C.byref(sin), C.byref(sout), K, _ptr(sp), _ptr(vw), _ptr(vws),
+                  C.byref(chist) if chist is not None else None, self._stream(), check=check)
         return out, sh_out, hist
 
 

@@ -438,7 +438,9 @@ class Oracle:
 
     # ── frame step (jax_simulation.py:397-699) ──────────────────────────────
     def frame_step(self, st: OState, ship: OShip, setpoint, setpoint_next, v_water,
-                   dpdem_eligible, v_water_ship=None):
+                   dpdem_eligible, v_water_ship=None, u_ctrl=None):
+        """One frame (``jax_simulation.py:397-699``); ``u_ctrl`` (body-frame [X, Y, N])
+        drives the ship instead of the setpoints, as planner rollouts do."""
         p = self.p
         dt = self.dt_
         st = OState(*[np.asarray(a, dtype=(bool if np.asarray(a).dtype == bool else dt)) for a in st])
@@ -512,14 +514,18 @@ class Oracle:
             st = self.fracture(st, force_mag, new_active, new_elig)
         st = st._replace(dpdem_floe_eligible=new_elig)
         # 8. ship (jax_simulation.py:655-690)
-        if p.ice_brake_threshold > 0.0:
+        if u_ctrl is not None:
+            # planner rollouts: controls drive the ship (no setpoints, no ice brake)
+            z3 = np.zeros(3, dtype=dt)
+            ship_new = self.ship_step(ship, z3, z3, tau_ice, v_water_ship, u_ctrl=u_ctrl)
+        elif p.ice_brake_threshold > 0.0:
             surge = np.abs(tau_ice[0])
             bf = np.clip(p.ice_brake_threshold / np.maximum(surge, p.ice_brake_threshold), 0.1, 1.0)
             eff_sp = np.array([ship.eta[0] + bf * (setpoint[0] - ship.eta[0]),
                                ship.eta[1] + bf * (setpoint[1] - ship.eta[1]), setpoint[2]], dtype=dt)
+            ship_new = self.ship_step(ship, eff_sp, setpoint_next, tau_ice, v_water_ship)
         else:
-            eff_sp = setpoint
-        ship_new = self.ship_step(ship, eff_sp, setpoint_next, tau_ice, v_water_ship)
+            ship_new = self.ship_step(ship, setpoint, setpoint_next, tau_ice, v_water_ship)
         diag = {"pen_max": pen, "force_mag": force_mag,
                 "F_ice_on_ship": np.array([F_ship[0], F_ship[1]], dtype=dt),
                 "J_cumul_incr": (np.linalg.norm(tau_ice[:2]) * p.dt).astype(dt)}
@@ -574,12 +580,12 @@ class Oracle:
         return st._replace(bond_damage=nd.astype(dt), bond_delta_m_max=nmax.astype(dt),
                            bond_delta_m_0=n0.astype(dt), bond_delta_s=new_ds, bond_intact=final)
 
-    def ship_step(self, ship: OShip, setpoint, setpoint_next, tau_ice, v_water_ship) -> OShip:
+    def ship_step(self, ship: OShip, setpoint, setpoint_next, tau_ice, v_water_ship, u_ctrl=None) -> OShip:
         e, nu, na, ei = ship_step(ship.eta, ship.nu, ship.n_actual, ship.e_int, setpoint,
                                   setpoint_next, tau_ice, self.M3inv, self.D3, self.Kp, self.Kd,
                                   self.Ki, self.B_pinv, self.n_max, self.B_mat, self.p.T_n,
                                   self.p.dt, v_water_ship, self.p.use_auto_icenav,
-                                  self.p.vc_ship, self.dt_)
+                                  self.p.vc_ship, self.dt_, u_ctrl=u_ctrl)
         return OShip(e, nu, na, ei)
 
     # ── scan (jax_simulation.py:1308-1335) ──────────────────────────────────
@@ -722,15 +728,22 @@ def bond_damage_update(delta_n, delta_s, sigma_n, sigma_t, sigma_bar, C, mu_b, G
 
 
 def ship_step(eta, nu, n_actual, e_int, setpoint, setpoint_next, tau_ice, M3inv, D3, Kp, Kd, Ki,
-              B_pinv, n_max, B, T_n, dt_f, v_water_ship, use_auto, vc, dt):
+              B_pinv, n_max, B, T_n, dt_f, v_water_ship, use_auto, vc, dt, u_ctrl=None):
     """DP pole placement + feed-forward, allocation, propeller lag, Fossen Euler
-    (``jax_vessel_dynamics.py:246-348`` with ``:54-84``, ``:127-228``, ``:233-243``)."""
+    (``jax_vessel_dynamics.py:246-348`` with ``:54-84``, ``:127-228``, ``:233-243``).
+
+    With ``u_ctrl`` (body-frame [X, Y, N]) the control replaces the controller and
+    the allocation, as planner rollouts compose ``ship_euler_step_jax`` with the ice
+    force; RPMs and the integral error are kept."""
     pi = math.pi
     psi = eta[2]
     c, s = np.cos(psi), np.sin(psi)
     R = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]], dtype=dt)
     nu_c = (R.T @ np.array([v_water_ship[0], v_water_ship[1], 0.0], dtype=dt)).astype(dt)
     tau_ice_b = (R.T @ tau_ice).astype(dt)
+    if u_ctrl is not None:
+        return _euler_clip(eta, nu, np.asarray(u_ctrl, dt) + tau_ice_b, nu_c, M3inv, D3, dt_f, vc, dt) + (
+            np.asarray(n_actual, dt), np.asarray(e_int, dt))
     dpsi_d = (setpoint_next[2] - setpoint[2] + pi) % (2.0 * pi) - pi
     v_d = np.array([(setpoint_next[0] - setpoint[0]) / dt_f,
                     (setpoint_next[1] - setpoint[1]) / dt_f, dpsi_d / dt_f], dtype=dt)
@@ -752,6 +765,14 @@ def ship_step(eta, nu, n_actual, e_int, setpoint, setpoint_next, tau_ice, M3inv,
         tau_act = (tau_c + tau_ff).astype(dt)
         na_new = n_actual
     tau_tot = (tau_act + tau_ice_b).astype(dt)
+    return _euler_clip(eta, nu, tau_tot, nu_c, M3inv, D3, dt_f, vc, dt) + (np.asarray(na_new, dt), e_int_new)
+
+
+def _euler_clip(eta, nu, tau_tot, nu_c, M3inv, D3, dt_f, vc, dt):
+    """Fossen Euler step and velocity clip (``jax_vessel_dynamics.py:54-84``, ``:233-243``)."""
+    pi = math.pi
+    psi = eta[2]
+    tau_tot = np.asarray(tau_tot, dt)
     # Euler (jax_vessel_dynamics.py:54-84)
     nu_r = nu - nu_c
     nu_dot = M3inv @ (tau_tot - D3 @ nu_r)
@@ -763,4 +784,4 @@ def ship_step(eta, nu, n_actual, e_int, setpoint, setpoint_next, tau_ice, M3inv,
     eta_new = np.array([eta[0] + dt_f * vx, eta[1] + dt_f * vy, psi_new], dtype=dt)
     nu_new = np.array([np.clip(nu_new[0], -vc[0], vc[0]), np.clip(nu_new[1], -vc[1], vc[1]),
                        np.clip(nu_new[2], -vc[2], vc[2])], dtype=dt)
-    return eta_new, nu_new, np.asarray(na_new, dt), e_int_new
+    return eta_new, nu_new
