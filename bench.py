@@ -387,6 +387,143 @@ def run_ours(args, rank: int, world: int):
     return line
 
 
+ROLLOUT_METRIC = "planner rollouts/s"
+ROLLOUT_UNIT = "rollouts/s"
+
+
+def run_rollouts(args, rank: int, world: int):
+    """Batched planner rollouts: Q candidates x H control steps on their own ice
+    windows cut from the medium field, one persistent launch per batch plus the
+    device cost kernel; a step is one batch."""
+    import numpy as np
+    import torch
+    _pkg()
+    from mbd_icenav_b200 import rollouts
+    device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(device)
+    field = load_field("medium", args.seed)
+    dt = torch.float32 if args.dtype == "f32" else torch.float64
+    wl = rollouts.planner_workload(field, Q=args.rollouts, H=args.horizon, seed=args.seed + 1000 * rank, dtype=dt,
+                                   device=device, bucket_capacity=args.bucket_capacity, skin=args.skin)
+    b = wl.batch
+    fs = b.frame_step
+    Q, H = b.n_rollouts, args.horizon
+    n, nb, V = fs.n, fs.n_bonds, fs.max_v
+    K, W = args.steps, args.warmup
+    stream = torch.cuda.current_stream(device)
+    u_d = torch.as_tensor(wl.controls, dtype=dt, device=device)
+    vw = torch.zeros((H, n, 2), dtype=dt, device=device)  # still water
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+    cost_out = torch.empty((Q, 5), dtype=torch.float64, device=device)
+
+    def step(u, check=False):
+        res = rollouts.run(b, u, vw, history="ship", check=check)
+        mid = torch.cuda.Event(enable_timing=True)
+        mid.record(stream)
+        rollouts.costs(b, res, wl.costmap, wl.goal, wl.ship_length, wl.ship_beam, out=cost_out)
+        return res, mid
+
+    for _ in range(W):
+        step(u_d, check=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    mids = [None] * K
+    for attempt in range(4):
+        with ClockSampler(device.index) as clk:
+            torch.cuda.synchronize()
+            for i in range(K):
+                flush.fill_(i & 0xFF)  # evict L2 before every timed batch
+                starts[i].record(stream)
+                _, mids[i] = step(u_d)
+                ends[i].record(stream)
+            torch.cuda.synchronize()
+        rc = fs.lib.dem_sync_status(fs._h, fs._stream())
+        msg = fs._error() if rc != 0 else ""
+        grown = rc == _abi_mod().DEM_ERR_CAPACITY and attempt < 3 and fs.grow_capacity()
+        verdict = retry_verdict(rc, grown, world, device)
+        if verdict == 0:
+            break
+        if verdict == 2:
+            raise RuntimeError(f"device status {rc}: {msg}" if rc else "device error on another rank")
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    kern_ms = [s.elapsed_time(m) for s, m in zip(starts, mids)]
+    total_s = sum(step_ms) / 1e3
+    total_max = max_over_ranks(total_s, world, device)
+    value = world * Q * K / total_max
+
+    # end to end through the public API: per batch the controls go up from
+    # pinned host memory and the (Q, 5) costs come back, inside the timed region
+    E = max(1, min(K, 5))
+    u_h = torch.as_tensor(wl.controls, dtype=dt).pin_memory()
+    c_h = torch.empty((Q, 5), dtype=torch.float64, pin_memory=True)
+    u_in = torch.empty_like(u_d)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(E):
+        u_in.copy_(u_h, non_blocking=True)
+        step(u_in)
+        c_h.copy_(cost_out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_value = world * Q * E / max_over_ranks(e0.elapsed_time(e1) / 1e3, world, device)
+    rc = fs.lib.dem_sync_status(fs._h, fs._stream())
+    if rc != 0:
+        raise RuntimeError(f"device status {rc}: {fs._error()}")
+    c = c_h.numpy()
+    if not np.isfinite(c).all():
+        raise RuntimeError("non-finite rollout costs")
+    info = fs.info()
+    if rank != 0:
+        return None
+    sizes = np.diff(b.system_start)
+    bpl = H * algorithmic_bytes_per_frame(n, nb, V, N_SUB)
+    kern_s = sum(kern_ms) / 1e3 / K
+    achieved = bpl / kern_s / 1e9
+    peak, peak_kind = peak_hbm()
+    line = {
+        "metric": ROLLOUT_METRIC, "value": value, "unit": ROLLOUT_UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * total_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype, "data": "synthetic (seeded medium field, seeded Gaussian controls)",
+        "config": {"workload": f"batched planner rollouts: {Q} candidates x {H} control steps x {N_SUB} substeps, "
+                               f"windows of {int(sizes.min())}-{int(sizes.max())} elements (mean "
+                               f"{sizes.mean():.0f}) cut from the medium field along each path, "
+                               f"{wl.costmap.rows}x{wl.costmap.cols} costmap of 2 m cells + transferred ice KE",
+                   "rollouts": Q, "horizon": H, "elements": n, "bonds": nb, "seed": args.seed,
+                   "elem_steps_per_s": value * sizes.mean() * H * N_SUB,
+                   "l2": "flushed before every timed batch (256 MB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "launch": "one cooperative persistent kernel per batch (all H steps) + one cost kernel",
+                   "neighbor_rebuild_rounds": info["neighbor_rebuilds"],
+                   "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity,
+                   "skin_m": fs.params.skin,
+                   "mean_transferred_ke_J": float(c[:, 4].mean()),
+                   "rollouts_touching_ice": int((c[:, 4] > 0).sum())},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} copy bandwidth", "algorithmic_bytes_per_launch": bpl,
+                     "kernel_ms_per_launch": 1e3 * kern_s,
+                     "traffic": committed_traffic(f"rollouts-Q{Q}-H{H}-seed{args.seed}-{args.dtype}")},
+        "e2e": {"value": e2e_value, "unit": ROLLOUT_UNIT, "h2d_bytes_per_step": int(u_h.numel() * u_h.element_size()),
+                "d2h_bytes_per_step": int(c_h.numel() * c_h.element_size()), "steps": E},
+        "gpu_launches": 2 * K,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        m = int(round(sizes.mean()))
+        steps, secs, frames, nw = _oracle_frames(field, field.trajectory[START_FRAME], m, args.cpu_seconds,
+                                                 min_frames=2)
+        line["cpu_baseline"] = {"value": frames / secs / H, "unit": ROLLOUT_UNIT, "cores": 1, "kind": "port",
+                                "sample": f"NumPy oracle (float64), {frames} frames x {N_SUB} substeps on one "
+                                          f"{nw}-element window (the batch's mean window size) of the same field; "
+                                          f"rollouts/s = frames/s / {H} steps; one core"}
+    return line
+
+
 def print_phase_times(fs, st, sh, sp, vw, frames: int = 5):
     """Per-phase device time of a few frames (profiling switch of the library)."""
     import collections
@@ -523,7 +660,10 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["large", "medium", "small"], default="large")
+    ap.add_argument("--config", choices=["large", "medium", "small", "rollouts"], default="large",
+                    help="plain-DEM field, or batched planner rollouts on windows of the medium field")
+    ap.add_argument("--rollouts", type=int, default=2048, help="candidates per batch (--config rollouts)")
+    ap.add_argument("--horizon", type=int, default=64, help="control steps per candidate (--config rollouts)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     ap.add_argument("--e2e-steps", type=int, default=200)
@@ -554,7 +694,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        line = run_ours(args, rank, world)
+        line = run_rollouts(args, rank, world) if args.config == "rollouts" else run_ours(args, rank, world)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:

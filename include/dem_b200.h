@@ -203,7 +203,8 @@ int dem_frame_step(DemHandle* h, const DemIceState* in, DemIceState* out,
  * Each frame uses the previous frame's dpdem_floe_eligible (jax_simulation.py:1314).
  * With Q = n_systems > 1: ship states are (Q,3) / (Q,6) arrays, setpoints (K,Q,6),
  * v_water_ship (K,Q,2), and the history's eta (K,Q,3), J_cumul_incr (K,Q),
- * F_ice_on_ship (K,Q,2). */
+ * F_ice_on_ship (K,Q,2).  hist may be NULL, and so may any of its arrays (that
+ * row is then not written). */
 int dem_scan_segment(DemHandle* h, const DemIceState* in, DemIceState* out,
                      const DemShipState* ship_in, DemShipState* ship_out, int32_t K,
                      const void* setpoints_K6, const void* v_water_Kn2,
@@ -286,6 +287,40 @@ typedef struct DemCostmapParams {
 int dem_ke_costmap(int32_t dtype, int32_t n, const void* centroids, const void* radii,
                    const void* thicknesses, const void* masses, const DemCostmapParams* params,
                    float* grid, float* tmp, int32_t* flag, void* stream);
+
+/* Cost arguments of dem_rollout_costs: the planner's costmap query and cost
+ * terms (jax_mbd_planner.py:_make_query :128-168, _make_raw_components_fn
+ * :569-665, with the action normalisation of :2782-2783). */
+typedef struct DemRolloutCostParams {
+    double x_origin, y_origin;     /* costmap geometry (meta of the costmap)            */
+    double resolution;
+    int32_t rows, cols;
+    double oob_penalty;            /* added when a query leaves the grid's x-extent     */
+    double ship_length, ship_beam; /* hull centre + 4 box corners when both are > 0     */
+    double goal_x, goal_y;
+    double action_center[3];       /* u_norm = (u - center) / scale for the jerk term   */
+    double action_scale[3];
+    int32_t has_truncate;          /* cost_truncate_y given                             */
+    int32_t reserved;
+    double truncate_y;
+} DemRolloutCostParams;
+
+/* Per-rollout costs after dem_rollout_segment (no reference counterpart as a
+ * whole; each term follows the reference planner's).  For every system q of
+ * n_systems: the pose path eta0[q] (Q,3), eta_hist[:, q] (H,Q,3) (the pose
+ * history of the segment) gives out[q] = [costmap integral, path length,
+ * discounted goal distance, jerk, transferred kinetic energy] (Q,5) double,
+ * the first four in float32 arithmetic as _make_raw_components_fn
+ * (jax_mbd_planner.py:569-665) computes its raw components on the costmap
+ * grid (rows, cols) float32.  controls (H,Q,3) give the jerk (NULL: 0).
+ * masses (n,), vel0 and vel1 (n,2) (the segment's input and output ice
+ * velocities) with system_start (Q+1) give sum 0.5 m (|v1|^2 - |v0|^2) over
+ * each system's elements in double (all NULL: 0).  All arrays are device
+ * arrays of `dtype` (grid float32, system_start int32); 1 <= horizon <= 2000. */
+int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const int32_t* system_start,
+                      const void* eta0, const void* eta_hist, const void* controls, const float* grid,
+                      const DemRolloutCostParams* params, const void* masses, const void* vel0,
+                      const void* vel1, double* out, void* stream);
 
 /* Largest n accepted by dem_ship_contact_noalloc. */
 #define DEM_CONTACT_NOALLOC_MAX_ELEMENTS 262144

@@ -107,9 +107,17 @@ class DemCostmapParams(C.Structure):
                 ("dilate_half", _i), ("has_masses", _i)]
 
 
+class DemRolloutCostParams(C.Structure):
+    _fields_ = [("x_origin", _d), ("y_origin", _d), ("resolution", _d), ("rows", _i), ("cols", _i),
+                ("oob_penalty", _d), ("ship_length", _d), ("ship_beam", _d), ("goal_x", _d), ("goal_y", _d),
+                ("action_center", _d * 3), ("action_scale", _d * 3), ("has_truncate", _i), ("reserved", _i),
+                ("truncate_y", _d)]
+
+
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
            "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_set_profiling",
-           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap", "dem_rollout_segment")
+           "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap", "dem_rollout_segment",
+           "dem_rollout_costs")
 
 _LIB = None
 
@@ -148,6 +156,8 @@ def load_library(path: str = None):
     lib.dem_destroy.argtypes = [H]
     lib.dem_debug_fail_barrier.argtypes = [H, _i]
     lib.dem_ke_costmap.argtypes = [_i, _i, _vp, _vp, _vp, _vp, C.POINTER(DemCostmapParams), _vp, _vp, _vp, _vp]
+    lib.dem_rollout_costs.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, C.POINTER(DemRolloutCostParams), _vp,
+                                      _vp, _vp, _vp, _vp]
     lib.dem_version.restype = C.c_char_p
     for name in EXPORTS:
         if name != "dem_version":

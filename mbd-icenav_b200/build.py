@@ -19,7 +19,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB_NAME = "libdem_b200.so"
 LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
 
-SOURCES = [os.path.join(CSRC, "dem_b200.cu"), os.path.join(CSRC, "dem_costmap.cu")]
+SOURCES = [os.path.join(CSRC, f) for f in ("dem_b200.cu", "dem_costmap.cu", "dem_rollout.cu")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("dem_kernels.cuh", "dem_math.cuh")] + [
     os.path.join(INCLUDE, "dem_b200.h")]
 

@@ -249,9 +249,16 @@ __device__ __forceinline__ int2 cell_of(const KArgs<T>& a, T x, T y) {
     double cy = fmin(fmax(floor((double)y / (double)a.cell), -lim), lim);
     return make_int2((int)cx, (int)cy);
 }
-__device__ __forceinline__ int bucket_of(int2 c, int n_buckets) {
-    unsigned h = (unsigned)c.x * 73856093u ^ (unsigned)c.y * 19349663u;
+// The system id is part of the key: systems that occupy the same space (planner
+// rollouts on overlapping windows) hash their cells to different buckets, so a
+// neighbourhood scan reads its own system's entries only.
+__device__ __forceinline__ int bucket_of(int2 c, int sys, int n_buckets) {
+    unsigned h = (unsigned)c.x * 73856093u ^ (unsigned)c.y * 19349663u ^ (unsigned)sys * 83492791u;
     return (int)(h & (unsigned)(n_buckets - 1));
+}
+template <typename T>
+__device__ __forceinline__ int sys_id(const KArgs<T>& a, int e) {
+    return a.nsys > 1 ? a.sys_of[e] : 0;
 }
 
 // Neighbour lists are Verlet lists over reference positions: list(e) holds every
@@ -299,7 +306,7 @@ __device__ __forceinline__ void grid_put(const KArgs<T>& a, int e, T px, T py) {
     }
     int2 c = cell_of(a, px, py);
     a.ecell[e] = c;
-    int b = bucket_of(c, a.n_buckets);
+    int b = bucket_of(c, sys_id(a, e), a.n_buckets);
     int slot = atomicAdd(&a.bcnt[b], 1);
     if (slot < a.bucket_cap) {
         a.bitems[(size_t)b * a.bucket_cap + slot] = e;
@@ -320,10 +327,11 @@ __device__ __forceinline__ void warp_near_at(const KArgs<T>& a, int e, T px, T p
     if (c.x == INT_MIN) return;
     const double re = (double)a.radii[e] + (double)a.skin;
     // lanes 0..8 own one stencil bucket each; warp prefix of their fills
+    const int se = sys_id(a, e);
     int b = 0, m = 0;
     if (lane < 9) {
         const int2 cc = make_int2(c.x + (lane % 3) - 1, c.y + (lane / 3) - 1);
-        b = bucket_of(cc, a.n_buckets);
+        b = bucket_of(cc, se, a.n_buckets);
         m = min(a.bcnt[b], a.bucket_cap);
     }
     int incl = m;
@@ -352,7 +360,7 @@ __device__ __forceinline__ void warp_near_at(const KArgs<T>& a, int e, T px, T p
         // can show an old value (-1 or a valid stale index), never an invalid one
         const int o = ((volatile const int*)a.bitems)[(size_t)qb * a.bucket_cap + (t - qe)];
         if (o < 0 || o >= a.n || o == e) continue;
-        if (a.nsys > 1 && a.sys_of[o] != a.sys_of[e]) continue;  // systems never interact
+        if (a.nsys > 1 && a.sys_of[o] != se) continue;  // systems never interact
         const int2 cc = make_int2(c.x + (q % 3) - 1, c.y + (q / 3) - 1);
         const int2 oc = a.ecell[o];
         if (oc.x != cc.x || oc.y != cc.y) continue;  // stale entry or hash collision
@@ -372,7 +380,7 @@ __device__ __forceinline__ void block_near_at(const KArgs<T>& a, int e, T px, T 
     if (c.x == INT_MIN) return;  // depends on e only: uniform over the CTA
     if (threadIdx.x < 9) {
         const int2 cc = make_int2(c.x + ((int)threadIdx.x % 3) - 1, c.y + ((int)threadIdx.x / 3) - 1);
-        const int b = bucket_of(cc, a.n_buckets);
+        const int b = bucket_of(cc, sys_id(a, e), a.n_buckets);
         s_b[threadIdx.x] = b;
         s_start[threadIdx.x + 1] = min(a.bcnt[b], a.bucket_cap);
     }
@@ -529,8 +537,9 @@ __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int 
         a.pos_ref[2 * e] = px;
         a.pos_ref[2 * e + 1] = py;
         a.ecell[e] = c;
-        const int bo = (old.x != INT_MIN) ? bucket_of(old, a.n_buckets) : -1;
-        const int bn = (c.x != INT_MIN) ? bucket_of(c, a.n_buckets) : -1;
+        const int se = sys_id(a, e);
+        const int bo = (old.x != INT_MIN) ? bucket_of(old, se, a.n_buckets) : -1;
+        const int bn = (c.x != INT_MIN) ? bucket_of(c, se, a.n_buckets) : -1;
         const int slot = (bn >= 0) ? atomicAdd(&a.bcnt[bn], 1) : 0;
         const int fo = (bo >= 0) ? atomicExch(&a.bflag[bo], 1) : 1;
         const int fn = (bn >= 0 && bn != bo) ? atomicExch(&a.bflag[bn], 1) : 1;
@@ -587,7 +596,7 @@ __device__ void compact_buckets(const KArgs<T>& a) {
             bool keep = false;
             if (o >= 0 && o < a.n) {
                 const int2 c = a.ecell[o];
-                keep = c.x != INT_MIN && bucket_of(c, a.n_buckets) == b;
+                keep = c.x != INT_MIN && bucket_of(c, sys_id(a, o), a.n_buckets) == b;
             }
             for (int q = 0; keep && q < w; ++q)  // kept in earlier chunks
                 if (it[q] == o) keep = false;

@@ -1,0 +1,211 @@
+// dem_rollout.cu — per-rollout costs of a batch of planner rollouts.
+//
+// One CTA per rollout q, after dem_rollout_segment has stepped every rollout's
+// ship and ice window:
+//   * the reference planner's four unweighted cost components
+//     (medea_ice_ship/jax_mbd_planner.py:_make_raw_components_fn, :569-665) of
+//     the pose path eta0, eta_1 .. eta_H, in float32 as the planner runs them:
+//     costmap integral (bilinear query :128-168 at the hull centre and four
+//     box corners, maximum, trapezoid rule over segment lengths), path length,
+//     exponentially discounted goal distance, and jerk of the normalised
+//     controls; the optional goal-line truncation (:621-637) masks waypoints
+//     after the first crossing;
+//   * the kinetic energy the rollout transferred to its ice window,
+//     sum_e 0.5 m_e (|v_e(H)|^2 - |v_e(0)|^2) over the window's elements, in
+//     double with a fixed summation order (run to run identical).
+// Waypoint terms are computed one thread per waypoint into shared memory; the
+// sums over waypoints run in waypoint order on one thread.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "dem_b200.h"
+
+namespace {
+
+constexpr int kRcThreads = 128;
+constexpr int kRcMaxHorizon = 2000;  // 6 (H + 1) floats of shared memory stay under 48 KB
+
+struct RcArgs {
+    int Q, H, rows, cols, use_hull, has_truncate, has_jerk, has_ke;
+    float xo, yo, res, oob, hl, hw, gx, gy, trunc_y, tau;
+    float ac[3], as[3];
+};
+
+// jnp.max semantics: NaN wins
+__device__ __forceinline__ float max_nan(float a, float b) { return (a > b || a != a) ? a : b; }
+
+// _make_query (jax_mbd_planner.py:128-168) in float32
+__device__ __forceinline__ float query(const RcArgs& c, const float* __restrict__ g, float x, float y) {
+    const float cf = (x - c.xo) / c.res - 0.5f;
+    const float rf = (y - c.yo) / c.res - 0.5f;
+    const int r0 = (int)floorf(rf), c0 = (int)floorf(cf);
+    const float fr = rf - (float)r0, fc = cf - (float)c0;
+    const int r0c = min(max(r0, 0), c.rows - 1), r1c = min(max(r0 + 1, 0), c.rows - 1);
+    const int c0c = min(max(c0, 0), c.cols - 1), c1c = min(max(c0 + 1, 0), c.cols - 1);
+    const float oob = (c0 < 0 || c0 + 1 >= c.cols) ? c.oob : 0.0f;
+    const float g00 = __ldg(g + (size_t)r0c * c.cols + c0c), g01 = __ldg(g + (size_t)r0c * c.cols + c1c);
+    const float g10 = __ldg(g + (size_t)r1c * c.cols + c0c), g11 = __ldg(g + (size_t)r1c * c.cols + c1c);
+    const float val = g00 * (1.0f - fr) * (1.0f - fc) + g01 * (1.0f - fr) * fc + g10 * fr * (1.0f - fc) + g11 * fr * fc;
+    return val + oob;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRcThreads) rollout_cost_kernel(RcArgs c, const int* __restrict__ sys_start,
+                                                                  const T* __restrict__ eta0,
+                                                                  const T* __restrict__ eta_hist,
+                                                                  const T* __restrict__ u, const float* __restrict__ grid,
+                                                                  const T* __restrict__ masses,
+                                                                  const T* __restrict__ v0, const T* __restrict__ v1,
+                                                                  double* __restrict__ out) {
+    extern __shared__ float sm[];
+    const int H = c.H, W = H + 1, q = blockIdx.x;
+    float* wp = sm;            // (W) waypoint cost
+    float* tx = wp + W;        // (W) path x
+    float* ty = tx + W;        // (W) path y
+    float* dsc = ty + W;       // (W) undiscounted weights exp(-t / tau)
+    float* dd = dsc + W;       // (W) goal distance
+    float* jk = dd + W;        // (H) squared jerk of step t, summed over the 3 controls
+    __shared__ double s_ke[kRcThreads];
+    for (int t = threadIdx.x; t < W; t += blockDim.x) {
+        const T* p = (t == 0) ? eta0 + 3 * (size_t)q : eta_hist + 3 * ((size_t)(t - 1) * c.Q + q);
+        const float x = (float)p[0], y = (float)p[1], psi = (float)p[2];
+        float w;
+        if (c.use_hull) {
+            const float cs = cosf(psi), sn = sinf(psi);
+            const float dxb[5] = {0.0f, c.hl, c.hl, -c.hl, -c.hl};
+            const float dyb[5] = {0.0f, c.hw, -c.hw, c.hw, -c.hw};
+            w = 0.0f;
+            for (int k = 0; k < 5; ++k) {
+                const float wx = x + cs * dxb[k] - sn * dyb[k];
+                const float wy = y + sn * dxb[k] + cs * dyb[k];
+                const float v = query(c, grid, wx, wy);
+                w = (k == 0) ? v : max_nan(w, v);
+            }
+        } else {
+            w = query(c, grid, x, y);
+        }
+        wp[t] = w;
+        tx[t] = x;
+        ty[t] = y;
+        dsc[t] = expf(-(float)t / c.tau);
+        const float gdx = x - c.gx, gdy = y - c.gy;
+        dd[t] = sqrtf(gdx * gdx + gdy * gdy + 1e-4f);
+        if (t < H) {
+            float j = 0.0f;
+            if (c.has_jerk) {
+                for (int k = 0; k < 3; ++k) {
+                    const float a = ((float)u[3 * ((size_t)t * c.Q + q) + k] - c.ac[k]) / c.as[k];
+                    const float b = ((float)u[3 * ((size_t)(t + 1 < H ? t + 1 : t) * c.Q + q) + k] - c.ac[k]) / c.as[k];
+                    const float du = b - a;
+                    j = j + du * du;
+                }
+            }
+            jk[t] = j;
+        }
+    }
+    // kinetic energy transferred to the window (double, fixed order)
+    double ke = 0.0;
+    if (c.has_ke) {
+        const int e0 = sys_start[q], e1 = sys_start[q + 1];
+        for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+            const double m = (double)masses[e];
+            const double a0 = (double)v0[2 * (size_t)e], b0 = (double)v0[2 * (size_t)e + 1];
+            const double a1 = (double)v1[2 * (size_t)e], b1 = (double)v1[2 * (size_t)e + 1];
+            ke += 0.5 * m * ((a1 * a1 + b1 * b1) - (a0 * a0 + b0 * b0));
+        }
+    }
+    s_ke[threadIdx.x] = ke;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) s_ke[threadIdx.x] += s_ke[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    // goal-line truncation: waypoint t counts while max(y_0 .. y_{t-1}) < truncate_y
+    float cum = -1e9f, cost = 0.0f, len = 0.0f;
+    float mprev = (-1e9f < c.trunc_y) ? 1.0f : 0.0f;  // mask of waypoint 0
+    for (int t = 0; t < H; ++t) {
+        float m0 = 1.0f, m1 = 1.0f;
+        if (c.has_truncate) {
+            m0 = mprev;
+            cum = (t == 0) ? ty[0] : max_nan(cum, ty[t]);
+            m1 = (cum < c.trunc_y) ? 1.0f : 0.0f;  // mask of waypoint t + 1
+            mprev = m1;
+        }
+        const float dx = tx[t + 1] - tx[t], dy = ty[t + 1] - ty[t];
+        const float seg = sqrtf(dx * dx + dy * dy + 1e-8f);
+        len = len + seg * m0;
+        cost = cost + 0.5f * (wp[t] * m0 + wp[t + 1] * m1) * seg;
+    }
+    float dsum = 0.0f;
+    for (int t = 0; t < W; ++t) dsum = dsum + dsc[t];
+    float goal = 0.0f;
+    for (int t = 0; t < W; ++t) goal = goal + (dsc[t] / dsum) * dd[t];
+    float jsum = 0.0f;
+    for (int t = 0; t + 1 < H; ++t) jsum = jsum + jk[t];
+    const float jerk = c.has_jerk ? jsum / (float)(3 * (H - 1)) : 0.0f;
+    double* o = out + 5 * (size_t)q;
+    o[0] = (double)cost;
+    o[1] = (double)len;
+    o[2] = (double)goal;
+    o[3] = (double)jerk;
+    o[4] = s_ke[0];
+}
+
+template <typename T>
+int launch_costs(const RcArgs& c, const int32_t* sys_start, const void* eta0, const void* eta_hist,
+                 const void* u, const float* grid, const void* masses, const void* v0, const void* v1, double* out,
+                 cudaStream_t st) {
+    const size_t smem = sizeof(float) * (6 * (size_t)(c.H + 1));
+    rollout_cost_kernel<T><<<c.Q, kRcThreads, smem, st>>>(c, sys_start, (const T*)eta0, (const T*)eta_hist,
+                                                          (const T*)u, grid, (const T*)masses, (const T*)v0,
+                                                          (const T*)v1, out);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const int32_t* system_start,
+                                 const void* eta0, const void* eta_hist, const void* controls, const float* grid,
+                                 const DemRolloutCostParams* p, const void* masses, const void* vel0,
+                                 const void* vel1, double* out, void* stream) {
+    if (!p || !out || !eta0 || !eta_hist || !grid || (dtype != DEM_F32 && dtype != DEM_F64)) return DEM_ERR_INVALID;
+    if (n_systems < 1 || horizon < 1 || horizon > kRcMaxHorizon) return DEM_ERR_INVALID;
+    if (p->rows < 1 || p->cols < 1 || (long long)p->rows * p->cols >= (1LL << 31) || !(p->resolution > 0.0))
+        return DEM_ERR_INVALID;
+    const bool has_ke = masses || vel0 || vel1;
+    if (has_ke && (!masses || !vel0 || !vel1 || !system_start)) return DEM_ERR_INVALID;
+    if (controls)
+        for (int k = 0; k < 3; ++k)
+            if (!(p->action_scale[k] != 0.0) || !std::isfinite(p->action_scale[k])) return DEM_ERR_INVALID;
+    RcArgs c{};
+    c.Q = n_systems;
+    c.H = horizon;
+    c.rows = p->rows;
+    c.cols = p->cols;
+    c.use_hull = (p->ship_length > 0.0 && p->ship_beam > 0.0) ? 1 : 0;
+    c.has_truncate = p->has_truncate ? 1 : 0;
+    c.has_jerk = controls ? 1 : 0;
+    c.has_ke = has_ke ? 1 : 0;
+    // the planner's Python scalars meet float32 arrays: each is rounded to float
+    c.xo = (float)p->x_origin;
+    c.yo = (float)p->y_origin;
+    c.res = (float)p->resolution;
+    c.oob = (float)p->oob_penalty;
+    c.hl = (float)(p->ship_length / 2.0);
+    c.hw = (float)(p->ship_beam / 2.0);
+    c.gx = (float)p->goal_x;
+    c.gy = (float)p->goal_y;
+    c.trunc_y = (float)p->truncate_y;
+    c.tau = (float)((double)(horizon + 1) / 3.0);
+    for (int k = 0; k < 3; ++k) {
+        c.ac[k] = (float)p->action_center[k];
+        c.as[k] = (float)p->action_scale[k];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == DEM_F32)
+        return launch_costs<float>(c, system_start, eta0, eta_hist, controls, grid, masses, vel0, vel1, out, st);
+    return launch_costs<double>(c, system_start, eta0, eta_hist, controls, grid, masses, vel0, vel1, out, st);
+}

@@ -357,8 +357,10 @@ class FrameStep:
 
         Returns ``(final_state, final_ship, (positions (K,n,2), rotations (K,n),
         bond_intact (K,n_bonds), eta (K,3), submergence (K,n), J_cumul_incr (K,),
-        F_ice_on_ship (K,2)))``; with ``history=False`` the tuple is ``None``.
-        With Q systems the per-ship arrays gain a (Q,) axis after K.
+        F_ice_on_ship (K,2)))``; with ``history=False`` the tuple is ``None``, with
+        ``history="ship"`` only eta, J_cumul_incr and F_ice_on_ship are recorded
+        (the ice rows are ``None``).  With Q systems the per-ship arrays gain a
+        (Q,) axis after K.
         """
         return self._segment(self.lib.dem_scan_segment, 6, state, ship_state, setpoints_K6, v_water_Kn2,
                              v_water_ship_K2, history, check)
@@ -389,12 +391,15 @@ class FrameStep:
         hist = None
         chist = None
         if history:
+            if history not in (True, "ship"):
+                raise ValueError("history must be True, False or 'ship'")
             d, dev = self.dtype, self.device
-            hist = (torch.empty((K, self.n, 2), dtype=d, device=dev),
-                    torch.empty((K, self.n), dtype=d, device=dev),
-                    torch.empty((K, self.n_bonds), dtype=torch.bool, device=dev),
+            ice = history is True
+            hist = (torch.empty((K, self.n, 2), dtype=d, device=dev) if ice else None,
+                    torch.empty((K, self.n), dtype=d, device=dev) if ice else None,
+                    torch.empty((K, self.n_bonds), dtype=torch.bool, device=dev) if ice else None,
                     torch.empty((K,) + qs + (3,), dtype=d, device=dev),
-                    torch.empty((K, self.n), dtype=d, device=dev),
+                    torch.empty((K, self.n), dtype=d, device=dev) if ice else None,
                     torch.empty((K,) + qs, dtype=d, device=dev),
                     torch.empty((K,) + qs + (2,), dtype=d, device=dev))
             chist = _abi.DemHistory(*[_ptr(t) for t in hist])

@@ -8,7 +8,8 @@ exactly the API surface those files touch:
 * ``jax.jit`` (identity, with or without ``static_argnames``),
   ``jax.block_until_ready``, ``jax.config.update("jax_enable_x64", ...)``;
 * ``jax.lax.scan`` and ``jax.lax.fori_loop`` (eager Python loops);
-* about 40 ``jax.numpy`` creation / elementwise / reduction functions;
+* about 40 ``jax.numpy`` creation / elementwise / reduction functions
+  (``jnp.maximum.accumulate`` included);
 * the functional scatters ``x.at[idx].add/max/min/set`` mapped onto
   ``np.add.at`` / ``np.maximum.at`` / ``np.minimum.at`` / item assignment,
   which apply updates sequentially in index order.
@@ -195,8 +196,9 @@ def _make_jnp():
                  "power", "repeat", "roll", "sign", "sqrt", "stack", "sum", "tile",
                  "where", "exp", "log", "mean", "any", "all", "floor", "ceil",
                  "arctan2", "square", "dot", "matmul", "logical_and", "logical_or",
-                 "logical_not", "cumsum", "prod"):
+                 "logical_not", "cumsum", "prod", "diff"):
         setattr(m, name, _wrapfn(getattr(np, name)))
+    m.maximum.accumulate = _wrapfn(np.maximum.accumulate)
 
     linalg = types.ModuleType("jax.numpy.linalg")
 
