@@ -621,6 +621,8 @@ def run_reference(args):
     import multiprocessing as mp
     import numpy as np
     _pkg()
+    if args.config == "rollouts":
+        return run_reference_rollouts(args)
     field = load_field(args.config, args.seed)
     cores = len(os.sched_getaffinity(0))
     procs = max(1, min(cores, 32))
@@ -652,6 +654,41 @@ def run_reference(args):
                                        f"be installed in this image"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
+
+
+def run_reference_rollouts(args):
+    """Oracle port on all host cores for the rollout workload: each process rolls
+    out one candidate per step (H frames) on its own window of the medium field,
+    of the batch's mean window size."""
+    import multiprocessing as mp
+    import numpy as np
+    K, W, H = args.steps, args.warmup, args.horizon
+    field = load_field("medium", args.seed)
+    cores = len(os.sched_getaffinity(0))
+    procs = max(1, min(cores, 32))
+    n_keep = 1011  # mean window of the 2048-candidate batch (log-uniform 200-3000 elements)
+    rng = np.random.default_rng(args.seed)
+    near = np.argsort(np.linalg.norm(field.centroids - field.trajectory[START_FRAME][:2], axis=1))[:procs * 8]
+    centers = field.centroids[rng.choice(near, procs, replace=False)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        pool.map(_ref_worker, [("medium", args.seed, c, n_keep, 0.0, 1) for c in centers])  # warm-up
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [("medium", args.seed, c, n_keep, 0.0, H * K) for c in centers])
+        wall = time.perf_counter() - t0
+    rollouts_done = procs * K
+    value = rollouts_done / wall
+    sample = (f"{K} rollouts x {H} frames x {N_SUB} substeps per process on {procs} windows of "
+              f"{res[0][3]} elements near the ship (restated broad phase); the reference JAX code cannot be "
+              f"installed in this image")
+    return {"impl": "reference", "metric": ROLLOUT_METRIC, "value": value, "unit": ROLLOUT_UNIT, "n_gpus": 0,
+            "steps": K, "warmup": W, "ms_per_step": 1e3 * wall / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded medium field)",
+            "config": {"workload": f"planner rollouts, NumPy oracle port: {procs} processes, one candidate of "
+                                   f"{H} steps each per step", "processes": procs, "horizon": H,
+                       "elements_per_window": n_keep},
+            "cpu_baseline": {"value": value, "unit": ROLLOUT_UNIT, "cores": procs, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": ROLLOUT_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
