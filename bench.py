@@ -88,16 +88,28 @@ def load_field(name: str, seed: int):
     return f
 
 
-def algorithmic_bytes_per_frame(n: int, nb: int, V: int, k: int) -> int:
+def algorithmic_bytes_per_frame(n: int, nb: int, V: int, k: int, n_act=None, nb_act=None) -> int:
     """Bytes each frame must move at minimum, fp32, bool = 1 B, i32 = 4 B.
 
-    Per substep and element: read pos 8 + vel 8 + rot 4 + w 4 + sub 4 + active 1
-    + mass 4 + inertia 4 + radius 4 + area 4 + thickness 4 + ship force 8 +
-    v_water 8, write pos 8 + vel 8 + rot 4 + w 4 = 89 B; per substep and bond:
-    i 4 + j 4 + rest length 4 + damage 4 + intact 1 = 17 B.  Per frame: ship
-    contact n (9V + 64) B and the bond update 50 B per bond.
+    Per substep and active element: read pos 8 + vel 8 + rot 4 + w 4 + sub 4 +
+    active 1 + mass 4 + inertia 4 + radius 4 + area 4 + thickness 4 + ship force
+    8 + v_water 8, write pos 8 + vel 8 + rot 4 + w 4 = 89 B.  A frozen element
+    keeps its state whatever its forces (jax_simulation.py:257-262), so it only
+    carries it over: read pos, vel, rot, w, active, write pos, vel, rot, w = 49 B.
+    Per substep and bond with an active end: i 4 + j 4 + rest length 4 + damage
+    4 + intact 1 = 17 B (a bond between two frozen elements is not read).  Per
+    frame: ship contact n (9V + 64) B and the bond update 50 B per bond.
+    ``n_act`` / ``nb_act`` default to n / nb (every element active).
     """
-    return k * (89 * n + 17 * nb) + n * (9 * V + 64) + 50 * nb
+    n_act = n if n_act is None else n_act
+    nb_act = nb if nb_act is None else nb_act
+    return int(k * (89 * n_act + 49 * (n - n_act) + 17 * nb_act) + n * (9 * V + 64) + 50 * nb)
+
+
+def active_counts(elem_active, bond_i, bond_j):
+    """(active elements, bonds with an active end) of a state, on the device."""
+    a = elem_active.bool()
+    return int(a.sum().item()), int((a[bond_i.long()] | a[bond_j.long()]).sum().item())
 
 
 def peak_hbm():
@@ -258,6 +270,7 @@ def run_ours(args, rank: int, world: int):
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     st_w, sh_w, fr_w = st, sh, fr
+    act0 = active_counts(st.elem_active, static.bond_i, static.bond_j)
     for attempt in range(4):
         # the device status is read once after the timed frames; a capacity
         # overflow grows the scratch and times the same frames again (every rank
@@ -282,6 +295,8 @@ def run_ours(args, rank: int, world: int):
             raise RuntimeError(f"device status {rc}: {msg}" if rc else "device error on another rank")
     if world > 1:
         dist.barrier()
+    act1 = active_counts(st.elem_active, static.bond_i, static.bond_j)
+    n_act, nb_act = 0.5 * (act0[0] + act1[0]), 0.5 * (act0[1] + act1[1])
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_s = sum(frame_ms) / 1e3
     total_max = max_over_ranks(total_s, world, device)
@@ -351,7 +366,7 @@ def run_ours(args, rank: int, world: int):
 
     if rank != 0:
         return None
-    bpf = algorithmic_bytes_per_frame(n, nb, V, N_SUB)
+    bpf = algorithmic_bytes_per_frame(n, nb, V, N_SUB, n_act, nb_act)
     mean_s = total_s / K
     achieved = bpf / mean_s / 1e9
     peak, peak_kind = peak_hbm()
@@ -372,10 +387,12 @@ def run_ours(args, rank: int, world: int):
                    "elements_reref_total": info["escaped_total"],
                    "lists_rebuilt_total": info["rebuilt_lists_total"],
                    "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity,
-                   "skin_m": fs.params.skin},
+                   "skin_m": fs.params.skin,
+                   "active_elements": [act0[0], act1[0]], "bonds_with_active_end": [act0[1], act1[1]]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} copy bandwidth",
                      "algorithmic_bytes_per_launch": bpf,
+                     "algorithmic_bytes_if_all_active": algorithmic_bytes_per_frame(n, nb, V, N_SUB),
                      "traffic": traffic},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": E},
@@ -449,6 +466,10 @@ def run_rollouts(args, rank: int, world: int):
             break
         if verdict == 2:
             raise RuntimeError(f"device status {rc}: {msg}" if rc else "device error on another rank")
+    res_end, _ = step(u_d)
+    bi, bj = fs._keep["bi"], fs._keep["bj"]
+    act0 = active_counts(b.state.elem_active, bi, bj)
+    act1 = active_counts(res_end.state.elem_active, bi, bj)
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     kern_ms = [s.elapsed_time(m) for s, m in zip(starts, mids)]
     total_s = sum(step_ms) / 1e3
@@ -482,7 +503,7 @@ def run_rollouts(args, rank: int, world: int):
     if rank != 0:
         return None
     sizes = np.diff(b.system_start)
-    bpl = H * algorithmic_bytes_per_frame(n, nb, V, N_SUB)
+    bpl = H * algorithmic_bytes_per_frame(n, nb, V, N_SUB, 0.5 * (act0[0] + act1[0]), 0.5 * (act0[1] + act1[1]))
     kern_s = sum(kern_ms) / 1e3 / K
     achieved = bpl / kern_s / 1e9
     peak, peak_kind = peak_hbm()
@@ -502,10 +523,12 @@ def run_rollouts(args, rank: int, world: int):
                    "neighbor_rebuild_rounds": info["neighbor_rebuilds"],
                    "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity,
                    "skin_m": fs.params.skin,
+                   "active_elements": [act0[0], act1[0]], "bonds_with_active_end": [act0[1], act1[1]],
                    "mean_transferred_ke_J": float(c[:, 4].mean()),
                    "rollouts_touching_ice": int((c[:, 4] > 0).sum())},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} copy bandwidth", "algorithmic_bytes_per_launch": bpl,
+                     "algorithmic_bytes_if_all_active": H * algorithmic_bytes_per_frame(n, nb, V, N_SUB),
                      "kernel_ms_per_launch": 1e3 * kern_s,
                      "traffic": committed_traffic(f"rollouts-Q{Q}-H{H}-seed{args.seed}-{args.dtype}")},
         "e2e": {"value": e2e_value, "unit": ROLLOUT_UNIT, "h2d_bytes_per_step": int(u_h.numel() * u_h.element_size()),

@@ -1314,6 +1314,22 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
     const V4 ke = ld4(kin, e);  // x, y, radius, radius^3
     const V2 ve = ld2(kvin, e);
     const bool ae = cx.act[e] != 0;
+    if (!ae) {
+        // a frozen element keeps its state (jax_simulation.py:257-262) whatever its
+        // forces are, and no other element reads them (each element sums its own
+        // bond and contact forces): carry the state over, compute nothing
+        const T av0 = cx.ain[e], rot0 = cx.rin[e];
+        if (last) {
+            st2(F.dst.pos, e, ke.x, ke.y);
+            st2(F.dst.vel, e, ve.x, ve.y);
+        } else {
+            reinterpret_cast<V4*>(cx.kout)[e] = ke;
+            st2(cx.kvout, e, ve.x, ve.y);
+        }
+        cx.rout[e] = rot0;
+        cx.aout[e] = av0;
+        return !last && escaped(a, e, ke.x, ke.y);
+    }
     const int s0 = a.boff[e], s1 = a.boff[e + 1];
     const int nc = a.ncnt[e];
     const V4 ec = ld4(a.econ, e);  // mass, inertia, thickness, area
