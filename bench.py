@@ -516,6 +516,7 @@ def run_rollouts(args, rank: int, world: int):
                                f"{sizes.mean():.0f}) cut from the medium field along each path, "
                                f"{wl.costmap.rows}x{wl.costmap.cols} costmap of 2 m cells + transferred ice KE",
                    "rollouts": Q, "horizon": H, "elements": n, "bonds": nb, "seed": args.seed,
+                   "step_ms": [round(x, 3) for x in step_ms],
                    "elem_steps_per_s": value * sizes.mean() * H * N_SUB,
                    "l2": "flushed before every timed batch (256 MB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",

@@ -60,6 +60,8 @@ struct DemHandle {
     int* dirty_list = nullptr;
     int* dirty_cnt = nullptr;
     int* work_cnt = nullptr;
+    int* act_list = nullptr;
+    int* act_cnt = nullptr;
     int* slot_owner = nullptr;
     unsigned* esc_cnt = nullptr;
     int* near_list = nullptr;
@@ -340,6 +342,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.dirty_list = h->dirty_list;
     a.dirty_cnt = h->dirty_cnt;
     a.work_cnt = h->work_cnt;
+    a.act_list = h->act_list;
+    a.act_cnt = h->act_cnt;
     a.slot_owner = h->slot_owner;
     a.esc_cnt = h->esc_cnt;
     a.soi = (T*)h->soi;
@@ -647,6 +651,8 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->dirty_list, sizeof(int) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->dirty_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->work_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->esc_cnt, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);

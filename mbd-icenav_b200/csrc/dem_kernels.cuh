@@ -147,6 +147,8 @@ struct KArgs {
     int* dirty_list;    // (n) elements whose list is rebuilt
     int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
     int* work_cnt;      // (k_sub + 2) element chunks handed out dynamically, per substep
+    int* act_list;      // (n) elements active this frame (built by phase_reduce)
+    int* act_cnt;       // (1) entries of act_list
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
     int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
     ForceConst<T> fc;     // force-phase constants
@@ -713,6 +715,7 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
     const T reach = a.hull_r * T(1.0001) + T(1e-3);
     // nothing reads the grid in this phase: drop stale entries queued last frame
     compact_buckets(a);
+    if (gtid == 0) *a.act_cnt = 0;  // read last by the previous frame's force phases
     // per-floe scratch of this frame (read last by the previous frame's fracture)
     for (int fl = gtid; fl < a.nf; fl += gsz) {
         a.fcoll[fl] = 0;
@@ -1179,66 +1182,66 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     if ((int)blockIdx.x < c0) return;
     const int gtid = (blockIdx.x - c0) * blockDim.x + threadIdx.x;
     const int gsz = (gridDim.x - c0) * blockDim.x;
+    SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
+    typedef typename vec4_of<T>::type V4;
     for (int e = gtid; e < a.n; e += gsz) {
         // activation (jax_simulation.py:498-509)
         const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
         F.dst.active[e] = ae ? 1 : 0;
         // packed kinematics read by substep 0
         const V2 p = ld2(F.src.pos, e), v = ld2(F.src.vel, e);
-        typename vec4_of<T>::type k4;
+        V4 k4;
         k4.x = p.x;
         k4.y = p.y;
         k4.z = a.radii[e];
         k4.w = a.r3[e];
-        reinterpret_cast<typename vec4_of<T>::type*>(a.kin[0])[e] = k4;
+        reinterpret_cast<V4*>(a.kin[0])[e] = k4;
         st2(a.kvel[0], e, v.x, v.y);
-    }
-    // bond slot records for this frame; crack front = element touches a bond
-    // that is broken at frame start.  Four slots per thread and step, their
-    // loads issued level by level (slot -> endpoints -> floe flags).
-    SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
-    const int nsl = 2 * a.nb;
-    constexpr int kS = DEM_SLOT_BATCH;
-    for (int base = gtid; base < nsl; base += kS * gsz) {
-        int sl[kS], e[kS];
-        int2 ent[kS];
-#pragma unroll
-        for (int k = 0; k < kS; ++k) {
-            sl[k] = base + k * gsz;
-            if (sl[k] < nsl) {
-                e[k] = a.slot_owner[sl[k]];
-                ent[k] = a.bslot[sl[k]];
+        warp_append(a.act_list, a.act_cnt, ae, e);
+        if (!ae) {
+            // frozen for the whole frame, it keeps its state (jax_simulation.py:
+            // 257-262): both substep buffers and the frame's output hold it now,
+            // and the substeps skip the element
+            reinterpret_cast<V4*>(a.kin[1])[e] = k4;
+            st2(a.kvel[1], e, v.x, v.y);
+            st2(F.dst.pos, e, p.x, p.y);
+            st2(F.dst.vel, e, v.x, v.y);
+            F.dst.rot[e] = F.src.rot[e];
+            F.dst.avel[e] = F.src.avel[e];
+            continue;
+        }
+        // the bond slot records of an active element for this frame (only active
+        // elements read them); crack front = e touches a bond broken at frame
+        // start (read for bonds between two active elements only).  Two slots per
+        // step, their loads issued level by level (slot -> partner -> floe flag).
+        const int s0 = a.boff[e], s1 = a.boff[e + 1];
+        for (int sl = s0; sl < s1; sl += 2) {
+            const bool two = sl + 1 < s1;
+            const int2 ent0 = a.bslot[sl];
+            const int2 ent1 = two ? a.bslot[sl + 1] : ent0;
+            const int b0 = ent0.x & 0x7fffffff, b1 = ent1.x & 0x7fffffff;
+            const bool in0 = F.src.intact[b0] != 0, in1 = F.src.intact[b1] != 0;
+            const bool sa0 = F.src.active[ent0.y] != 0, sa1 = F.src.active[ent1.y] != 0;
+            const int fo0 = a.floe_of[ent0.y], fo1 = a.floe_of[ent1.y];
+            const T d0 = F.src.dmg[b0], d1 = F.src.dmg[b1];
+            const T r0 = a.slot_rest[sl], r1 = two ? a.slot_rest[sl + 1] : r0;
+            const T k0 = a.slot_stiff[sl], k1 = two ? a.slot_stiff[sl + 1] : k0;
+            const bool ao0 = sa0 || a.fcoll[fo0];
+            const bool ao1 = sa1 || a.fcoll[fo1];
+            if (!in0 || (two && !in1)) a.crack[e] = 1;
+            SlotRec<T> q;
+            q.o = (ent0.x < 0) ? (int)((unsigned)ent0.y | 0x80000000u) : ent0.y;
+            q.rest = r0;
+            q.stiff = k0;
+            q.omd = (in0 && ao0) ? T(1) - d0 : T(-1);  // e is active: both ends must be
+            rec[sl] = q;
+            if (two) {
+                q.o = (ent1.x < 0) ? (int)((unsigned)ent1.y | 0x80000000u) : ent1.y;
+                q.rest = r1;
+                q.stiff = k1;
+                q.omd = (in1 && ao1) ? T(1) - d1 : T(-1);
+                rec[sl + 1] = q;
             }
-        }
-        bool in[kS], sae[kS], sao[kS];
-        int fe[kS], fo[kS];
-        T dmg[kS], rest[kS], stiff[kS];
-#pragma unroll
-        for (int k = 0; k < kS; ++k) {
-            if (sl[k] >= nsl) continue;
-            const int b = ent[k].x & 0x7fffffff, o = ent[k].y;
-            in[k] = F.src.intact[b] != 0;
-            sae[k] = F.src.active[e[k]] != 0;
-            sao[k] = F.src.active[o] != 0;
-            fe[k] = a.floe_of[e[k]];
-            fo[k] = a.floe_of[o];
-            dmg[k] = F.src.dmg[b];
-            rest[k] = a.slot_rest[sl[k]];
-            stiff[k] = a.slot_stiff[sl[k]];
-        }
-#pragma unroll
-        for (int k = 0; k < kS; ++k) {
-            if (sl[k] >= nsl) continue;
-            if (!in[k]) a.crack[e[k]] = 1;
-            const bool ae = sae[k] || a.fcoll[fe[k]];
-            const bool ao = sao[k] || a.fcoll[fo[k]];
-            const int o = ent[k].y;
-            SlotRec<T> r;
-            r.o = (ent[k].x < 0) ? (int)((unsigned)o | 0x80000000u) : o;
-            r.rest = rest[k];
-            r.stiff = stiff[k];
-            r.omd = (in[k] && ao == ae) ? T(1) - dmg[k] : T(-1);
-            rec[sl[k]] = r;
         }
     }
 }
@@ -1291,8 +1294,131 @@ __device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<
     return c;
 }
 
-// Forces, torque and the semi-implicit update of element e for one substep;
-// returns whether e escaped its reference ball.
+// Bond slot term (jax_simulation.py:63-108) of a slot record with omd >= 0:
+// the force and half-moment that the slot's role adds to (role i) or
+// subtracts from (role j) the element's bond sums.
+template <typename T>
+__device__ __forceinline__ void bond_term(const SlotRec<T>& r, typename vec2_of<T>::type kb, T ex, T ey, T& fx,
+                                          T& fy, T& cr) {
+    const bool role_j = r.o < 0;
+    const T dx = role_j ? ex - kb.x : kb.x - ex;
+    const T dy = role_j ? ey - kb.y : kb.y - ey;
+    const T dist = jsqrt(dx * dx + dy * dy);
+    const T inv = jrcp(jmax(dist, T(1e-10)));
+    const T fmag = r.stiff * (dist - r.rest) * r.omd;
+    fx = (dx * inv) * fmag;
+    fy = (dy * inv) * fmag;
+    cr = T(0.5) * jfma(dx, fy, -(dy * fx));
+}
+
+// Ice-ice contact term (jax_simulation.py:111-164) of element e (kinematics
+// ke, ve) with candidate o (ko, vo); e_is_i = e < o.  Returns false when the
+// pair does not touch; else e adds (tx, ty) to its contact force and adds
+// (e_is_i) or subtracts hm from its contact moment.
+template <typename T>
+__device__ __forceinline__ bool contact_term(const ForceConst<T>& fc, bool h15, typename vec4_of<T>::type ke,
+                                             typename vec2_of<T>::type ve, typename vec4_of<T>::type ko,
+                                             typename vec2_of<T>::type vo, bool e_is_i, T& tx, T& ty, T& hm) {
+    const T dx = e_is_i ? ko.x - ke.x : ke.x - ko.x;
+    const T dy = e_is_i ? ko.y - ke.y : ke.y - ko.y;
+    const T d2 = dx * dx + dy * dy;
+    const T min_dist = e_is_i ? ke.z + ko.z : ko.z + ke.z;
+    // d2 > (min_dist (1 + 1e-5))^2, all roundings included, puts the rounded
+    // square root above min_dist, where the reference's overlap is exactly
+    // 0: such candidates skip the square root (NaN falls through)
+    const T mdm = min_dist * T(1.00001);
+    if (d2 > mdm * mdm) return false;
+    // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
+    const T dist = jsqrt(d2);
+    const T overlap = jmax(min_dist - dist, T(0));
+    if (!((dist > T(1e-6)) && (overlap > T(0)))) return false;
+    const T inv = jrcp(dist);
+    const T ux = dx * inv, uy = dy * inv;
+    const T fn = fc.hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, fc.hexp));
+    const T fnx = ux * fn, fny = uy * fn;
+    const T vrx = e_is_i ? vo.x - ve.x : ve.x - vo.x;
+    const T vry = e_is_i ? vo.y - ve.y : ve.y - vo.y;
+    const T vdot = jfma(vrx, ux, vry * uy);
+    const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
+    const T vtm = jsqrt(vtx * vtx + vty * vty);
+    T ftx = T(0), fty = T(0);
+    if (vtm > T(1e-6)) {
+        const T ftm = jmin(fc.mu * fn, fc.fcap) * jrcp(vtm);
+        ftx = -vtx * ftm;
+        fty = -vty * ftm;
+    }
+    const T oix = -fnx - ftx, oiy = -fny - fty;
+    const T cr = -jfma(dx, oiy, -(dy * oix));
+    tx = e_is_i ? ftx - fnx : fnx - ftx;
+    ty = e_is_i ? fty - fny : fny - fty;
+    hm = T(0.5) * cr;
+    return true;
+}
+
+// Drag, rotational drag and the semi-implicit update of an active element
+// from its bond and contact sums; stores the substep's output and returns
+// whether e escaped its reference ball.
+template <typename T>
+__device__ __forceinline__ bool integrate_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx, int e,
+                                                  typename vec4_of<T>::type ke, typename vec2_of<T>::type ve,
+                                                  typename vec4_of<T>::type ec, typename vec2_of<T>::type w, T sub,
+                                                  typename vec2_of<T>::type so, T av, T rot, T fbx, T fby, T mb,
+                                                  T fix, T fiy, T mi) {
+    typedef typename vec4_of<T>::type V4;
+    // drag (jax_simulation.py:167-192)
+    const T m = ec.x, inertia = ec.y, h = ec.z, A = ec.w;
+    const T a_drag = A * (h / a.fc.href);
+    const T vrx = ve.x - w.x, vry = ve.y - w.y;
+    const T vm = jsqrt(vrx * vrx + vry * vry);
+    T fdx, fdy;
+    if (vm > T(1e-6)) {
+        const T q = a.fc.c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
+        fdx = vrx * q;
+        fdy = vry * q;
+    } else {
+        const T cl = a.fc.c_drag * a_drag * a.fc.lin;
+        fdx = cl * vrx;
+        fdy = cl * vry;
+    }
+    // rotational drag (jax_simulation.py:195-212)
+    const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
+    const T md = a.fc.c_rot * ke.w * av * fabs(av) * a_sub;
+    const T Fx = ((fbx + fix) - fdx) + so.x;
+    const T Fy = ((fby + fiy) - fdy) + so.y;
+    const T Mz = (mb + mi) + md;
+    // semi-implicit Euler (jax_simulation.py:215-268)
+    const T dti = a.fc.dti, vclip = a.fc.vclip, pclip = a.fc.pclip;
+    T nvx = jclip(ve.x + (Fx / m) * dti, -vclip, vclip);
+    T nvy = jclip(ve.y + (Fy / m) * dti, -vclip, vclip);
+    T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
+    const T alpha = Mz / inertia;
+    const T nav = jclip(av * a.fc.damp + alpha * dti, a.fc.alo, a.fc.ahi);
+    const T nrot = rot + nav * dti;
+    if (!jfinite(nvx)) nvx = T(0);
+    if (!jfinite(nvy)) nvy = T(0);
+    if (!jfinite(npx)) npx = ke.x;
+    if (!jfinite(npy)) npy = ke.y;
+    npx = jclip(npx, -pclip, pclip);
+    npy = jclip(npy, -pclip, pclip);
+    if (cx.last) {
+        st2(F.dst.pos, e, npx, npy);
+        st2(F.dst.vel, e, nvx, nvy);
+    } else {
+        V4 v4;
+        v4.x = npx;
+        v4.y = npy;
+        v4.z = ke.z;
+        v4.w = ke.w;
+        reinterpret_cast<V4*>(cx.kout)[e] = v4;
+        st2(cx.kvout, e, nvx, nvy);
+    }
+    cx.rout[e] = nrot;
+    cx.aout[e] = nav;
+    return !cx.last && escaped(a, e, npx, npy);
+}
+
+// Forces, torque and the semi-implicit update of element e for one substep,
+// one thread per element; returns whether e escaped its reference ball.
 //
 // Latency layout: every load that depends only on e is issued first; then one
 // loop walks the bond slots and the contact candidates together, kBatch of
@@ -1308,18 +1434,16 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
     typedef typename vec4_of<T>::type V4;
     const T *kin = cx.kin, *kvin = cx.kvin;
     const SlotRec<T>* rec = cx.rec;
-    const T hf = a.fc.hf, hexp = a.fc.hexp, mu = a.fc.mu, fcap = a.fc.fcap;
-    const bool h15 = a.fc.h15 != 0, last = cx.last;
+    const bool h15 = a.fc.h15 != 0;
     // loads that depend on e only
     const V4 ke = ld4(kin, e);  // x, y, radius, radius^3
     const V2 ve = ld2(kvin, e);
-    const bool ae = cx.act[e] != 0;
-    if (!ae) {
+    if (!(cx.act[e] != 0)) {
         // a frozen element keeps its state (jax_simulation.py:257-262) whatever its
         // forces are, and no other element reads them (each element sums its own
         // bond and contact forces): carry the state over, compute nothing
         const T av0 = cx.ain[e], rot0 = cx.rin[e];
-        if (last) {
+        if (cx.last) {
             st2(F.dst.pos, e, ke.x, ke.y);
             st2(F.dst.vel, e, ve.x, ve.y);
         } else {
@@ -1328,7 +1452,7 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
         }
         cx.rout[e] = rot0;
         cx.aout[e] = av0;
-        return !last && escaped(a, e, ke.x, ke.y);
+        return !cx.last && escaped(a, e, ke.x, ke.y);
     }
     const int s0 = a.boff[e], s1 = a.boff[e + 1];
     const int nc = a.ncnt[e];
@@ -1338,7 +1462,6 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
     const V2 so = ld2(a.soi, e);
     const T av = cx.ain[e];
     const T rot = cx.rin[e];
-    const T re = ke.z;
     // bonds (jax_simulation.py:63-108) and ice-ice contacts (:111-164)
     T fbx = T(0), fby = T(0), mb = T(0);
     T fix = T(0), fiy = T(0), mi = T(0);
@@ -1372,15 +1495,9 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
             if (r[j].omd < T(0)) continue;  // no slot, broken, or active/frozen endpoints
-            const bool role_j = r[j].o < 0;
-            const T dx = role_j ? ke.x - kb[j].x : kb[j].x - ke.x;
-            const T dy = role_j ? ke.y - kb[j].y : kb[j].y - ke.y;
-            const T dist = jsqrt(dx * dx + dy * dy);
-            const T inv = jrcp(jmax(dist, T(1e-10)));
-            const T fmag = r[j].stiff * (dist - r[j].rest) * r[j].omd;
-            const T fx = (dx * inv) * fmag, fy = (dy * inv) * fmag;
-            const T cr = T(0.5) * jfma(dx, fy, -(dy * fx));
-            if (!role_j) {
+            T fx, fy, cr;
+            bond_term(r[j], kb[j], ke.x, ke.y, fx, fy, cr);
+            if (!(r[j].o < 0)) {
                 fbx += fx;
                 fby += fy;
                 mb += cr;
@@ -1395,105 +1512,92 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
             const int o = idx[j];
             if (o < 0) continue;
             const bool e_is_i = e < o;
-            const T dx = e_is_i ? ko[j].x - ke.x : ke.x - ko[j].x;
-            const T dy = e_is_i ? ko[j].y - ke.y : ke.y - ko[j].y;
-            const T d2 = dx * dx + dy * dy;
-            const T min_dist = e_is_i ? re + ko[j].z : ko[j].z + re;
-            // d2 > (min_dist (1 + 1e-5))^2, all roundings included, puts the rounded
-            // square root above min_dist, where the reference's overlap is exactly
-            // 0: such candidates skip the square root (NaN falls through)
-            const T mdm = min_dist * T(1.00001);
-            if (d2 > mdm * mdm) continue;
-            // the contact predicate, unfused as in the reference (jax_simulation.py:127-131)
-            const T dist = jsqrt(d2);
-            const T overlap = jmax(min_dist - dist, T(0));
-            if (!((dist > T(1e-6)) && (overlap > T(0)))) continue;
-            const T inv = jrcp(dist);
-            const T ux = dx * inv, uy = dy * inv;
-            const T fn = hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, hexp));
-            const T fnx = ux * fn, fny = uy * fn;
-            const T vrx = e_is_i ? vo[j].x - ve.x : ve.x - vo[j].x;
-            const T vry = e_is_i ? vo[j].y - ve.y : ve.y - vo[j].y;
-            const T vdot = jfma(vrx, ux, vry * uy);
-            const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
-            const T vtm = jsqrt(vtx * vtx + vty * vty);
-            T ftx = T(0), fty = T(0);
-            if (vtm > T(1e-6)) {
-                const T ftm = jmin(mu * fn, fcap) * jrcp(vtm);
-                ftx = -vtx * ftm;
-                fty = -vty * ftm;
-            }
-            const T oix = -fnx - ftx, oiy = -fny - fty;
-            const T cr = -jfma(dx, oiy, -(dy * oix));
-            if (e_is_i) {
-                fix += ftx - fnx;
-                fiy += fty - fny;
-                mi += T(0.5) * cr;
-            } else {
-                fix += fnx - ftx;
-                fiy += fny - fty;
-                mi -= T(0.5) * cr;
-            }
+            T tx, ty, hm;
+            if (!contact_term(a.fc, h15, ke, ve, ko[j], vo[j], e_is_i, tx, ty, hm)) continue;
+            fix += tx;
+            fiy += ty;
+            mi = e_is_i ? mi + hm : mi - hm;
         }
     }
-    // drag (jax_simulation.py:167-192)
-    const T m = ec.x, inertia = ec.y, h = ec.z, A = ec.w;
-    const T a_drag = A * (h / a.fc.href);
-    const T vrx = ve.x - w.x, vry = ve.y - w.y;
-    const T vm = jsqrt(vrx * vrx + vry * vry);
-    T fdx, fdy;
-    if (vm > T(1e-6)) {
-        const T q = a.fc.c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
-        fdx = vrx * q;
-        fdy = vry * q;
-    } else {
-        const T cl = a.fc.c_drag * a_drag * a.fc.lin;
-        fdx = cl * vrx;
-        fdy = cl * vry;
+    return integrate_element(a, F, cx, e, ke, ve, ec, w, sub, so, av, rot, fbx, fby, mb, fix, fiy, mi);
+}
+
+// The same substep for one active element computed by a whole warp: lane j
+// takes bond slot j and contact candidate j (32 at a time), so all partner
+// gathers are in flight at once; the terms are then summed in slot / candidate
+// order through shuffles, exactly as force_element adds them.  For substeps
+// with few active elements, where one element's chain of dependent gathers
+// decides the phase's length.  Every lane returns the escape flag.
+template <typename T>
+__device__ __forceinline__ bool force_element_warp(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
+                                                   int e) {
+    typedef typename vec2_of<T>::type V2;
+    typedef typename vec4_of<T>::type V4;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const T *kin = cx.kin, *kvin = cx.kvin;
+    const bool h15 = a.fc.h15 != 0;
+    const V4 ke = ld4(kin, e);
+    const V2 ve = ld2(kvin, e);
+    const int s0 = a.boff[e], s1 = a.boff[e + 1];
+    const int nc = a.ncnt[e];
+    const int nbe = s1 - s0;
+    const int m = max(nbe, nc);
+    T fbx = T(0), fby = T(0), mb = T(0);
+    T fix = T(0), fiy = T(0), mi = T(0);
+    for (int j0 = 0; j0 < m; j0 += 32) {
+        const int j = j0 + lane;
+        SlotRec<T> r;
+        r.o = 0;
+        r.omd = T(-1);
+        if (j < nbe) r = cx.rec[s0 + j];
+        const int o = (j < nc) ? a.nbr[(size_t)j * a.n + e] : -1;
+        const bool bv = r.omd >= T(0);
+        V2 kb;
+        V4 ko;
+        V2 vo;
+        if (bv) kb = reinterpret_cast<const V2*>(kin)[2 * (r.o & 0x7fffffff)];
+        if (o >= 0) {
+            ko = ld4(kin, o);
+            vo = ld2(kvin, o);
+        }
+        T bfx = T(0), bfy = T(0), bcr = T(0);
+        if (bv) bond_term(r, kb, ke.x, ke.y, bfx, bfy, bcr);
+        T tx = T(0), ty = T(0), hm = T(0);
+        const bool eis = e < o;
+        const bool cv = (o >= 0) && contact_term(a.fc, h15, ke, ve, ko, vo, eis, tx, ty, hm);
+        unsigned bm = __ballot_sync(full, bv);
+        const unsigned rm = __ballot_sync(full, bv && r.o < 0);
+        unsigned cm = __ballot_sync(full, cv);
+        const unsigned em = __ballot_sync(full, cv && eis);
+        while (bm) {  // warp-uniform trip count
+            const int l = __ffs(bm) - 1;
+            bm &= bm - 1;
+            const T x = __shfl_sync(full, bfx, l), y = __shfl_sync(full, bfy, l), c = __shfl_sync(full, bcr, l);
+            if ((rm >> l) & 1u) {
+                fbx -= x;
+                fby -= y;
+                mb -= c;
+            } else {
+                fbx += x;
+                fby += y;
+                mb += c;
+            }
+        }
+        while (cm) {
+            const int l = __ffs(cm) - 1;
+            cm &= cm - 1;
+            const T x = __shfl_sync(full, tx, l), y = __shfl_sync(full, ty, l), h = __shfl_sync(full, hm, l);
+            fix += x;
+            fiy += y;
+            mi = ((em >> l) & 1u) ? mi + h : mi - h;
+        }
     }
-    // rotational drag (jax_simulation.py:195-212)
-    const T a_sub = A * jmin(sub / jmax(h, T(1e-10)), T(1));
-    const T md = a.fc.c_rot * ke.w * av * fabs(av) * a_sub;
-    const T Fx = ((fbx + fix) - fdx) + so.x;
-    const T Fy = ((fby + fiy) - fdy) + so.y;
-    const T Mz = (mb + mi) + md;
-    // semi-implicit Euler (jax_simulation.py:215-268)
-    const T dti = a.fc.dti, vclip = a.fc.vclip, pclip = a.fc.pclip;
-    T nvx = jclip(ve.x + (Fx / m) * dti, -vclip, vclip);
-    T nvy = jclip(ve.y + (Fy / m) * dti, -vclip, vclip);
-    T npx = ke.x + nvx * dti, npy = ke.y + nvy * dti;
-    const T alpha = Mz / inertia;
-    T nav = jclip(av * a.fc.damp + alpha * dti, a.fc.alo, a.fc.ahi);
-    T nrot = rot + nav * dti;
-    if (!jfinite(nvx)) nvx = T(0);
-    if (!jfinite(nvy)) nvy = T(0);
-    if (!jfinite(npx)) npx = ke.x;
-    if (!jfinite(npy)) npy = ke.y;
-    npx = jclip(npx, -pclip, pclip);
-    npy = jclip(npy, -pclip, pclip);
-    if (!ae) {
-        nvx = ve.x;
-        nvy = ve.y;
-        npx = ke.x;
-        npy = ke.y;
-        nav = av;
-        nrot = rot;
-    }
-    if (last) {
-        st2(F.dst.pos, e, npx, npy);
-        st2(F.dst.vel, e, nvx, nvy);
-    } else {
-        V4 v4;
-        v4.x = npx;
-        v4.y = npy;
-        v4.z = re;
-        v4.w = ke.w;
-        reinterpret_cast<V4*>(cx.kout)[e] = v4;
-        st2(cx.kvout, e, nvx, nvy);
-    }
-    cx.rout[e] = nrot;
-    cx.aout[e] = nav;
-    return !last && escaped(a, e, npx, npy);
+    bool esc = false;
+    if (lane == 0)
+        esc = integrate_element(a, F, cx, e, ke, ve, ld4(a.econ, e), ld2(F.vw, e), F.dst.sub[e], ld2(a.soi, e),
+                                cx.ain[e], cx.rin[e], fbx, fby, mb, fix, fiy, mi);
+    return __shfl_sync(full, esc, 0);
 }
 
 template <typename T>
@@ -1514,7 +1618,8 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
         for (int q = warp; q < nd; q += nwarps) {
             const int e = a.dirty_list[q];
             warp_build(a, e, sbuf[wl], &scnt[wl]);
-            if (lane == 0 && force_element(a, F, cx, e)) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+            // a frozen element's substep buffers and output are written for the frame
+            if (cx.act[e] && force_element_warp(a, F, cx, e) && lane == 0) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
             __syncwarp();
         }
     }
@@ -1522,18 +1627,31 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     // (while enough warps remain), so they do not finish the phase last.
     const int skip = (nd < nwarps / 2) ? nd : 0;
     if (warp < skip) return;
-    // Chunks of 32 elements: every warp starts with one chunk of its own, then
-    // takes further chunks from a counter (the next grab is issued before the
-    // current chunk is computed), so uneven chunks do not leave warps idle.
-    const int nchunks = (a.n + 31) >> 5;
+    // Only active elements move (frozen ones were carried over by phase_reduce).
+    // Chunks of 32 active elements: every warp starts with one chunk of its own,
+    // then takes further chunks from a counter (the next grab is issued before
+    // the current chunk is computed), so uneven chunks do not leave warps idle.
+    const int na = *((volatile int*)a.act_cnt);
     const int nw2 = nwarps - skip;
+    if (na <= 2 * nw2) {
+        // at most two active elements per warp: a warp per element
+        for (int i = warp - skip; i < na; i += nw2) {
+            const int e = a.act_list[i];
+            if (has_dirty && a.dirty[e] == round) continue;
+            const bool esc = force_element_warp(a, F, cx, e);
+            if (!cx.last && esc && lane == 0) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+        }
+        return;
+    }
+    const int nchunks = (na + 31) >> 5;
     int c = warp - skip;
     int* ctr = &a.work_cnt[s];
     while (c < nchunks) {
         int next = 0;
         if (lane == 0) next = nw2 + atomicAdd(ctr, 1);
-        const int e = c * 32 + lane;
-        if (e < a.n && !(has_dirty && a.dirty[e] == round)) {
+        const int i = c * 32 + lane;
+        const int e = (i < na) ? a.act_list[i] : -1;
+        if (e >= 0 && !(has_dirty && a.dirty[e] == round)) {
             const bool esc = force_element(a, F, cx, e);
             if (!cx.last) warp_append(a.esc_list, esc_ctr, esc, e);
         }
