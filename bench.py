@@ -500,6 +500,9 @@ def run_rollouts(args, rank: int, world: int):
     if not np.isfinite(c).all():
         raise RuntimeError("non-finite rollout costs")
     info = fs.info()
+    if args.phase_times:
+        print_phase_times(fs, None, None, None, None, frames=1, frames_per_run=H,
+                          run=lambda: rollouts.run(b, u_d, vw, history="ship", check=False))
     if rank != 0:
         return None
     sizes = np.diff(b.system_start)
@@ -522,6 +525,8 @@ def run_rollouts(args, rank: int, world: int):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "launch": "one cooperative persistent kernel per batch (all H steps) + one cost kernel",
                    "neighbor_rebuild_rounds": info["neighbor_rebuilds"],
+                   "elements_reref_total": info["escaped_total"],
+                   "lists_rebuilt_total": info["rebuilt_lists_total"],
                    "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity,
                    "skin_m": fs.params.skin,
                    "active_elements": [act0[0], act1[0]], "bonds_with_active_end": [act0[1], act1[1]],
@@ -548,8 +553,10 @@ def run_rollouts(args, rank: int, world: int):
     return line
 
 
-def print_phase_times(fs, st, sh, sp, vw, frames: int = 5):
-    """Per-phase device time of a few frames (profiling switch of the library)."""
+def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_run: int = 1):
+    """Per-phase device time of a few frames (profiling switch of the library).
+    ``run()`` replaces the default one-frame scan (``frames`` calls of it, each
+    ``frames_per_run`` frames long)."""
     import collections
     import torch
     k = fs.n_ice_steps
@@ -559,7 +566,10 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5):
     acc = collections.defaultdict(list)
     fs.set_profiling(True)
     for _ in range(frames):
-        st, sh, _ = fs.scan_segment(st, sh, sp, vw, history=False)
+        if run is None:
+            st, sh, _ = fs.scan_segment(st, sh, sp, vw, history=False)
+        else:
+            run()
         torch.cuda.synchronize()
         pts = fs.phase_times()
         prev = 0
@@ -568,6 +578,7 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5):
             prev = t
     fs.set_profiling(False)
     tot = 0.0
+    frames = frames * frames_per_run
     for nm in ("cull", "near", "cforce", "reduce", "escape", "build_all", "force", "fracture"):
         v = acc.get(nm, [])
         s = sum(v) / frames

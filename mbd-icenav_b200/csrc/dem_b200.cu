@@ -302,6 +302,17 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     double cell = (2.0 * h->r_max + h->P.skin) * 1.0001;
     a.cell = (T)(cell > 1e-6 ? cell : 1.0);  // zero radii and skin: no pair can touch
     a.skin = (T)h->P.skin;
+    {
+        // escape period and thresholds (see the Verlet-list notes in dem_kernels.cuh)
+        const double S = h->P.skin;
+        const double dmax = std::sqrt(2.0) * std::fabs(h->P.velocity_clip) * h->P.dt_ice;
+        const double h_urgent = 0.45 * 0.99 * S;
+        const double h_two = 0.99 * (0.5 * S - dmax);
+        const bool two = std::isfinite(dmax) && h_two >= 0.25 * S;
+        a.esc_period = two ? 2 : 1;
+        a.esc_h_check = (T)(two ? std::min(h_two, h_urgent) : h_urgent);
+        a.esc_h_urgent = (T)h_urgent;
+    }
     a.hull_r = (T)h->hull_r;
     for (int i = 0; i < dem::kMaxEdgeSamples; ++i) a.t_samp[i] = (T)h->t_samp[i];
     a.polys = (const T*)h->S.local_polys_padded;

@@ -107,6 +107,11 @@ struct KArgs {
     const T* u_ctrl;          // (K, nsys, 3) body-frame ship controls of planner rollouts, or NULL
     int n_buckets, bucket_cap, max_nb, mode;
     T k_n, k_s, min_bstr, cell, skin, hull_r;
+    // escape thresholds: a substep whose successor is a check substep (s + 1 a
+    // multiple of esc_period) tests against esc_h_check, every other one
+    // against esc_h_urgent (the limit of an element's next use)
+    T esc_h_check, esc_h_urgent;
+    int esc_period;
     T t_samp[kMaxEdgeSamples];
     // static data (caller-owned)
     const T* polys;
@@ -265,23 +270,31 @@ __device__ __forceinline__ int sys_id(const KArgs<T>& a, int e) {
 
 // Neighbour lists are Verlet lists over reference positions: list(e) holds every
 // o with |ref_e - ref_o| < r_e + r_o + skin.  An element whose position leaves the
-// ball of radius 0.45 skin around its reference "escapes": it takes its current
+// ball of radius h around its reference "escapes": it takes its current
 // position as new reference, and every element within reach of that new
-// reference rebuilds its list.  With |p - ref| <= skin/2 for every element, any
-// pair closer than r_e + r_o is in both lists, so the contact set equals the
-// all-pairs one of the reference (jax_ice_state.py:212-214).
+// reference rebuilds its list.  With |p - ref| < skin/2 for every element at
+// every use of the lists, any pair closer than r_e + r_o is in both lists, so the
+// contact set equals the all-pairs one of the reference (jax_ice_state.py:212-214).
+//
+// Escapes are processed only before check substeps (s a multiple of the escape
+// period P, 1 or 2).  Before a check substep the test uses h = esc_h_check,
+// chosen so that h + (one substep's largest move, sqrt(2) vclip dt_ice) stays
+// below skin/2: the element is then safe through the next, unchecked substep.
+// Before any other substep the test uses h = esc_h_urgent = 0.4455 skin, the
+// limit for the very next use; only a move larger than that bound (an input
+// position outside the clip box) can trip it, and then the escape is processed
+// at once.  P = 1 (the default skin) tests every substep at 0.4455 skin.
 
 template <typename T>
-__device__ __forceinline__ bool escaped(const KArgs<T>& a, int e, T px, T py) {
+__device__ __forceinline__ bool escaped(const KArgs<T>& a, int e, T px, T py, T h) {
     const T rx = a.pos_ref[2 * e], ry = a.pos_ref[2 * e + 1];
     const bool fp = jfinite(px) && jfinite(py);
     const bool fr = jfinite(rx) && jfinite(ry);
     if (fp != fr) return true;
     if (!fp) return false;
-    // |p - ref| > 0.45 skin, evaluated with a 1 % lower threshold so rounding of
-    // the test can only make an element escape early, never late
+    // |p - ref| > h; h carries a 1 % margin so rounding of the test can only make
+    // an element escape early, never late
     const T dx = px - rx, dy = py - ry;
-    const T h = a.skin * T(0.45 * 0.99);
     return dx * dx + dy * dy > h * h;
 }
 
@@ -510,31 +523,50 @@ __device__ __forceinline__ void mark_dirty(const KArgs<T>& a, int o, int s, unsi
     if (atomicExch(&a.dirty[o], round) != round) a.dirty_list[atomicAdd(&a.dirty_cnt[s], 1)] = o;
 }
 
-// One rebuild round before substep s.  Work items 0..cnt-1 (one CTA each)
-// stamp dirty every element within reach of an escaped element's new
-// reference, and the element itself; items cnt..2cnt-1 (one thread each)
-// re-reference the escaped element and append it to its new home bucket.  The
-// two run concurrently: marking only needs the new position (from the packed
-// kinematics) and the references of elements that did not escape, which do
-// not move.  Marking is skipped when most elements escaped (every list is
-// then rebuilt).
+// One rebuild round before substep s.  Marking stamps dirty every element
+// within reach of an escaped element's new reference, and the element itself:
+// a CTA per escaped element when they fit one per CTA, else a warp each.
+// Re-referencing (a thread per escaped element) moves the element to its new
+// home bucket.  The two run concurrently: marking only needs the new position
+// (from the packed kinematics) and the references of elements that did not
+// escape, which do not move.  Marking is skipped when most elements escaped
+// (every list is then rebuilt).
 template <typename T>
 __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int s, unsigned round, bool all) {
-    const int items = all ? (int)cnt : 2 * (int)cnt;
-    for (int q = blockIdx.x; q < items; q += gridDim.x) {
-        const bool reref = all || q >= (int)cnt;
-        const int e = a.esc_list[reref && !all ? q - (int)cnt : q];
-        const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-        const bool fin = jfinite(px) && jfinite(py);
-        const int2 c = fin ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
-        if (!reref) {
-            block_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
-            if (threadIdx.x == 0) mark_dirty(a, e, s, round);
-            continue;
+    const int n_esc = (int)cnt;
+    if (!all) {
+        if (n_esc <= (int)gridDim.x) {
+            // few escapes: a CTA per element, its stencil entries in one load round
+            for (int q = blockIdx.x; q < n_esc; q += gridDim.x) {
+                const int e = a.esc_list[q];
+                const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+                const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+                block_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
+                if (threadIdx.x == 0) mark_dirty(a, e, s, round);
+            }
+        } else {
+            // many escapes (batched windows): a warp per element
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nwarps = (gridDim.x * blockDim.x) >> 5;
+            for (int q = warp; q < n_esc; q += nwarps) {
+                const int e = a.esc_list[q];
+                const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+                const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+                warp_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
+                if (lane == 0) mark_dirty(a, e, s, round);
+            }
         }
-        if (threadIdx.x != 0) continue;
-        // old and new buckets are queued for compaction at the next frame
-        // start; the independent atomics of each level are issued together
+    }
+    // re-reference: a thread per escaped element; old and new buckets are
+    // queued for compaction at the next frame start; the independent atomics of
+    // each level are issued together
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    for (int q = gtid; q < n_esc; q += gsz) {
+        const int e = a.esc_list[q];
+        const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+        const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
         const int2 old = a.ecell[e];
         a.pos_ref[2 * e] = px;
         a.pos_ref[2 * e + 1] = py;
@@ -739,7 +771,7 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
             a.cny[e] = T(0);
         }
         a.crack[e] = 0;  // set by phase_reduce for elements touching a broken bond
-        warp_append(a.esc_list, (int*)&a.esc_cnt[0], escaped(a, e, p.x, p.y), e);
+        warp_append(a.esc_list, (int*)&a.esc_cnt[0], escaped(a, e, p.x, p.y, a.esc_h_check), e);
     }
 }
 
@@ -1272,6 +1304,7 @@ struct ForceCtx {
     const T *kin, *kvin, *rin, *ain;
     T *kout, *kvout, *rout, *aout;
     const uint8_t* act;
+    T esc_h;  // escape threshold of this substep's test
     const SlotRec<T>* rec;
     bool last;
 };
@@ -1290,6 +1323,7 @@ __device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<
     c.rout = c.last ? F.dst.rot : a.sp_rot[s & 1];
     c.aout = c.last ? F.dst.avel : a.sp_avel[s & 1];
     c.act = F.dst.active;
+    c.esc_h = ((s + 1) % a.esc_period == 0) ? a.esc_h_check : a.esc_h_urgent;
     c.rec = reinterpret_cast<const SlotRec<T>*>(a.slotrec);
     return c;
 }
@@ -1414,7 +1448,7 @@ __device__ __forceinline__ bool integrate_element(const KArgs<T>& a, const Frame
     }
     cx.rout[e] = nrot;
     cx.aout[e] = nav;
-    return !cx.last && escaped(a, e, npx, npy);
+    return !cx.last && escaped(a, e, npx, npy, cx.esc_h);
 }
 
 // Forces, torque and the semi-implicit update of element e for one substep,
@@ -1452,7 +1486,7 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
         }
         cx.rout[e] = rot0;
         cx.aout[e] = av0;
-        return !cx.last && escaped(a, e, ke.x, ke.y);
+        return !cx.last && escaped(a, e, ke.x, ke.y, cx.esc_h);
     }
     const int s0 = a.boff[e], s1 = a.boff[e + 1];
     const int nc = a.ncnt[e];
@@ -1756,6 +1790,12 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
             ii[k] = ok[k] ? a.bi[bb[k]] : 0;
             jj[k] = ok[k] ? a.bj[bb[k]] : 0;
         }
+        // A bond between two frozen elements keeps its state: neither end touches
+        // the ship (a touched element's floe is active this frame), so both contact
+        // forces are 0, no DPDEM gate opens and no collision breaks it
+        bool frz[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) frz[k] = ok[k] && !F.dst.active[ii[k]] && !F.dst.active[jj[k]];
         V2 pi[kB], pj[kB], vi[kB], vj[kB];
         bool both_act[kB], breakable[kB], at_crack[kB], intact[kB];
         int fli[kB], flj[kB];
@@ -1764,6 +1804,12 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
         for (int k = 0; k < kB; ++k) {
             if (!ok[k]) continue;
             const int i = ii[k], j = jj[k], b = bb[k];
+            ds0[k] = F.src.ds[b];
+            cur_d[k] = F.src.dmg[b];
+            intact[k] = F.src.intact[b] != 0;
+            dmmax0[k] = F.src.dmmax[b];
+            dm00[k] = F.src.dm0[b];
+            if (frz[k]) continue;
             pi[k] = ld2(F.dst.pos, i);
             pj[k] = ld2(F.dst.pos, j);
             vi[k] = ld2(F.dst.vel, i);
@@ -1776,19 +1822,14 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
             fmi[k] = a.fraw[i] * sc;
             fmj[k] = a.fraw[j] * sc;
             at_crack[k] = a.crack[i] || a.crack[j];
-            ds0[k] = F.src.ds[b];
             rest[k] = a.rest[b];
-            cur_d[k] = F.src.dmg[b];
-            intact[k] = F.src.intact[b] != 0;
-            dmmax0[k] = F.src.dmmax[b];
-            dm00[k] = F.src.dm0[b];
             sbar[k] = a.sbar[b];
             bstr[k] = a.bstr[b];
         }
         bool floe_ok[kB];
 #pragma unroll
         for (int k = 0; k < kB; ++k) {
-            if (!ok[k]) continue;
+            if (!ok[k] || frz[k]) continue;
             const T sc = sys_scale(a, scale, a.nsys > 1 ? a.floe_sys[fli[k]] : 0);
             const bool ei = new_elig(a, F, fli[k], sc);
             const bool ej = new_elig(a, F, flj[k], sc);
@@ -1798,6 +1839,15 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
         for (int k = 0; k < kB; ++k) {
             if (!ok[k]) continue;
             const int b = bb[k];
+            if (frz[k]) {  // the full path's result for such a bond, without its loads
+                F.dst.dmg[b] = cur_d[k];
+                F.dst.dmmax[b] = dmmax0[k];
+                F.dst.dm0[b] = dm00[k];
+                F.dst.ds[b] = ds0[k] + T(0);
+                F.dst.intact[b] = intact[k] ? 1 : 0;
+                if (a.h_intact) a.h_intact[(size_t)F.f * a.nb + b] = intact[k] ? 1 : 0;
+                continue;
+            }
             T dx = pj[k].x - pi[k].x, dy = pj[k].y - pi[k].y;
             T dist = jsqrt(dx * dx + dy * dy);
             T dsafe = jmax(dist, T(1e-10));

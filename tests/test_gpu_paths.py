@@ -71,3 +71,37 @@ def test_capacity_overflow_is_retried_with_identical_results(golden32):
         assert torch.equal(a, b)
     ref.close()
     tight.close()
+
+
+def test_results_do_not_depend_on_the_skin_or_the_escape_period(golden64):
+    """Verlet lists are supersets of the touching pairs whatever the skin, and a
+    skin wide enough for the largest move of one substep processes escapes only
+    every second substep: the trajectories stay the same bit for bit."""
+    from helpers import SCENARIOS, default_cfg
+    g = golden64
+    prefix = "small"
+    K = 100
+    _, _, _, _, dti, _, _ = SCENARIOS[prefix]
+    vclip = float(default_cfg().velocity_clip[1])
+    dmax = np.sqrt(2.0) * vclip * dti
+    o_st, o_sh = initial_state(g, prefix, np.float64)
+    runs = {}
+    for skin in (0.3, 0.6, 1.2):
+        fs = gpu_frame_step(g, prefix, torch.float64, skin=skin)
+        st0, sh0 = to_gpu_state(o_st, o_sh, torch.float64)
+        runs[skin] = (fs.scan_segment(st0, sh0, *_scan_inputs(g, prefix, 0, K, torch.float64)),
+                      fs.info()["neighbor_rebuilds"])
+        fs.close()
+    assert 0.99 * (0.5 * 0.3 - dmax) < 0.25 * 0.3       # skin 0.3: every substep
+    assert 0.99 * (0.5 * 0.6 - dmax) >= 0.25 * 0.6      # skin 0.6: every second substep
+    (ref_st, ref_sh, ref_h), rounds_03 = runs[0.3]
+    for skin in (0.6, 1.2):
+        (st, sh, h), rounds = runs[skin]
+        for a, b in zip(ref_st, st):
+            assert torch.equal(a, b), skin
+        for a, b in zip(ref_sh, sh):
+            assert torch.equal(a, b), skin
+        for a, b in zip(ref_h, h):
+            assert torch.equal(a, b), skin
+        assert rounds < rounds_03, skin  # fewer rebuild rounds
+    assert rounds_03 > 0
