@@ -523,72 +523,104 @@ __device__ __forceinline__ void mark_dirty(const KArgs<T>& a, int o, int s, unsi
     if (atomicExch(&a.dirty[o], round) != round) a.dirty_list[atomicAdd(&a.dirty_cnt[s], 1)] = o;
 }
 
-// One rebuild round before substep s.  Marking stamps dirty every element
-// within reach of an escaped element's new reference, and the element itself:
-// a CTA per escaped element when they fit one per CTA, else a warp each.
-// Re-referencing (a thread per escaped element) moves the element to its new
-// home bucket.  The two run concurrently: marking only needs the new position
-// (from the packed kinematics) and the references of elements that did not
-// escape, which do not move.  Marking is skipped when most elements escaped
-// (every list is then rebuilt).
+// Move escaped element e to its new reference (px, py) and home bucket; old and
+// new buckets are queued for compaction at the next frame start, the
+// independent atomics of each level issued together.
+template <typename T>
+__device__ __forceinline__ void rereference(const KArgs<T>& a, int e, T px, T py, int2 c) {
+    const int2 old = a.ecell[e];
+    a.pos_ref[2 * e] = px;
+    a.pos_ref[2 * e + 1] = py;
+    a.ecell[e] = c;
+    const int se = sys_id(a, e);
+    const int bo = (old.x != INT_MIN) ? bucket_of(old, se, a.n_buckets) : -1;
+    const int bn = (c.x != INT_MIN) ? bucket_of(c, se, a.n_buckets) : -1;
+    const int slot = (bn >= 0) ? atomicAdd(&a.bcnt[bn], 1) : 0;
+    const int fo = (bo >= 0) ? atomicExch(&a.bflag[bo], 1) : 1;
+    const int fn = (bn >= 0 && bn != bo) ? atomicExch(&a.bflag[bn], 1) : 1;
+    if (bn >= 0) {
+        if (slot < a.bucket_cap) {
+            a.bitems[(size_t)bn * a.bucket_cap + slot] = e;
+        } else {
+            atomicMax(a.status, DEM_ERR_CAPACITY);
+            atomicOr((unsigned long long*)&a.stats[5], 1ull);  // a grid bucket overflowed
+        }
+        if (slot + 1 > a.bucket_cap / 2) atomicMax((unsigned long long*)&a.stats[2], (unsigned long long)(slot + 1));
+    }
+    if (fo == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = bo;
+    if (fn == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = bn;
+}
+
+// Whether o's list already holds e, whose reference was (rx, ry): o's list
+// was built with e's reference there, and it takes every element within
+// (r_o + skin + r_e)(1 + 1e-5) + 1e-6 of its own reference (warp_near_at, seen
+// from o).  The test is made a little stricter than the builder's, so rounding
+// can only send o to a needless rebuild.
+template <typename T>
+__device__ __forceinline__ bool list_holds(const KArgs<T>& a, int o, int e, double rx, double ry) {
+    const double dx = rx - (double)a.pos_ref[2 * o], dy = ry - (double)a.pos_ref[2 * o + 1];
+    const double lim = ((double)a.radii[o] + (double)a.skin + (double)a.radii[e]) * (1.0 + 1e-5) + 1e-6;
+    return dx * dx + dy * dy < lim * lim * (1.0 - 1e-9);
+}
+
+// One rebuild round before substep s.  For each escaped element e (a CTA each
+// when they fit one per CTA, else a warp each): e is stamped dirty, and so is
+// every element o within reach of e's new reference whose list does not hold e
+// yet (e was out of o's reach at its old reference).  An o whose list holds e
+// keeps it, and keeps an entry of an e that moved out of reach: such an entry is
+// a candidate that does not touch, whose terms are exact zeros, and it goes at
+// o's next rebuild.  The same unit then re-references e, after reading e's old
+// reference.  Candidates' references are read concurrently with other escaped
+// elements' re-referencing; those elements rebuild their own lists anyway.
+// When most elements escaped, every list is rebuilt instead (no marking).
 template <typename T>
 __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int s, unsigned round, bool all) {
     const int n_esc = (int)cnt;
-    if (!all) {
-        if (n_esc <= (int)gridDim.x) {
-            // few escapes: a CTA per element, its stencil entries in one load round
-            for (int q = blockIdx.x; q < n_esc; q += gridDim.x) {
-                const int e = a.esc_list[q];
-                const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-                const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
-                block_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
-                if (threadIdx.x == 0) mark_dirty(a, e, s, round);
-            }
-        } else {
-            // many escapes (batched windows): a warp per element
-            const int lane = threadIdx.x & 31;
-            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-            const int nwarps = (gridDim.x * blockDim.x) >> 5;
-            for (int q = warp; q < n_esc; q += nwarps) {
-                const int e = a.esc_list[q];
-                const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-                const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
-                warp_near_at(a, e, px, py, c, [&](int o) { mark_dirty(a, o, s, round); });
-                if (lane == 0) mark_dirty(a, e, s, round);
+    if (all) {
+        const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+        const int gsz = gridDim.x * blockDim.x;
+        for (int q = gtid; q < n_esc; q += gsz) {
+            const int e = a.esc_list[q];
+            const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+            const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+            rereference(a, e, px, py, c);
+        }
+    } else if (n_esc <= (int)gridDim.x) {
+        // few escapes: a CTA per element, its stencil entries in one load round
+        for (int q = blockIdx.x; q < n_esc; q += gridDim.x) {
+            const int e = a.esc_list[q];
+            const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+            const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+            const double rx = (double)a.pos_ref[2 * e], ry = (double)a.pos_ref[2 * e + 1];
+            const bool had = isfinite(rx) && isfinite(ry) && a.ecell[e].x != INT_MIN;
+            block_near_at(a, e, px, py, c, [&](int o) {
+                if (!(had && list_holds(a, o, e, rx, ry))) mark_dirty(a, o, s, round);
+            });  // ends with __syncthreads: every read of e's old reference is done
+            if (threadIdx.x == 0) {
+                mark_dirty(a, e, s, round);
+                rereference(a, e, px, py, c);
             }
         }
-    }
-    // re-reference: a thread per escaped element; old and new buckets are
-    // queued for compaction at the next frame start; the independent atomics of
-    // each level are issued together
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
-    for (int q = gtid; q < n_esc; q += gsz) {
-        const int e = a.esc_list[q];
-        const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
-        const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
-        const int2 old = a.ecell[e];
-        a.pos_ref[2 * e] = px;
-        a.pos_ref[2 * e + 1] = py;
-        a.ecell[e] = c;
-        const int se = sys_id(a, e);
-        const int bo = (old.x != INT_MIN) ? bucket_of(old, se, a.n_buckets) : -1;
-        const int bn = (c.x != INT_MIN) ? bucket_of(c, se, a.n_buckets) : -1;
-        const int slot = (bn >= 0) ? atomicAdd(&a.bcnt[bn], 1) : 0;
-        const int fo = (bo >= 0) ? atomicExch(&a.bflag[bo], 1) : 1;
-        const int fn = (bn >= 0 && bn != bo) ? atomicExch(&a.bflag[bn], 1) : 1;
-        if (bn >= 0) {
-            if (slot < a.bucket_cap) {
-                a.bitems[(size_t)bn * a.bucket_cap + slot] = e;
-            } else {
-                atomicMax(a.status, DEM_ERR_CAPACITY);
-                atomicOr((unsigned long long*)&a.stats[5], 1ull);  // a grid bucket overflowed
+    } else {
+        // many escapes (batched windows): a warp per element
+        const int lane = threadIdx.x & 31;
+        const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int nwarps = (gridDim.x * blockDim.x) >> 5;
+        for (int q = warp; q < n_esc; q += nwarps) {
+            const int e = a.esc_list[q];
+            const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+            const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+            const double rx = (double)a.pos_ref[2 * e], ry = (double)a.pos_ref[2 * e + 1];
+            const bool had = isfinite(rx) && isfinite(ry) && a.ecell[e].x != INT_MIN;
+            warp_near_at(a, e, px, py, c, [&](int o) {
+                if (!(had && list_holds(a, o, e, rx, ry))) mark_dirty(a, o, s, round);
+            });
+            __syncwarp();  // every lane is done with e's old reference
+            if (lane == 0) {
+                mark_dirty(a, e, s, round);
+                rereference(a, e, px, py, c);
             }
-            if (slot + 1 > a.bucket_cap / 2)
-                atomicMax((unsigned long long*)&a.stats[2], (unsigned long long)(slot + 1));
         }
-        if (fo == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = bo;
-        if (fn == 0) a.comp_list[atomicAdd(a.comp_cnt, 1)] = bn;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd((unsigned long long*)&a.stats[0], 1ull);
