@@ -188,7 +188,7 @@ class ClockSampler:
                 "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def build_stepper(field, dtype_name: str, device, bucket_capacity: int = 64, skin: float = 0.3):
+def build_stepper(field, dtype_name: str, device, bucket_capacity: int = 64, skin: float = 0.8):
     import numpy as np
     import torch
     from mbd_icenav_b200 import sim
@@ -742,7 +742,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch", choices=["persistent", "phased"], default="persistent")
-    ap.add_argument("--skin", type=float, default=0.3, help="Verlet skin of the neighbour lists [m]")
+    ap.add_argument("--skin", type=float, default=0.8, help="Verlet skin of the neighbour lists [m]")
     ap.add_argument("--bucket-capacity", type=int, default=64,
                     help="grid-bucket capacity at start (grown automatically on overflow)")
     ap.add_argument("--order", choices=["floe", "morton"], default="floe",

@@ -733,28 +733,41 @@ __device__ __forceinline__ void hull_point(const HullPose<T>& H, T px, T py, T& 
     pen = jmax(praw, T(0));
 }
 
-// ─── fixed-order block sum (deterministic, independent of the grid size) ────
+// ─── fixed-order sums (deterministic, independent of the grid size) ─────────
+// lane 0 receives the warp's sum (shuffle-down tree)
+__device__ __forceinline__ double warp_sum_lane0(double v) {
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// thread 0 receives the block's sums: a tree in each warp, then over the warps
 template <int N>
 __device__ __forceinline__ void block_sum3(double v0, double v1, double v2, double* out3) {
-    __shared__ double sh[3][N];
-    sh[0][threadIdx.x] = v0;
-    sh[1][threadIdx.x] = v1;
-    sh[2][threadIdx.x] = v2;
+    constexpr int kW = N / 32;
+    __shared__ double sh[3][kW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v0 = warp_sum_lane0(v0);
+    v1 = warp_sum_lane0(v1);
+    v2 = warp_sum_lane0(v2);
+    if (lane == 0) {
+        sh[0][w] = v0;
+        sh[1][w] = v1;
+        sh[2][w] = v2;
+    }
     __syncthreads();
-    for (int w = N / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
-            sh[2][threadIdx.x] += sh[2][threadIdx.x + w];
+    if (w == 0) {
+        double u0 = lane < kW ? sh[0][lane] : 0.0, u1 = lane < kW ? sh[1][lane] : 0.0;
+        double u2 = lane < kW ? sh[2][lane] : 0.0;
+        u0 = warp_sum_lane0(u0);
+        u1 = warp_sum_lane0(u1);
+        u2 = warp_sum_lane0(u2);
+        if (lane == 0) {
+            out3[0] = u0;
+            out3[1] = u1;
+            out3[2] = u2;
         }
-        __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out3[0] = sh[0][0];
-        out3[1] = sh[1][0];
-        out3[2] = sh[2][0];
-    }
-    __syncthreads();
+    __syncthreads();  // sh is reused by the next call
 }
 
 template <typename T>
@@ -1154,16 +1167,19 @@ __device__ void ship_step(const DemParams& P, const T* eta, const T* nu, const T
 }
 
 // ─── P_REDUCE ───────────────────────────────────────────────────────────────
+// A warp reduces one system's chunk partials in a fixed order (lane 0 gets them).
 template <typename T>
 __device__ void frame_totals(const KArgs<T>& a, int sys, double* tot3) {
-    // a CTA reduces one system's partials in a fixed order
+    const int lane = threadIdx.x & 31;
     double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-    for (int i = a.part_base[sys] + threadIdx.x; i < a.part_base[sys + 1]; i += blockDim.x) {
+    for (int i = a.part_base[sys] + lane; i < a.part_base[sys + 1]; i += 32) {
         v0 += a.part[3 * i];
         v1 += a.part[3 * i + 1];
         v2 += a.part[3 * i + 2];
     }
-    block_sum3<kThreads>(v0, v1, v2, tot3);
+    tot3[0] = warp_sum_lane0(v0);
+    tot3[1] = warp_sum_lane0(v1);
+    tot3[2] = warp_sum_lane0(v2);
 }
 
 template <typename T>
@@ -1178,18 +1194,14 @@ __device__ __forceinline__ T thrust_scale_of(const KArgs<T>& a, const double* to
 template <typename T>
 __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     typedef typename vec2_of<T>::type V2;
-    // one CTA per system: totals, thrust cap and the vessel step
-    for (int sys = blockIdx.x; sys < a.nsys; sys += gridDim.x) {
-        __shared__ double tot3[3];
-        double r[3];
-        frame_totals(a, sys, r);
-        if (threadIdx.x == 0) {
-            tot3[0] = r[0];
-            tot3[1] = r[1];
-            tot3[2] = r[2];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+    // one warp per system: totals, thrust cap and the vessel step (warp 0 of
+    // CTA 0 for a single system)
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ngwarp = (gridDim.x * blockDim.x) >> 5;
+    for (int sys = gwarp; sys < a.nsys; sys += ngwarp) {
+        double tot3[3];
+        frame_totals(a, sys, tot3);
+        if ((threadIdx.x & 31) == 0) {
             const T scale = thrust_scale_of(a, tot3);
             // reaction on the ship (jax_simulation.py:470-478)
             T Fx = -(T(tot3[0]) * scale), Fy = -(T(tot3[1]) * scale), M = T(tot3[2]);
@@ -1237,7 +1249,6 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
                 a.h_F[fs_i * 2 + 1] = Fy;
             }
         }
-        __syncthreads();  // tot3 is reused by this CTA's next system
     }
     // With one system, CTA 0 runs the vessel step above and the other CTAs share
     // the element and slot work (all CTAs when the grid has one); with several

@@ -73,7 +73,7 @@ def _host(x) -> np.ndarray:
 
 
 def build_params(cfg, ship_dyn, ship_length, ship_beam, n_ice_steps, dt, dt_ice, use_auto_icenav,
-                 B_mat, T_n, material: IceMaterial = DEFAULT_MATERIAL, skin: float = 0.3,
+                 B_mat, T_n, material: IceMaterial = DEFAULT_MATERIAL, skin: float = 0.8,
                  max_neighbors: int = 32, bucket_capacity: int = 32) -> _abi.DemParams:
     """Fill ``DemParams`` from a config the way the factory reads it (``jax_simulation.py:325-361``)."""
     P = _abi.DemParams()
@@ -125,7 +125,7 @@ class FrameStep:
     def __init__(self, static: IceStaticData, cfg, ship_dyn: ShipDynamicsData, ship_length: float,
                  ship_beam: float, n_ice_steps: int, dt: float, dt_ice: float,
                  use_auto_icenav: bool, B_mat, T_n: float, material: IceMaterial = DEFAULT_MATERIAL,
-                 skin: float = 0.3, max_neighbors: int = 32, bucket_capacity: int = 32,
+                 skin: float = 0.8, max_neighbors: int = 32, bucket_capacity: int = 32,
                  device=None, dtype=None, launch_mode: int = _abi.DEM_LAUNCH_PERSISTENT,
                  system_start=None):
         """``system_start`` (Q+1 element offsets) splits the field into Q independent
