@@ -564,6 +564,7 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_
     names = ["cull", "near", "cforce", "reduce"] + [f"{x}" for s in range(k)
                                                      for x in ("escape", "build_all", "force")] + ["fracture"]
     acc = collections.defaultdict(list)
+    per_sub = collections.defaultdict(list)
     fs.set_profiling(True)
     for _ in range(frames):
         if run is None:
@@ -575,6 +576,9 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_
         prev = 0
         for ph, t in pts:
             acc[names[ph % per]].append((t - prev) / 1e3)
+            p = ph % per
+            if 4 <= p < per - 1:
+                per_sub[(names[p], (p - 4) // 3)].append((t - prev) / 1e3)
             prev = t
     fs.set_profiling(False)
     tot = 0.0
@@ -585,6 +589,9 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_
         tot += s
         sys.stderr.write(f"phase {nm:9s} {s:9.1f} us/frame  ({len(v) / frames:.1f} runs/frame)\n")
     sys.stderr.write(f"phase total     {tot:9.1f} us/frame\n")
+    for nm in ("escape", "force"):
+        row = " ".join(f"{sum(per_sub[(nm, i)]) / max(len(per_sub[(nm, i)]), 1):6.1f}" for i in range(k))
+        sys.stderr.write(f"phase {nm:9s} by substep (us per run): {row}\n")
 
 
 # ── CPU side (the oracle is the checker/baseline only) ─────────────────────────
