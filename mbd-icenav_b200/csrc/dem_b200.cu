@@ -61,6 +61,7 @@ struct DemHandle {
     int* dirty_cnt = nullptr;
     int* work_cnt = nullptr;
     int* act_list = nullptr;
+    unsigned* bstamp = nullptr;  // (nb) frame stamps of bonds with an active end
     int* act_cnt = nullptr;
     int* slot_owner = nullptr;
     unsigned* esc_cnt = nullptr;
@@ -209,6 +210,7 @@ int reset_broad_phase(DemHandle* h, cudaStream_t st) {
     CUDA_TRY(h, cudaMemsetAsync(h->comp_cnt, 0, sizeof(int), st));
     CUDA_TRY(h, cudaMemsetAsync(h->pos_ref, 0xFF, h->esz * 2 * (size_t)h->n, st));
     CUDA_TRY(h, cudaMemsetAsync(h->dirty, 0, sizeof(unsigned) * (size_t)h->n, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->bstamp, 0, sizeof(unsigned) * (size_t)std::max(h->nb, 1), st));
     CUDA_TRY(h, cudaMemsetAsync(h->bflag, 0, sizeof(int) * (size_t)h->n_buckets, st));
     CUDA_TRY(h, cudaMemsetAsync(h->ncnt, 0, sizeof(int) * (size_t)h->n, st));
     return DEM_OK;
@@ -354,6 +356,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.dirty_cnt = h->dirty_cnt;
     a.work_cnt = h->work_cnt;
     a.act_list = h->act_list;
+    a.bstamp = h->bstamp;
     a.act_cnt = h->act_cnt;
     a.slot_owner = h->slot_owner;
     a.esc_cnt = h->esc_cnt;
@@ -453,6 +456,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
         const unsigned need = (unsigned)K * (unsigned)h->P.n_ice_steps + 1u;
         if (h->round_base > 0xFFFFFFFFu - need) {
             CUDA_TRY(h, cudaMemsetAsync(h->dirty, 0, sizeof(unsigned) * (size_t)h->n, stream));
+            CUDA_TRY(h, cudaMemsetAsync(h->bstamp, 0, sizeof(unsigned) * (size_t)std::max(h->nb, 1), stream));
             h->round_base = 0;
         }
         a.round_base = h->round_base;
@@ -663,6 +667,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->dirty_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->work_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->bstamp, sizeof(unsigned) * std::max(nb, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->esc_cnt, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);

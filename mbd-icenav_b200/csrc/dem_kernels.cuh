@@ -49,9 +49,6 @@ __host__ __device__ constexpr int phases_per_frame(int k_sub) { return 5 + 3 * k
 #ifndef DEM_SLOT_BATCH
 #define DEM_SLOT_BATCH 1
 #endif
-#ifndef DEM_FRACTURE_BATCH
-#define DEM_FRACTURE_BATCH 1
-#endif
 #ifndef DEM_MIN_BLOCKS
 #define DEM_MIN_BLOCKS 2  // resident CTAs per SM the register allocation targets
 #endif
@@ -153,6 +150,7 @@ struct KArgs {
     int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
     int* work_cnt;      // (k_sub + 2) element chunks handed out dynamically, per substep
     int* act_list;      // (n) elements active this frame (built by phase_reduce)
+    unsigned* bstamp;   // (nb) frame stamp of the bonds with an active end (set by phase_reduce)
     int* act_cnt;       // (1) entries of act_list
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
     int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
@@ -214,6 +212,13 @@ __device__ __forceinline__ Frame<T> make_frame(const KArgs<T>& a, int f) {
     F.sp = a.setpoints ? a.setpoints + (size_t)f * a.nsys * 6 : nullptr;
     F.vws = a.vws ? a.vws + (size_t)f * a.nsys * 2 : nullptr;
     return F;
+}
+
+// Stamp of frame f of this call: the dirty stamp of its first rebuild round,
+// unique since the stamps were last cleared (never 0)
+template <typename T>
+__device__ __forceinline__ unsigned frame_stamp(const KArgs<T>& a, const Frame<T>& F) {
+    return a.round_base + (unsigned)(F.f * a.k_sub) + 1u;
 }
 
 // ─── grid barrier (bounded) ──────────────────────────────────────────────────
@@ -1259,6 +1264,7 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     const int gsz = (gridDim.x - c0) * blockDim.x;
     SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
     typedef typename vec4_of<T>::type V4;
+    const unsigned fstamp = frame_stamp(a, F);
     for (int e = gtid; e < a.n; e += gsz) {
         // activation (jax_simulation.py:498-509)
         const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
@@ -1295,6 +1301,8 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             const int2 ent0 = a.bslot[sl];
             const int2 ent1 = two ? a.bslot[sl + 1] : ent0;
             const int b0 = ent0.x & 0x7fffffff, b1 = ent1.x & 0x7fffffff;
+            a.bstamp[b0] = fstamp;  // the bond has an active end this frame
+            a.bstamp[b1] = fstamp;
             const bool in0 = F.src.intact[b0] != 0, in1 = F.src.intact[b1] != 0;
             const bool sa0 = F.src.active[ent0.y] != 0, sa1 = F.src.active[ent1.y] != 0;
             const int fo0 = a.floe_of[ent0.y], fo1 = a.floe_of[ent1.y];
@@ -1810,129 +1818,156 @@ __device__ __forceinline__ T sys_scale(const KArgs<T>& a, T scale1, int sys) {
     return a.nsys == 1 ? scale1 : T(*((volatile double*)&a.fscal[4 * sys]));
 }
 
+// The full fracture update of bond b (jax_simulation.py:534-653), for a bond
+// with an active end.
 template <typename T>
-__device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
+__device__ __forceinline__ void fracture_bond(const KArgs<T>& a, const Frame<T>& F, T scale, int b) {
+    typedef typename vec2_of<T>::type V2;
     const DemParams& P = a.P;
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gsz = gridDim.x * blockDim.x;
     const T mft = T(P.max_fracture_thickness);
     const T esc = T(P.effective_strength_collision);
     const T dti = T(P.dt_ice);
     const T kn = a.k_n, ks = a.k_s;
-    // two bonds per thread and step: every load of both (bond -> endpoints ->
-    // floe flags) is issued before any store
-    typedef typename vec2_of<T>::type V2;
-    constexpr int kB = DEM_FRACTURE_BATCH;
-    for (int base = gtid; base < a.nb; base += kB * gsz) {
-        int bb[kB], ii[kB], jj[kB];
-        bool ok[kB];
-#pragma unroll
-        for (int k = 0; k < kB; ++k) {
-            bb[k] = base + k * gsz;
-            ok[k] = bb[k] < a.nb;
-            ii[k] = ok[k] ? a.bi[bb[k]] : 0;
-            jj[k] = ok[k] ? a.bj[bb[k]] : 0;
-        }
-        // A bond between two frozen elements keeps its state: neither end touches
-        // the ship (a touched element's floe is active this frame), so both contact
-        // forces are 0, no DPDEM gate opens and no collision breaks it
-        bool frz[kB];
-#pragma unroll
-        for (int k = 0; k < kB; ++k) frz[k] = ok[k] && !F.dst.active[ii[k]] && !F.dst.active[jj[k]];
-        V2 pi[kB], pj[kB], vi[kB], vj[kB];
-        bool both_act[kB], breakable[kB], at_crack[kB], intact[kB];
-        int fli[kB], flj[kB];
-        T fmi[kB], fmj[kB], ds0[kB], rest[kB], cur_d[kB], dmmax0[kB], dm00[kB], sbar[kB], bstr[kB];
-#pragma unroll
-        for (int k = 0; k < kB; ++k) {
-            if (!ok[k]) continue;
-            const int i = ii[k], j = jj[k], b = bb[k];
-            ds0[k] = F.src.ds[b];
-            cur_d[k] = F.src.dmg[b];
-            intact[k] = F.src.intact[b] != 0;
-            dmmax0[k] = F.src.dmmax[b];
-            dm00[k] = F.src.dm0[b];
-            if (frz[k]) continue;
-            pi[k] = ld2(F.dst.pos, i);
-            pj[k] = ld2(F.dst.pos, j);
-            vi[k] = ld2(F.dst.vel, i);
-            vj[k] = ld2(F.dst.vel, j);
-            both_act[k] = F.dst.active[i] && F.dst.active[j];
-            fli[k] = a.floe_of[i];
-            flj[k] = a.floe_of[j];
-            breakable[k] = (a.thick[i] <= mft) && (a.thick[j] <= mft);
-            const T sc = sys_scale(a, scale, a.nsys > 1 ? a.sys_of[i] : 0);  // i and j share a system
-            fmi[k] = a.fraw[i] * sc;
-            fmj[k] = a.fraw[j] * sc;
-            at_crack[k] = a.crack[i] || a.crack[j];
-            rest[k] = a.rest[b];
-            sbar[k] = a.sbar[b];
-            bstr[k] = a.bstr[b];
-        }
-        bool floe_ok[kB];
-#pragma unroll
-        for (int k = 0; k < kB; ++k) {
-            if (!ok[k] || frz[k]) continue;
-            const T sc = sys_scale(a, scale, a.nsys > 1 ? a.floe_sys[fli[k]] : 0);
-            const bool ei = new_elig(a, F, fli[k], sc);
-            const bool ej = new_elig(a, F, flj[k], sc);
-            floe_ok[k] = ei && ej;
-        }
-#pragma unroll
-        for (int k = 0; k < kB; ++k) {
-            if (!ok[k]) continue;
-            const int b = bb[k];
-            if (frz[k]) {  // the full path's result for such a bond, without its loads
-                F.dst.dmg[b] = cur_d[k];
-                F.dst.dmmax[b] = dmmax0[k];
-                F.dst.dm0[b] = dm00[k];
-                F.dst.ds[b] = ds0[k] + T(0);
-                F.dst.intact[b] = intact[k] ? 1 : 0;
-                if (a.h_intact) a.h_intact[(size_t)F.f * a.nb + b] = intact[k] ? 1 : 0;
-                continue;
+    const int i = a.bi[b], j = a.bj[b];
+    const T ds0 = F.src.ds[b], cur_d = F.src.dmg[b], dmmax0 = F.src.dmmax[b], dm00 = F.src.dm0[b];
+    const bool intact = F.src.intact[b] != 0;
+    const T rest = a.rest[b], sbar = a.sbar[b], bstr = a.bstr[b];
+    const V2 pi = ld2(F.dst.pos, i), pj = ld2(F.dst.pos, j);
+    const V2 vi = ld2(F.dst.vel, i), vj = ld2(F.dst.vel, j);
+    const bool both_act = F.dst.active[i] && F.dst.active[j];
+    const int fli = a.floe_of[i], flj = a.floe_of[j];
+    const bool breakable = (a.thick[i] <= mft) && (a.thick[j] <= mft);
+    const T sc = sys_scale(a, scale, a.nsys > 1 ? a.sys_of[i] : 0);  // i and j share a system
+    const T fmi = a.fraw[i] * sc, fmj = a.fraw[j] * sc;
+    const bool at_crack = a.crack[i] || a.crack[j];
+    const T scf = sys_scale(a, scale, a.nsys > 1 ? a.floe_sys[fli] : 0);
+    const bool floe_ok = new_elig(a, F, fli, scf) && new_elig(a, F, flj, scf);
+    T dx = pj.x - pi.x, dy = pj.y - pi.y;
+    T dist = jsqrt(dx * dx + dy * dy);
+    T dsafe = jmax(dist, T(1e-10));
+    T bx = dx / dsafe, by = dy / dsafe;
+    bool near = (fmi > T(0)) || (fmj > T(0));
+    bool dpdem_ok = both_act && floe_ok && (near || at_crack) && breakable;
+    T vrx = vj.x - vi.x, vry = vj.y - vi.y;
+    T vn = vrx * bx + vry * by;
+    T vtx = vrx - vn * bx, vty = vry - vn * by;
+    T ds_incr = jsqrt(vtx * vtx + vty * vty) * dti;
+    bool ds_gate = near && both_act && floe_ok && breakable;
+    T new_ds = ds0 + (ds_gate ? ds_incr : T(0));
+    T L0 = jmax(rest, T(1e-10));
+    T delta_n = dist - rest;
+    T dn_d = near ? delta_n : T(0);
+    T sn = (kn * (dn_d / L0)) * (T(1) - cur_d);
+    T st = (ks * (new_ds / L0)) * (T(1) - cur_d);
+    T od = cur_d, omax = dmmax0, o0 = dm00;
+    bool fin = intact;
+    if (dpdem_ok) {
+        // the damage law's result is only selected for DPDEM-eligible bonds
+        // (jnp.where at jax_simulation.py:620-623); elsewhere the old state stays
+        T nd, nmax, n0;
+        bool nint;
+        bond_damage<T>(P, delta_n, new_ds, sn, st, sbar, cur_d, omax, o0, intact, nd, nmax, n0, nint);
+        od = nd;
+        omax = nmax;
+        o0 = n0;
+        if (breakable) fin = nint;
+    }
+    // direct collision breaking (jax_simulation.py:629-637)
+    bool coll_on = (fmi > T(0)) || (fmj > T(0));
+    T coll_f = jmax(fmi, fmj);
+    bool brk = intact && coll_on && (coll_f > bstr * esc) && breakable;
+    fin = fin && !brk;
+    F.dst.dmg[b] = od;
+    F.dst.dmmax[b] = omax;
+    F.dst.dm0[b] = o0;
+    F.dst.ds[b] = new_ds;
+    F.dst.intact[b] = fin ? 1 : 0;
+    if (a.h_intact) a.h_intact[(size_t)F.f * a.nb + b] = fin ? 1 : 0;
+}
+
+template <typename T>
+__device__ __forceinline__ void copy4(const T* __restrict__ s, T* __restrict__ d, bool plus_zero);
+template <>
+__device__ __forceinline__ void copy4<float>(const float* __restrict__ s, float* __restrict__ d, bool plus_zero) {
+    float4 v = *reinterpret_cast<const float4*>(s);
+    if (plus_zero) {
+        v.x = v.x + 0.0f;
+        v.y = v.y + 0.0f;
+        v.z = v.z + 0.0f;
+        v.w = v.w + 0.0f;
+    }
+    *reinterpret_cast<float4*>(d) = v;
+}
+template <>
+__device__ __forceinline__ void copy4<double>(const double* __restrict__ s, double* __restrict__ d, bool plus_zero) {
+    double2 v = reinterpret_cast<const double2*>(s)[0], w = reinterpret_cast<const double2*>(s)[1];
+    if (plus_zero) {
+        v.x = v.x + 0.0;
+        v.y = v.y + 0.0;
+        w.x = w.x + 0.0;
+        w.y = w.y + 0.0;
+    }
+    reinterpret_cast<double2*>(d)[0] = v;
+    reinterpret_cast<double2*>(d)[1] = w;
+}
+
+template <typename T>
+__device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsz = gridDim.x * blockDim.x;
+    const unsigned fstamp = frame_stamp(a, F);
+    // Bonds in groups of four per thread.  A bond between two frozen elements
+    // keeps its state: neither end touches the ship (a touched element's floe is
+    // active this frame), so both contact forces are 0, no DPDEM gate opens and
+    // no collision breaks it; the update is then the copy of its state (shear
+    // displacement + 0, intact as 0/1).  Every bond of the group is copied first
+    // (16-byte accesses when all state arrays are aligned); then the bonds with an
+    // active end, which carry this frame's stamp (phase_reduce), take the full
+    // update and overwrite their copy.
+    auto al16 = [](const void* p) { return ((size_t)p & 15u) == 0; };
+    const bool vec = al16(F.src.ds) && al16(F.dst.ds) && al16(F.src.dmg) && al16(F.dst.dmg) && al16(F.src.dm0) &&
+                     al16(F.dst.dm0) && al16(F.src.dmmax) && al16(F.dst.dmmax) && al16(a.bstamp) &&
+                     ((size_t)F.src.intact & 3u) == 0 && ((size_t)F.dst.intact & 3u) == 0;
+    const int ng = (a.nb + 3) >> 2;
+    for (int g = gtid; g < ng; g += gsz) {
+        const int b0 = 4 * g;
+        const int cnt = min(4, a.nb - b0);
+        unsigned st[4] = {0u, 0u, 0u, 0u};
+        unsigned in4 = 0u;
+        if (vec && cnt == 4) {
+            const uint4 s4 = *reinterpret_cast<const uint4*>(a.bstamp + b0);
+            st[0] = s4.x;
+            st[1] = s4.y;
+            st[2] = s4.z;
+            st[3] = s4.w;
+            copy4<T>(F.src.ds + b0, F.dst.ds + b0, true);
+            copy4<T>(F.src.dmg + b0, F.dst.dmg + b0, false);
+            copy4<T>(F.src.dm0 + b0, F.dst.dm0 + b0, false);
+            copy4<T>(F.src.dmmax + b0, F.dst.dmmax + b0, false);
+            const unsigned raw = *reinterpret_cast<const unsigned*>(F.src.intact + b0);
+            for (int k = 0; k < 4; ++k)
+                if ((raw >> (8 * k)) & 0xffu) in4 |= 1u << (8 * k);
+            *reinterpret_cast<unsigned*>(F.dst.intact + b0) = in4;
+        } else {
+            for (int k = 0; k < cnt; ++k) {
+                const int b = b0 + k;
+                st[k] = a.bstamp[b];
+                F.dst.ds[b] = F.src.ds[b] + T(0);
+                F.dst.dmg[b] = F.src.dmg[b];
+                F.dst.dm0[b] = F.src.dm0[b];
+                F.dst.dmmax[b] = F.src.dmmax[b];
+                const unsigned v = F.src.intact[b] != 0 ? 1u : 0u;
+                F.dst.intact[b] = (uint8_t)v;
+                in4 |= v << (8 * k);
             }
-            T dx = pj[k].x - pi[k].x, dy = pj[k].y - pi[k].y;
-            T dist = jsqrt(dx * dx + dy * dy);
-            T dsafe = jmax(dist, T(1e-10));
-            T bx = dx / dsafe, by = dy / dsafe;
-            bool near = (fmi[k] > T(0)) || (fmj[k] > T(0));
-            bool dpdem_ok = both_act[k] && floe_ok[k] && (near || at_crack[k]) && breakable[k];
-            T vrx = vj[k].x - vi[k].x, vry = vj[k].y - vi[k].y;
-            T vn = vrx * bx + vry * by;
-            T vtx = vrx - vn * bx, vty = vry - vn * by;
-            T ds_incr = jsqrt(vtx * vtx + vty * vty) * dti;
-            bool ds_gate = near && both_act[k] && floe_ok[k] && breakable[k];
-            T new_ds = ds0[k] + (ds_gate ? ds_incr : T(0));
-            T L0 = jmax(rest[k], T(1e-10));
-            T delta_n = dist - rest[k];
-            T dn_d = near ? delta_n : T(0);
-            T sn = (kn * (dn_d / L0)) * (T(1) - cur_d[k]);
-            T st = (ks * (new_ds / L0)) * (T(1) - cur_d[k]);
-            T od = cur_d[k], omax = dmmax0[k], o0 = dm00[k];
-            bool fin = intact[k];
-            if (dpdem_ok) {
-                // the damage law's result is only selected for DPDEM-eligible bonds
-                // (jnp.where at jax_simulation.py:620-623); elsewhere the old state stays
-                T nd, nmax, n0;
-                bool nint;
-                bond_damage<T>(P, delta_n, new_ds, sn, st, sbar[k], cur_d[k], omax, o0, intact[k], nd, nmax, n0,
-                               nint);
-                od = nd;
-                omax = nmax;
-                o0 = n0;
-                if (breakable[k]) fin = nint;
+        }
+        for (int k = 0; k < cnt; ++k) {
+            const int b = b0 + k;
+            if (st[k] == fstamp) {
+                fracture_bond(a, F, scale, b);
+            } else if (a.h_intact) {
+                a.h_intact[(size_t)F.f * a.nb + b] = (uint8_t)((in4 >> (8 * k)) & 1u);
             }
-            // direct collision breaking (jax_simulation.py:629-637)
-            bool coll_on = (fmi[k] > T(0)) || (fmj[k] > T(0));
-            T coll_f = jmax(fmi[k], fmj[k]);
-            bool brk = intact[k] && coll_on && (coll_f > bstr[k] * esc) && breakable[k];
-            fin = fin && !brk;
-            F.dst.dmg[b] = od;
-            F.dst.dmmax[b] = omax;
-            F.dst.dm0[b] = o0;
-            F.dst.ds[b] = new_ds;
-            F.dst.intact[b] = fin ? 1 : 0;
-            if (a.h_intact) a.h_intact[(size_t)F.f * a.nb + b] = fin ? 1 : 0;
         }
     }
     for (int e = gtid; e < a.n; e += gsz) {
