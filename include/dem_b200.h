@@ -233,6 +233,18 @@ int dem_set_capacity(DemHandle* h, int32_t max_neighbors, int32_t bucket_capacit
 /* DEM_LAUNCH_PERSISTENT (default) or DEM_LAUNCH_PHASED; both give identical results. */
 int dem_set_launch_mode(DemHandle* h, int32_t mode);
 
+/* How the work of a substep is split (no reference counterpart; results are
+ * identical for every choice, this is for tests and tuning).  force_split:
+ * DEM_SPLIT_AUTO (a warp per active element when at most two fall to each warp,
+ * else a thread per element), DEM_SPLIT_THREAD or DEM_SPLIT_WARP.  mark_split,
+ * for the escape rounds: DEM_SPLIT_AUTO (a CTA per escaped element when they fit
+ * one per CTA, else a warp each), DEM_SPLIT_CTA or DEM_SPLIT_WARP. */
+#define DEM_SPLIT_AUTO 0
+#define DEM_SPLIT_THREAD 1
+#define DEM_SPLIT_CTA 1
+#define DEM_SPLIT_WARP 2
+int dem_set_work_split(DemHandle* h, int32_t force_split, int32_t mark_split);
+
 int dem_get_info(DemHandle* h, DemInfo* info);
 
 /* Record, in persistent launches, the device time at which each phase ends

@@ -21,6 +21,7 @@ DEM_F32 = 0
 DEM_F64 = 1
 DEM_LAUNCH_PERSISTENT = 0
 DEM_LAUNCH_PHASED = 1
+DEM_SPLIT_AUTO, DEM_SPLIT_THREAD, DEM_SPLIT_CTA, DEM_SPLIT_WARP = 0, 1, 1, 2
 
 _ERR_NAMES = {0: "DEM_OK", 1: "DEM_ERR_INVALID", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_CAPACITY",
               4: "DEM_ERR_TIMEOUT", 5: "DEM_ERR_ALIAS"}
@@ -115,7 +116,7 @@ class DemRolloutCostParams(C.Structure):
 
 
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
-           "dem_set_capacity", "dem_set_launch_mode", "dem_get_info", "dem_set_profiling",
+           "dem_set_capacity", "dem_set_launch_mode", "dem_set_work_split", "dem_get_info", "dem_set_profiling",
            "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap", "dem_rollout_segment",
            "dem_rollout_costs")
 
@@ -149,6 +150,7 @@ def load_library(path: str = None):
     lib.dem_sync_status.argtypes = [H, _vp]
     lib.dem_set_capacity.argtypes = [H, _i, _i]
     lib.dem_set_launch_mode.argtypes = [H, _i]
+    lib.dem_set_work_split.argtypes = [H, _i, _i]
     lib.dem_get_info.argtypes = [H, C.POINTER(DemInfo)]
     lib.dem_set_profiling.argtypes = [H, _i]
     lib.dem_get_phase_times.argtypes = [H, C.POINTER(C.c_int64), _i, C.POINTER(_i), C.POINTER(C.c_int64)]

@@ -26,6 +26,7 @@ struct DemHandle {
     int dtype = DEM_F32;
     int device = 0;
     int mode = DEM_LAUNCH_PERSISTENT;
+    int force_split = DEM_SPLIT_AUTO, mark_split = DEM_SPLIT_AUTO;
     DemParams P{};
     DemStatic S{};
     size_t esz = 4;
@@ -298,6 +299,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.bucket_cap = h->P.bucket_capacity;
     a.max_nb = h->P.max_neighbors;
     a.mode = h->mode;
+    a.force_split = h->force_split;
+    a.mark_split = h->mark_split;
     a.k_n = (T)h->k_n;
     a.k_s = (T)h->k_s;
     a.min_bstr = (T)h->min_bstr;
@@ -913,6 +916,16 @@ int dem_set_launch_mode(DemHandle* h, int32_t mode) {
     if (!h) return DEM_ERR_INVALID;
     if (mode != DEM_LAUNCH_PERSISTENT && mode != DEM_LAUNCH_PHASED) return set_err(h, DEM_ERR_INVALID, "bad launch mode");
     h->mode = mode;
+    return DEM_OK;
+}
+
+int dem_set_work_split(DemHandle* h, int32_t force_split, int32_t mark_split) {
+    if (!h) return DEM_ERR_INVALID;
+    if (force_split < DEM_SPLIT_AUTO || force_split > DEM_SPLIT_WARP || mark_split < DEM_SPLIT_AUTO ||
+        mark_split > DEM_SPLIT_WARP)
+        return set_err(h, DEM_ERR_INVALID, "bad work split");
+    h->force_split = force_split;
+    h->mark_split = mark_split;
     return DEM_OK;
 }
 

@@ -103,6 +103,7 @@ struct KArgs {
     const int* part_base;     // (nsys + 1) first chunk of each system
     const T* u_ctrl;          // (K, nsys, 3) body-frame ship controls of planner rollouts, or NULL
     int n_buckets, bucket_cap, max_nb, mode;
+    int force_split, mark_split;  // DEM_SPLIT_*: how substep work is split (tests and tuning)
     T k_n, k_s, min_bstr, cell, skin, hull_r;
     // escape thresholds: a substep whose successor is a check substep (s + 1 a
     // multiple of esc_period) tests against esc_h_check, every other one
@@ -590,7 +591,7 @@ __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int 
             const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
             rereference(a, e, px, py, c);
         }
-    } else if (n_esc <= (int)gridDim.x) {
+    } else if (a.mark_split == DEM_SPLIT_CTA || (a.mark_split == DEM_SPLIT_AUTO && n_esc <= (int)gridDim.x)) {
         // few escapes: a CTA per element, its stencil entries in one load round
         for (int q = blockIdx.x; q < n_esc; q += gridDim.x) {
             const int e = a.esc_list[q];
@@ -1718,7 +1719,7 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     // the current chunk is computed), so uneven chunks do not leave warps idle.
     const int na = *((volatile int*)a.act_cnt);
     const int nw2 = nwarps - skip;
-    if (na <= 2 * nw2) {
+    if (a.force_split == DEM_SPLIT_WARP || (a.force_split == DEM_SPLIT_AUTO && na <= 2 * nw2)) {
         // at most two active elements per warp: a warp per element
         for (int i = warp - skip; i < na; i += nw2) {
             const int e = a.act_list[i];

@@ -218,6 +218,10 @@ class FrameStep:
     def set_launch_mode(self, mode: int):
         self._check(self.lib.dem_set_launch_mode(self._h, int(mode)))
 
+    def set_work_split(self, force_split: int = 0, mark_split: int = 0):
+        """How substep work is split (``dem_set_work_split``; results are identical)."""
+        self._check(self.lib.dem_set_work_split(self._h, int(force_split), int(mark_split)))
+
     def info(self) -> dict:
         inf = _abi.DemInfo()
         self._check(self.lib.dem_get_info(self._h, C.byref(inf)))

@@ -105,3 +105,71 @@ def test_results_do_not_depend_on_the_skin_or_the_escape_period(golden64):
             assert torch.equal(a, b), skin
         assert rounds < rounds_03, skin  # fewer rebuild rounds
     assert rounds_03 > 0
+
+
+def _split_runs(fs, st0, sh0, inputs):
+    from mbd_icenav_b200 import _abi
+    out = []
+    for force_split, mark_split in ((_abi.DEM_SPLIT_AUTO, _abi.DEM_SPLIT_AUTO),
+                                    (_abi.DEM_SPLIT_THREAD, _abi.DEM_SPLIT_WARP),
+                                    (_abi.DEM_SPLIT_WARP, _abi.DEM_SPLIT_CTA)):
+        fs.set_work_split(force_split, mark_split)
+        out.append(fs.scan_segment(st0, sh0, *inputs))
+    fs.set_work_split()
+    return out
+
+
+def _assert_same(runs):
+    (st_a, sh_a, h_a) = runs[0]
+    for st, sh, h in runs[1:]:
+        for a, b in zip(st_a, st):
+            assert torch.equal(a, b)
+        for a, b in zip(sh_a, sh):
+            assert torch.equal(a, b)
+        for a, b in zip(h_a, h):
+            assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_work_splits_give_identical_results_golden_field(golden64, dtype):
+    """A thread or a warp per active element, a CTA or a warp per escaped element:
+    the same trajectories bit for bit (the small scenario, through first contact)."""
+    g = golden64
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    fs = gpu_frame_step(g, "small", dt)
+    o_st, o_sh = initial_state(g, "small", np.float64)
+    st0, sh0 = to_gpu_state(o_st, o_sh, dt)
+    runs = _split_runs(fs, st0, sh0, _scan_inputs(g, "small", 0, 100, dt))
+    _assert_same(runs)
+    assert runs[0][0].elem_active.any()  # the ship met the ice
+    fs.close()
+
+
+def test_work_splits_give_identical_results_ship_in_the_medium_field():
+    """The same on the 12k-element medium field with the ship pushing into the ice
+    edge for 40 frames (the forced splits run both paths on its active floes)."""
+    from mbd_icenav_b200 import rollouts, scene
+    from mbd_icenav_b200.sim import build_sim_context
+    from mbd_icenav_b200.state import build_initial_ice_state, build_initial_ship_state
+    f = scene.make_medium_field(seed=2, n_frames=40)
+    K = 40
+    eta0 = rollouts.ice_edge_pose(f, gap=0.5)
+    d = np.array([np.cos(eta0[2]), np.sin(eta0[2])])
+    path = np.array([[eta0[0] + 2.0 * 0.05 * i * d[0], eta0[1] + 2.0 * 0.05 * i * d[1], eta0[2]]
+                     for i in range(K + 2)])
+    ctx = build_sim_context(f.polygons, f.centroids, f.bonds, eta0[:2], f.ship_length, f.ship_beam, K, f.dt,
+                            (0.0, 0.0), f.thicknesses, f.ship_props, parent_ids=f.parent_ids, verbose=False,
+                            n_ice_steps=f.n_ice_steps, hull_local=f.hull_local, dilation=0.05,
+                            dtype=torch.float32, device="cuda")
+    fs = ctx.frame_step
+    st0 = build_initial_ice_state(f.n, f.centroids, len(f.bonds), ctx.static.initial_floe_of.cpu().numpy(),
+                                  dtype=torch.float32, device="cuda")
+    sh0 = build_initial_ship_state(eta0[:2], float(eta0[2]), dtype=torch.float32, device="cuda")
+    dev = torch.device("cuda", 0)
+    rows = torch.as_tensor(np.concatenate([path[:K], path[1:K + 1]], 1), dtype=torch.float32, device=dev)
+    vw = torch.zeros((K, f.n, 2), dtype=torch.float32, device=dev)
+    runs = _split_runs(fs, st0, sh0, (rows, vw))
+    _assert_same(runs)
+    assert int(runs[0][0].elem_active.sum()) > 0  # the ship met the ice
+    assert fs.info()["escaped_total"] > 0
+    fs.close()
