@@ -62,6 +62,8 @@ struct DemHandle {
     int* dirty_cnt = nullptr;
     int* work_cnt = nullptr;
     int* act_list = nullptr;
+    int* lazy_list = nullptr;
+    int* lazy_cnt = nullptr;
     unsigned* bstamp = nullptr;  // (nb) frame stamps of bonds with an active end
     int* act_cnt = nullptr;
     int* slot_owner = nullptr;
@@ -315,6 +317,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
         const double h_two = 0.99 * (0.5 * S - dmax);
         const bool two = std::isfinite(dmax) && h_two >= 0.25 * S;
         a.esc_period = two ? 2 : 1;
+        // lazy escapes replace the every-second-substep processing
+        a.lazy = (two && h->P.n_ice_steps >= 2) ? 1 : 0;
         a.esc_h_check = (T)(two ? std::min(h_two, h_urgent) : h_urgent);
         a.esc_h_urgent = (T)h_urgent;
     }
@@ -359,6 +363,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.dirty_cnt = h->dirty_cnt;
     a.work_cnt = h->work_cnt;
     a.act_list = h->act_list;
+    a.lazy_list = h->lazy_list;
+    a.lazy_cnt = h->lazy_cnt;
     a.bstamp = h->bstamp;
     a.act_cnt = h->act_cnt;
     a.slot_owner = h->slot_owner;
@@ -453,6 +459,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     CUDA_TRY(h, cudaMemsetAsync(h->esc_cnt, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->dirty_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
     CUDA_TRY(h, cudaMemsetAsync(h->work_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->lazy_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
     {
         // every rebuild round of every call gets its own dirty stamp; clear the
         // stamps before the counter would wrap
@@ -670,6 +677,8 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->dirty_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->work_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->lazy_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->lazy_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bstamp, sizeof(unsigned) * std::max(nb, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);

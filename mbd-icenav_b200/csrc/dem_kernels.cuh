@@ -110,6 +110,13 @@ struct KArgs {
     // against esc_h_urgent (the limit of an element's next use)
     T esc_h_check, esc_h_urgent;
     int esc_period;
+    // lazy escapes (with esc_period 2): before an even substep s (s + 1 < k_sub)
+    // an element beyond esc_h_check but within esc_h_urgent goes to lazy_list[s];
+    // the force phase of s re-references it and marks its neighbourhood for a
+    // rebuild at s + 1, beside the force work, instead of an escape phase
+    int lazy;
+    int* lazy_list;     // (n) lazily escaped elements of the current detection
+    int* lazy_cnt;      // (k_sub + 2) per substep
     T t_samp[kMaxEdgeSamples];
     // static data (caller-owned)
     const T* polys;
@@ -292,8 +299,7 @@ __device__ __forceinline__ int sys_id(const KArgs<T>& a, int e) {
 // at once.  P = 1 (the default skin) tests every substep at 0.4455 skin.
 
 template <typename T>
-__device__ __forceinline__ bool escaped(const KArgs<T>& a, int e, T px, T py, T h) {
-    const T rx = a.pos_ref[2 * e], ry = a.pos_ref[2 * e + 1];
+__device__ __forceinline__ bool escaped_from(T px, T py, T rx, T ry, T h) {
     const bool fp = jfinite(px) && jfinite(py);
     const bool fr = jfinite(rx) && jfinite(ry);
     if (fp != fr) return true;
@@ -302,6 +308,10 @@ __device__ __forceinline__ bool escaped(const KArgs<T>& a, int e, T px, T py, T 
     // an element escape early, never late
     const T dx = px - rx, dy = py - ry;
     return dx * dx + dy * dy > h * h;
+}
+template <typename T>
+__device__ __forceinline__ bool escaped(const KArgs<T>& a, int e, T px, T py, T h) {
+    return escaped_from(px, py, a.pos_ref[2 * e], a.pos_ref[2 * e + 1], h);
 }
 
 // one atomic per CTA: add the CTA's count of `v` to *ctr (all threads must call)
@@ -580,13 +590,16 @@ __device__ __forceinline__ bool list_holds(const KArgs<T>& a, int o, int e, doub
 // elements' re-referencing; those elements rebuild their own lists anyway.
 // When most elements escaped, every list is rebuilt instead (no marking).
 template <typename T>
-__device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int s, unsigned round, bool all) {
-    const int n_esc = (int)cnt;
+__device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int n_lazy, int s, unsigned round,
+                             bool all) {
+    // items: the escaped elements, then (lazy mode) this substep's lazily escaped ones
+    const int n_esc = (int)cnt + (all ? 0 : n_lazy);
+    auto item = [&](int q) { return q < (int)cnt ? a.esc_list[q] : a.lazy_list[q - (int)cnt]; };
     if (all) {
         const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
         const int gsz = gridDim.x * blockDim.x;
         for (int q = gtid; q < n_esc; q += gsz) {
-            const int e = a.esc_list[q];
+            const int e = item(q);
             const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
             const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
             rereference(a, e, px, py, c);
@@ -594,7 +607,7 @@ __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int 
     } else if (a.mark_split == DEM_SPLIT_CTA || (a.mark_split == DEM_SPLIT_AUTO && n_esc <= (int)gridDim.x)) {
         // few escapes: a CTA per element, its stencil entries in one load round
         for (int q = blockIdx.x; q < n_esc; q += gridDim.x) {
-            const int e = a.esc_list[q];
+            const int e = item(q);
             const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
             const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
             const double rx = (double)a.pos_ref[2 * e], ry = (double)a.pos_ref[2 * e + 1];
@@ -613,7 +626,7 @@ __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int 
         const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
         const int nwarps = (gridDim.x * blockDim.x) >> 5;
         for (int q = warp; q < n_esc; q += nwarps) {
-            const int e = a.esc_list[q];
+            const int e = item(q);
             const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
             const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
             const double rx = (double)a.pos_ref[2 * e], ry = (double)a.pos_ref[2 * e + 1];
@@ -630,7 +643,31 @@ __device__ void phase_escape(const KArgs<T>& a, const T* kin, unsigned cnt, int 
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd((unsigned long long*)&a.stats[0], 1ull);
-        atomicAdd((unsigned long long*)&a.stats[3], (unsigned long long)cnt);
+        atomicAdd((unsigned long long*)&a.stats[3], (unsigned long long)n_esc);
+    }
+}
+
+// Lazy escape of element e during the force phase of substep s (warp-wide):
+// the neighbours its move brings into reach, and e itself, are stamped dirty for
+// the rebuild at substep s + 1; then e takes its position at substep s as new
+// reference.  Nothing else in the force phase reads references, buckets or
+// dirty stamps; e's own force this substep uses its current list, which is
+// valid (e is within the urgent limit of its old reference).
+template <typename T>
+__device__ __forceinline__ void lazy_escape_warp(const KArgs<T>& a, const T* kin, int e, int s_next,
+                                                 unsigned round_next) {
+    const int lane = threadIdx.x & 31;
+    const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+    const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+    const double rx = (double)a.pos_ref[2 * e], ry = (double)a.pos_ref[2 * e + 1];
+    const bool had = isfinite(rx) && isfinite(ry) && a.ecell[e].x != INT_MIN;
+    warp_near_at(a, e, px, py, c, [&](int o) {
+        if (!(had && list_holds(a, o, e, rx, ry))) mark_dirty(a, o, s_next, round_next);
+    });
+    __syncwarp();
+    if (lane == 0) {
+        mark_dirty(a, e, s_next, round_next);
+        rereference(a, e, px, py, c);
     }
 }
 
@@ -822,7 +859,9 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
             a.cny[e] = T(0);
         }
         a.crack[e] = 0;  // set by phase_reduce for elements touching a broken bond
-        warp_append(a.esc_list, (int*)&a.esc_cnt[0], escaped(a, e, p.x, p.y, a.esc_h_check), e);
+        const bool urg = escaped(a, e, p.x, p.y, a.lazy ? a.esc_h_urgent : a.esc_h_check);
+        warp_append(a.esc_list, (int*)&a.esc_cnt[0], urg, e);
+        if (a.lazy) warp_append(a.lazy_list, &a.lazy_cnt[0], !urg && escaped(a, e, p.x, p.y, a.esc_h_check), e);
     }
 }
 
@@ -1356,7 +1395,9 @@ struct ForceCtx {
     const T *kin, *kvin, *rin, *ain;
     T *kout, *kvout, *rout, *aout;
     const uint8_t* act;
-    T esc_h;  // escape threshold of this substep's test
+    T esc_h;  // escape threshold of this substep's test (urgent in lazy mode)
+    T h_lazy;           // lazy threshold of this substep's test
+    bool lazy_detect;   // the next substep processes lazy escapes
     const SlotRec<T>* rec;
     bool last;
 };
@@ -1376,6 +1417,12 @@ __device__ __forceinline__ ForceCtx<T> force_ctx(const KArgs<T>& a, const Frame<
     c.aout = c.last ? F.dst.avel : a.sp_avel[s & 1];
     c.act = F.dst.active;
     c.esc_h = ((s + 1) % a.esc_period == 0) ? a.esc_h_check : a.esc_h_urgent;
+    c.h_lazy = a.esc_h_check;
+    c.lazy_detect = false;
+    if (a.lazy) {
+        c.esc_h = a.esc_h_urgent;
+        c.lazy_detect = ((s + 1) % 2 == 0) && (s + 2 < a.k_sub);
+    }
     c.rec = reinterpret_cast<const SlotRec<T>*>(a.slotrec);
     return c;
 }
@@ -1441,11 +1488,22 @@ __device__ __forceinline__ bool contact_term(const ForceConst<T>& fc, bool h15, 
     return true;
 }
 
+// Escape code of element e at its new position: 2 = escaped past this substep's
+// threshold (processed before the next substep), 1 = lazily escaped (re-referenced
+// during the next force phase), 0 = neither.
+template <typename T>
+__device__ __forceinline__ int esc_code(const KArgs<T>& a, const ForceCtx<T>& cx, int e, T px, T py) {
+    if (cx.last) return 0;
+    const T rx = a.pos_ref[2 * e], ry = a.pos_ref[2 * e + 1];
+    if (escaped_from(px, py, rx, ry, cx.esc_h)) return 2;
+    return (cx.lazy_detect && escaped_from(px, py, rx, ry, cx.h_lazy)) ? 1 : 0;
+}
+
 // Drag, rotational drag and the semi-implicit update of an active element
 // from its bond and contact sums; stores the substep's output and returns
-// whether e escaped its reference ball.
+// its escape code (esc_code).
 template <typename T>
-__device__ __forceinline__ bool integrate_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx, int e,
+__device__ __forceinline__ int integrate_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx, int e,
                                                   typename vec4_of<T>::type ke, typename vec2_of<T>::type ve,
                                                   typename vec4_of<T>::type ec, typename vec2_of<T>::type w, T sub,
                                                   typename vec2_of<T>::type so, T av, T rot, T fbx, T fby, T mb,
@@ -1500,11 +1558,11 @@ __device__ __forceinline__ bool integrate_element(const KArgs<T>& a, const Frame
     }
     cx.rout[e] = nrot;
     cx.aout[e] = nav;
-    return !cx.last && escaped(a, e, npx, npy, cx.esc_h);
+    return esc_code(a, cx, e, npx, npy);
 }
 
 // Forces, torque and the semi-implicit update of element e for one substep,
-// one thread per element; returns whether e escaped its reference ball.
+// one thread per element; returns e's escape code (esc_code).
 //
 // Latency layout: every load that depends only on e is issued first; then one
 // loop walks the bond slots and the contact candidates together, kBatch of
@@ -1514,7 +1572,7 @@ __device__ __forceinline__ bool integrate_element(const KArgs<T>& a, const Frame
 // e == bond_i first, then e == bond_j; candidates above e ascending, then
 // below e ascending), so the interleaving does not change any rounding.
 template <typename T>
-__device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
+__device__ __forceinline__ int force_element(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
                                               int e) {
     typedef typename vec2_of<T>::type V2;
     typedef typename vec4_of<T>::type V4;
@@ -1538,7 +1596,7 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
         }
         cx.rout[e] = rot0;
         cx.aout[e] = av0;
-        return !cx.last && escaped(a, e, ke.x, ke.y, cx.esc_h);
+        return esc_code(a, cx, e, ke.x, ke.y);
     }
     const int s0 = a.boff[e], s1 = a.boff[e + 1];
     const int nc = a.ncnt[e];
@@ -1613,9 +1671,9 @@ __device__ __forceinline__ bool force_element(const KArgs<T>& a, const Frame<T>&
 // gathers are in flight at once; the terms are then summed in slot / candidate
 // order through shuffles, exactly as force_element adds them.  For substeps
 // with few active elements, where one element's chain of dependent gathers
-// decides the phase's length.  Every lane returns the escape flag.
+// decides the phase's length.  Every lane returns the escape code.
 template <typename T>
-__device__ __forceinline__ bool force_element_warp(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
+__device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
                                                    int e) {
     typedef typename vec2_of<T>::type V2;
     typedef typename vec4_of<T>::type V4;
@@ -1679,7 +1737,7 @@ __device__ __forceinline__ bool force_element_warp(const KArgs<T>& a, const Fram
             mi = ((em >> l) & 1u) ? mi + h : mi - h;
         }
     }
-    bool esc = false;
+    int esc = 0;
     if (lane == 0)
         esc = integrate_element(a, F, cx, e, ke, ve, ld4(a.econ, e), ld2(F.vw, e), F.dst.sub[e], ld2(a.soi, e),
                                 cx.ain[e], cx.rin[e], fbx, fby, mb, fix, fiy, mi);
@@ -1687,11 +1745,13 @@ __device__ __forceinline__ bool force_element_warp(const KArgs<T>& a, const Fram
 }
 
 template <typename T>
-__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigned round, bool has_dirty) {
+__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigned round, bool has_dirty,
+                            int n_lazy) {
     const ForceCtx<T> cx = force_ctx(a, F, s);
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
     int* esc_ctr = (int*)&a.esc_cnt[s + 1];
+    int* lazy_ctr = &a.lazy_cnt[s + 1];
     const int warp = gtid >> 5, nwarps = gsz >> 5, lane = threadIdx.x & 31;
     const int nd = has_dirty ? *((volatile int*)&a.dirty_cnt[s]) : 0;
     if (has_dirty) {
@@ -1705,13 +1765,20 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
             const int e = a.dirty_list[q];
             warp_build(a, e, sbuf[wl], &scnt[wl]);
             // a frozen element's substep buffers and output are written for the frame
-            if (cx.act[e] && force_element_warp(a, F, cx, e) && lane == 0) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+            const int code = cx.act[e] ? force_element_warp(a, F, cx, e) : 0;
+            if (lane == 0 && code == 2) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+            if (lane == 0 && code == 1) a.lazy_list[atomicAdd(lazy_ctr, 1)] = e;
             __syncwarp();
         }
+    } else if (n_lazy > 0) {
+        // lazy escapes of this substep: a warp each, beside the force work
+        for (int q = warp; q < n_lazy; q += nwarps) lazy_escape_warp(a, cx.kin, a.lazy_list[q], s + 1, round + 1u);
     }
-    // The warps that rebuilt a list above take no share of the element loop
-    // (while enough warps remain), so they do not finish the phase last.
-    const int skip = (nd < nwarps / 2) ? nd : 0;
+    // The warps that rebuilt a list (or took a lazy escape) above take no share
+    // of the element loop (while enough warps remain), so they do not finish
+    // the phase last.
+    const int nspecial = has_dirty ? nd : n_lazy;
+    const int skip = (nspecial < nwarps / 2) ? nspecial : 0;
     if (warp < skip) return;
     // Only active elements move (frozen ones were carried over by phase_reduce).
     // Chunks of 32 active elements: every warp starts with one chunk of its own,
@@ -1724,8 +1791,9 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
         for (int i = warp - skip; i < na; i += nw2) {
             const int e = a.act_list[i];
             if (has_dirty && a.dirty[e] == round) continue;
-            const bool esc = force_element_warp(a, F, cx, e);
-            if (!cx.last && esc && lane == 0) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+            const int code = force_element_warp(a, F, cx, e);
+            if (lane == 0 && code == 2) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+            if (lane == 0 && code == 1) a.lazy_list[atomicAdd(lazy_ctr, 1)] = e;
         }
         return;
     }
@@ -1738,8 +1806,11 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
         const int i = c * 32 + lane;
         const int e = (i < na) ? a.act_list[i] : -1;
         if (e >= 0 && !(has_dirty && a.dirty[e] == round)) {
-            const bool esc = force_element(a, F, cx, e);
-            if (!cx.last) warp_append(a.esc_list, esc_ctr, esc, e);
+            const int code = force_element(a, F, cx, e);
+            if (!cx.last) {
+                warp_append(a.esc_list, esc_ctr, code == 2, e);
+                warp_append(a.lazy_list, lazy_ctr, code == 1, e);
+            }
         }
         c = __shfl_sync(0xffffffffu, next, 0);
     }
@@ -1986,6 +2057,7 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
             a.d_fmag[e] = a.fraw[e] * sys_scale(a, scale, a.nsys > 1 ? a.sys_of[e] : 0);
     for (int i = gtid; i < a.k_sub + 2; i += gsz) {
         a.esc_cnt[i] = 0u;
+        a.lazy_cnt[i] = 0;
         a.dirty_cnt[i] = 0;
         a.work_cnt[i] = 0;
     }
@@ -2026,16 +2098,23 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
             const int sub = (p - 4) % 3;
             const unsigned cnt = *((volatile unsigned*)&a.esc_cnt[s]);
             const bool all = (unsigned long long)cnt * 8ull > (unsigned long long)a.n;
+            // lazily escaped elements are taken at even substeps with a successor
+            const bool lazy_sub = a.lazy && (s % 2 == 0) && (s + 1 < k);
+            const int n_lazy = lazy_sub ? *((volatile int*)&a.lazy_cnt[s]) : 0;
             // stamp of this rebuild round, unique since the dirty stamps were last cleared
             const unsigned round = a.round_base + (unsigned)(f * k + s) + 1u;
             if (sub == 0) {
                 if (cnt == 0u) continue;  // uniform: no barrier either
-                phase_escape(a, a.kin[s & 1], cnt, s, round, all);
+                // with escapes to process now, the lazy ones of this substep join them
+                phase_escape(a, a.kin[s & 1], cnt, n_lazy, s, round, all);
             } else if (sub == 1) {
                 if (cnt == 0u || !all) continue;
                 phase_build_all(a);
             } else {
-                phase_force(a, F, s, round, cnt != 0u && !all);
+                // lists to rebuild: this round's marks (escape phase, or the lazy
+                // escapes of the previous substep)
+                const int nd = *((volatile int*)&a.dirty_cnt[s]);
+                phase_force(a, F, s, round, !all && nd > 0, (cnt == 0u) ? n_lazy : 0);
             }
         }
         // a barrier after every phase but the last; with profiling on, after the
