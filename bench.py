@@ -150,6 +150,11 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            # nvidia-smi's first query can hold the GPU up for a while: let it
+            # complete (first sample written, 5 s at most) before the timed region
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
