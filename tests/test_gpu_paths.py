@@ -173,3 +173,29 @@ def test_work_splits_give_identical_results_ship_in_the_medium_field():
     assert int(runs[0][0].elem_active.sum()) > 0  # the ship met the ice
     assert fs.info()["escaped_total"] > 0
     fs.close()
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_lazy_escapes_with_odd_and_even_substep_counts(golden64, k):
+    """Lazy escapes are taken at even substeps that have a successor in the frame;
+    with 3 or 4 substeps per frame the trajectory at skin 2.4 m (lazy: wide enough
+    for the longer substeps' largest move) equals the one at 0.3 m (every escape
+    processed at once) bit for bit."""
+    from mbd_icenav_b200 import sim
+    from mbd_icenav_b200.config import IceMaterial
+    from helpers import B_THRUST, SCENARIOS, default_cfg, shipdyn_from_golden, static_from_golden
+    g = golden64
+    L, B, _, dt, _, auto, flex = SCENARIOS["small"]
+    o_st, o_sh = initial_state(g, "small", np.float64)
+    dmax = np.sqrt(2.0) * float(default_cfg().velocity_clip[1]) * dt / k
+    assert 0.99 * (0.5 * 2.4 - dmax) >= 0.25 * 2.4  # lazy mode at 2.4 m
+    out = []
+    for skin in (0.3, 2.4):
+        fs = sim.make_frame_step(static_from_golden(g, "small"), default_cfg(), shipdyn_from_golden(g, "small"), L, B,
+                                 k, dt, dt / k, auto, B_THRUST, 1.0, material=IceMaterial(flexural_strength_base=flex),
+                                 device=torch.device("cuda", 0), dtype=torch.float64, skin=skin)
+        st0, sh0 = to_gpu_state(o_st, o_sh, torch.float64)
+        out.append(fs.scan_segment(st0, sh0, *_scan_inputs(g, "small", 0, 100, torch.float64)))
+        fs.close()
+    _assert_same(out)
+    assert out[0][0].elem_active.any()
