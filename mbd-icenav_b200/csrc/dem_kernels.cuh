@@ -211,8 +211,13 @@ __device__ __forceinline__ Frame<T> make_frame(const KArgs<T>& a, int f) {
     Frame<T> F;
     F.f = f;
     const int K = a.K;
-    F.dst = (((K - 1 - f) & 1) == 0) ? a.out : a.tmp;
-    F.src = (f == 0) ? a.in : ((((K - f) & 1) == 0) ? a.out : a.tmp);
+    // frame 0 reads the call's input and writes all of `out`; later frames update
+    // `out` in place (every phase reads and writes only its own element or bond,
+    // or reads a partner's flag that only turns on), so state that does not
+    // change (frozen elements, bonds between them) is not copied frame to frame
+    F.dst = a.out;
+    F.src = (f == 0) ? a.in : a.out;
+    (void)K;
     F.ship_dst = (f == K - 1) ? a.ship_out : a.ship_tmp[f & 1];
     F.ship_src = (f == 0) ? a.ship_in : a.ship_tmp[(f - 1) & 1];
     F.elig_in = (f == 0) ? a.elig0 : F.src.elig;
@@ -1307,7 +1312,12 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     const unsigned fstamp = frame_stamp(a, F);
     for (int e = gtid; e < a.n; e += gsz) {
         // activation (jax_simulation.py:498-509)
-        const bool ae = F.src.active[e] || a.fcoll[a.floe_of[e]];
+        const bool was = F.src.active[e] != 0;
+        const bool ae = was || a.fcoll[a.floe_of[e]];
+        // after the first frame of a call, an element frozen before and after
+        // this frame's activation has its state, substep buffers and frame
+        // output in place already (the previous frame wrote them)
+        if (F.f >= 1 && !ae) continue;
         F.dst.active[e] = ae ? 1 : 0;
         // packed kinematics read by substep 0
         const V2 p = ld2(F.src.pos, e), v = ld2(F.src.vel, e);
@@ -2001,11 +2011,25 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
                      al16(F.dst.dm0) && al16(F.src.dmmax) && al16(F.dst.dmmax) && al16(a.bstamp) &&
                      ((size_t)F.src.intact & 3u) == 0 && ((size_t)F.dst.intact & 3u) == 0;
     const int ng = (a.nb + 3) >> 2;
+    // updating in place (frames after the first of a call): bonds without an
+    // active end are already in place; only their history row is written
+    const bool inplace = F.src.ds == F.dst.ds;
     for (int g = gtid; g < ng; g += gsz) {
         const int b0 = 4 * g;
         const int cnt = min(4, a.nb - b0);
         unsigned st[4] = {0u, 0u, 0u, 0u};
         unsigned in4 = 0u;
+        if (inplace) {
+            for (int k = 0; k < cnt; ++k) {
+                const int b = b0 + k;
+                if (a.bstamp[b] == fstamp) {
+                    fracture_bond(a, F, scale, b);
+                } else if (a.h_intact) {
+                    a.h_intact[(size_t)F.f * a.nb + b] = F.src.intact[b] != 0 ? 1 : 0;
+                }
+            }
+            continue;
+        }
         if (vec && cnt == 4) {
             const uint4 s4 = *reinterpret_cast<const uint4*>(a.bstamp + b0);
             st[0] = s4.x;
