@@ -88,7 +88,7 @@ def load_field(name: str, seed: int):
     return f
 
 
-def algorithmic_bytes_per_frame(n: int, nb: int, V: int, k: int, n_act=None, nb_act=None) -> int:
+def algorithmic_bytes_per_frame(n: int, nb: int, V: int, k: int, n_act=None, nb_act=None, in_place=False) -> int:
     """Bytes each frame must move at minimum, fp32, bool = 1 B, i32 = 4 B.
 
     Per substep and active element: read pos 8 + vel 8 + rot 4 + w 4 + sub 4 +
@@ -99,11 +99,14 @@ def algorithmic_bytes_per_frame(n: int, nb: int, V: int, k: int, n_act=None, nb_
     Per substep and bond with an active end: i 4 + j 4 + rest length 4 + damage
     4 + intact 1 = 17 B (a bond between two frozen elements is not read).  Per
     frame: ship contact n (9V + 64) B and the bond update 50 B per bond.
-    ``n_act`` / ``nb_act`` default to n / nb (every element active).
+    ``n_act`` / ``nb_act`` default to n / nb (every element active).  ``in_place``:
+    a frame after the first of a multi-frame call, which updates the state in
+    place, so frozen elements have nothing to carry over (0 B per substep).
     """
     n_act = n if n_act is None else n_act
     nb_act = nb if nb_act is None else nb_act
-    return int(k * (89 * n_act + 49 * (n - n_act) + 17 * nb_act) + n * (9 * V + 64) + 50 * nb)
+    carry = 0 if in_place else 49 * (n - n_act)
+    return int(k * (89 * n_act + carry + 17 * nb_act) + n * (9 * V + 64) + 50 * nb)
 
 
 def active_counts(elem_active, bond_i, bond_j):
@@ -511,7 +514,11 @@ def run_rollouts(args, rank: int, world: int):
     if rank != 0:
         return None
     sizes = np.diff(b.system_start)
-    bpl = H * algorithmic_bytes_per_frame(n, nb, V, N_SUB, 0.5 * (act0[0] + act1[0]), 0.5 * (act0[1] + act1[1]))
+    # the batch's first frame carries frozen elements over; the other H - 1
+    # frames update the state in place
+    na_m, nba_m = 0.5 * (act0[0] + act1[0]), 0.5 * (act0[1] + act1[1])
+    bpl = (algorithmic_bytes_per_frame(n, nb, V, N_SUB, act0[0], act0[1])
+           + (H - 1) * algorithmic_bytes_per_frame(n, nb, V, N_SUB, na_m, nba_m, in_place=True))
     kern_s = sum(kern_ms) / 1e3 / K
     achieved = bpl / kern_s / 1e9
     peak, peak_kind = peak_hbm()
