@@ -64,6 +64,8 @@ struct DemHandle {
     int* act_list = nullptr;
     int* lazy_list = nullptr;
     int* lazy_cnt = nullptr;
+    int* counters = nullptr;  // block holding the per-call counters below
+    size_t counters_bytes = 0;
     unsigned* bstamp = nullptr;  // (nb) frame stamps of bonds with an active end
     int* act_cnt = nullptr;
     int* slot_owner = nullptr;
@@ -454,12 +456,9 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.stats = h->stats;
 
     // per-call scratch reset (the kernel keeps it clean between frames)
-    CUDA_TRY(h, cudaMemsetAsync(h->fcoll, 0, sizeof(int) * std::max(h->nf, 1), stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->fmax, 0, sizeof(unsigned long long) * std::max(h->nf, 1), stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->esc_cnt, 0, sizeof(unsigned) * (h->P.n_ice_steps + 2), stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->dirty_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->work_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->lazy_cnt, 0, sizeof(int) * (h->P.n_ice_steps + 2), stream));
+    // per-call counters (escapes, rebuilds, work, lazy escapes, barrier, near
+    // count) in one memset; the per-floe flags are cleared by each frame's cull
+    CUDA_TRY(h, cudaMemsetAsync(h->counters, 0, h->counters_bytes, stream));
     {
         // every rebuild round of every call gets its own dirty stamp; clear the
         // stamps before the counter would wrap
@@ -474,8 +473,6 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
         h->fail_phase = -1;
         h->round_base += need;
     }
-    CUDA_TRY(h, cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * 2, stream));
-    CUDA_TRY(h, cudaMemsetAsync(h->near_cnt, 0, sizeof(int), stream));
     if (h->profiling) CUDA_TRY(h, cudaMemsetAsync(h->ptimes, 0, sizeof(unsigned long long) * 2, stream));
 
     const int k = h->P.n_ice_steps;
@@ -660,7 +657,6 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->vert_r, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bcnt, sizeof(int) * (size_t)h->n_buckets))) return fail(rc);
     if ((rc = dev_alloc(h, &h->near_list, sizeof(int) * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->near_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->cpen, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->cnx, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->cny, es * n))) return fail(rc);
@@ -674,15 +670,24 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->comp_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->esc_list, sizeof(int) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->dirty_list, sizeof(int) * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->dirty_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->work_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->lazy_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->lazy_cnt, sizeof(int) * (h->P.n_ice_steps + 2)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bstamp, sizeof(unsigned) * std::max(nb, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->esc_cnt, sizeof(unsigned) * (h->P.n_ice_steps + 2)))) return fail(rc);
+    {
+        // the per-call counters in one block, cleared by one memset per call:
+        // esc_cnt, dirty_cnt, work_cnt, lazy_cnt (k + 2 each), bar (2), near_cnt (1)
+        const size_t k2 = (size_t)h->P.n_ice_steps + 2;
+        if ((rc = dev_alloc(h, &h->counters, sizeof(int) * (4 * k2 + 3)))) return fail(rc);
+        h->counters_bytes = sizeof(int) * (4 * k2 + 3);
+        h->esc_cnt = reinterpret_cast<unsigned*>(h->counters);
+        h->dirty_cnt = h->counters + k2;
+        h->work_cnt = h->counters + 2 * k2;
+        h->lazy_cnt = h->counters + 3 * k2;
+        h->bar = reinterpret_cast<unsigned*>(h->counters + 4 * k2);
+        h->near_cnt = h->counters + 4 * k2 + 2;
+    }
     if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fraw, es * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->crack, n))) return fail(rc);
@@ -719,7 +724,6 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->fscal, sizeof(double) * 4 * h->nsys))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ptimes, sizeof(unsigned long long) * (2 + 2 * dem::kMaxPhaseTimes)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->sprow, es * 6))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->bar, sizeof(unsigned) * 2))) return fail(rc);
     if ((rc = dev_alloc(h, &h->status, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->stats, sizeof(long long) * 8))) return fail(rc);
     ce = cudaMallocHost(&h->host_status, sizeof(int));
