@@ -86,18 +86,6 @@ struct DemHandle {
     void* sp_rot[2] = {nullptr, nullptr};
     void* sp_avel[2] = {nullptr, nullptr};
     // frame ping-pong state for scans
-    void* t_pos = nullptr;
-    void* t_vel = nullptr;
-    void* t_rot = nullptr;
-    void* t_avel = nullptr;
-    void* t_sub = nullptr;
-    uint8_t* t_intact = nullptr;
-    void* t_dmg = nullptr;
-    void* t_dm0 = nullptr;
-    void* t_dmmax = nullptr;
-    void* t_ds = nullptr;
-    uint8_t* t_active = nullptr;
-    uint8_t* t_elig = nullptr;
     void* slotrec = nullptr;
     void* r3 = nullptr;
     void* econ = nullptr;
@@ -408,20 +396,6 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.ptimes = h->profiling ? h->ptimes : nullptr;
     a.in = ice_ptrs<T>(in);
     a.out = ice_ptrs<T>(out);
-    DemIceState tmp;
-    tmp.positions = h->t_pos;
-    tmp.velocities = h->t_vel;
-    tmp.rotations = h->t_rot;
-    tmp.angular_vels = h->t_avel;
-    tmp.submergence = h->t_sub;
-    tmp.bond_intact = h->t_intact;
-    tmp.bond_damage = h->t_dmg;
-    tmp.bond_delta_m_0 = h->t_dm0;
-    tmp.bond_delta_m_max = h->t_dmmax;
-    tmp.bond_delta_s = h->t_ds;
-    tmp.elem_active = h->t_active;
-    tmp.dpdem_floe_eligible = h->t_elig;
-    a.tmp = ice_ptrs<T>(&tmp);
     a.ship_in = ship_ptrs<T>(ship_in);
     a.ship_out = ship_ptrs<T>(ship_out);
     T* st = (T*)h->ship_tmp;
@@ -705,18 +679,6 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
         if ((rc = dev_alloc(h, &h->sp_rot[i], es * n))) return fail(rc);
         if ((rc = dev_alloc(h, &h->sp_avel[i], es * n))) return fail(rc);
     }
-    if ((rc = dev_alloc(h, &h->t_pos, es * 2 * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_vel, es * 2 * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_rot, es * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_avel, es * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_sub, es * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_intact, std::max(nb, 1)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_dmg, es * std::max(nb, 1)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_dm0, es * std::max(nb, 1)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_dmmax, es * std::max(nb, 1)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_ds, es * std::max(nb, 1)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_active, n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->t_elig, nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->ship_tmp, es * 30 * h->nsys))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slotrec, (es == 4 ? 16 : 32) * slots.size()))) return fail(rc);
     if ((rc = dev_alloc(h, &h->r3, es * n))) return fail(rc);

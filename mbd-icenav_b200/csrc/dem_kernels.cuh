@@ -171,7 +171,7 @@ struct KArgs {
     double* fscal;      // (4) frame scalars: thrust scale, F_x, F_y, M
     unsigned long long* ptimes;  // (2 * kMaxPhaseTimes) [phase, globaltimer ns] or null
     // call arguments
-    IcePtrs<T> in, out, tmp;
+    IcePtrs<T> in, out;  // frame 0 reads in; every frame writes out (in place after frame 0)
     ShipPtrs<T> ship_in, ship_out, ship_tmp[2];
     const T* setpoints;   // (K,6)
     const T* vw;          // (K,n,2)
@@ -217,7 +217,6 @@ __device__ __forceinline__ Frame<T> make_frame(const KArgs<T>& a, int f) {
     // change (frozen elements, bonds between them) is not copied frame to frame
     F.dst = a.out;
     F.src = (f == 0) ? a.in : a.out;
-    (void)K;
     F.ship_dst = (f == K - 1) ? a.ship_out : a.ship_tmp[f & 1];
     F.ship_src = (f == 0) ? a.ship_in : a.ship_tmp[(f - 1) & 1];
     F.elig_in = (f == 0) ? a.elig0 : F.src.elig;
