@@ -7,8 +7,8 @@ passed in its place (fields are read by name with ``getattr``).
 
 ``IceMaterial`` holds the constants the reference keeps as class attributes of
 ``IceProperties`` (``medea_ice_ship/properties.py:6-22``).  They are explicit
-here so a run can change them (BASELINE config 0 asks for a 900 kg/m^3 ice
-density and a 0.5 MPa strength) without patching a class.
+here so a run can change them (the small three-floe workload uses a 900 kg/m^3
+ice density and a 0.5 MPa strength) without patching a class.
 """
 from __future__ import annotations
 

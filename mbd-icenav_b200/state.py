@@ -200,7 +200,7 @@ def ship_dynamics_arrays(ship_props, cfg, ship_length: float, ship_beam: float,
     """Vessel matrices, pole-placement gains and hull outline (``jax_ice_state.py:270-343``).
 
     ``hull_local`` overrides the default 62-point tapered outline (used by the
-    7-vertex pointed hull of BASELINE config 0).
+    7-vertex pointed hull of the seeded benchmark fields).
     """
     m = ship_props.mass
     izz = (1.0 / 12.0) * m * (ship_length ** 2 + ship_beam ** 2)

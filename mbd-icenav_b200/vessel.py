@@ -84,7 +84,7 @@ def tapered_hull_outline(ship_length: float, ship_beam: float, n_pts: int = 30) 
 
 
 def pointed_hull_outline(ship_length: float, ship_beam: float) -> np.ndarray:
-    """A 7-vertex pointed hull (bow at +x), as BASELINE config 0 specifies."""
+    """A 7-vertex pointed hull (bow at +x), 60 x 12 m in the seeded benchmark fields."""
     L2, B2 = ship_length / 2.0, ship_beam / 2.0
     return np.array([[L2, 0.0], [0.5 * L2, B2], [-0.8 * L2, B2], [-L2, 0.6 * B2],
                      [-L2, -0.6 * B2], [-0.8 * L2, -B2], [0.5 * L2, -B2]], dtype=np.float64)

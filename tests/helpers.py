@@ -18,7 +18,7 @@ STATIC_FIELDS = ("local_polys_padded", "poly_mask", "poly_n_verts", "masses", "i
                  "bond_areas", "sigma_bar_bond", "initial_floe_of", "k_n", "k_s")
 SHIPDYN_FIELDS = ("M3inv", "D3", "mass", "Izz", "Kp", "Kd", "Ki", "B_pinv", "n_max", "ship_hull_local")
 
-# BASELINE's small workload material (rho 900, 0.5 MPa) and dilation
+# material of the small three-floe workload (rho 900, 0.5 MPa) and its dilation
 SMALL_FLEX = 0.5e6
 
 B_THRUST = np.array([[0, 0, 0, 0, 1, 1], [1, 1, 1, 1, 0, 0], [30, 22, -22, -30, -8, 8]], float) \
