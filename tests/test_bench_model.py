@@ -1,0 +1,33 @@
+"""The bench's algorithmic byte count (the roofline's numerator), on CPU."""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+N, NB, V, K = 244_819, 825_618, 11, 10
+
+
+def test_all_active_count_of_the_large_field():
+    # k (89 n + 17 n_b) + n (9 V + 64) + 50 n_b
+    assert bench.algorithmic_bytes_per_frame(N, NB, V, K) == 439_430_367
+
+
+def test_frozen_elements_carry_their_state_over_at_49_bytes():
+    full = bench.algorithmic_bytes_per_frame(N, NB, V, K)
+    frozen = bench.algorithmic_bytes_per_frame(N, NB, V, K, n_act=0, nb_act=0)
+    assert full - frozen == K * ((89 - 49) * N + 17 * NB)
+    # in place (frames after the first of a call) they carry nothing over
+    inplace = bench.algorithmic_bytes_per_frame(N, NB, V, K, n_act=0, nb_act=0, in_place=True)
+    assert frozen - inplace == K * 49 * N
+    assert inplace == N * (9 * V + 64) + 50 * NB
+
+
+def test_active_counts_on_cpu_tensors():
+    torch = __import__("torch")
+    act = torch.tensor([True, False, False, True, False])
+    bi = torch.tensor([0, 1, 2], dtype=torch.int32)
+    bj = torch.tensor([1, 2, 4], dtype=torch.int32)
+    assert bench.active_counts(act, bi, bj) == (2, 1)
