@@ -482,7 +482,9 @@ __device__ void warp_build(const KArgs<T>& a, int e, int* sbuf, int* scnt) {
     const int found = *scnt;
     const int cnt = min(found, cap);
     // drop repeats (a stale and a current entry of one element), in parallel:
-    // entry i stays if no earlier entry holds the same index
+    // entry i stays if no earlier entry holds the same index.  All lanes walk
+    // the buffer together (broadcast reads, no early exit, so the reads
+    // pipeline); a lane holds entries lane, lane + 32, ...
     constexpr int kPer = (2 * kMaxNbLocal + 31) / 32;
     int v[kPer];
     bool keep[kPer];
@@ -491,8 +493,21 @@ __device__ void warp_build(const KArgs<T>& a, int e, int* sbuf, int* scnt) {
         const int i = lane + 32 * k;
         v[k] = (i < cnt) ? sbuf[i] : -1;
         keep[k] = i < cnt;
-        for (int j = 0; keep[k] && j < i; ++j)
-            if (sbuf[j] == v[k]) keep[k] = false;
+    }
+    if (cnt <= 64) {
+#pragma unroll 4
+        for (int j = 0; j < cnt; ++j) {
+            const int u = sbuf[j];
+            keep[0] = keep[0] && !(j < lane && u == v[0]);
+            keep[1] = keep[1] && !(j < lane + 32 && u == v[1]);
+        }
+    } else {
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) {
+            const int u = sbuf[j];
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) keep[k] = keep[k] && !(j < lane + 32 * k && u == v[k]);
+        }
     }
     __syncwarp();
 #pragma unroll
@@ -516,19 +531,88 @@ __device__ void warp_build(const KArgs<T>& a, int e, int* sbuf, int* scnt) {
     }
     const int m = min(w, a.max_nb);
     // slot of a kept index = its rank among the kept ones, indices above e first
+    int r[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) r[k] = 0;
+    if (cnt <= 64) {
+#pragma unroll 4
+        for (int j = 0; j < cnt; ++j) {
+            const int u = sbuf[j];
+            r[0] += (u >= 0 && u < v[0]) ? 1 : 0;
+            r[1] += (u >= 0 && u < v[1]) ? 1 : 0;
+        }
+    } else {
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) {
+            const int u = sbuf[j];
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) r[k] += (u >= 0 && u < v[k]) ? 1 : 0;
+        }
+    }
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
         if (!keep[k]) continue;
-        int r = 0;
-        for (int j = 0; j < cnt; ++j) {
-            const int u = sbuf[j];
-            r += (u >= 0 && u < v[k]) ? 1 : 0;
-        }
-        const int pos = (v[k] > e) ? r - split : (w - split) + r;
+        const int pos = (v[k] > e) ? r[k] - split : (w - split) + r[k];
         if (pos < m) a.nbr[(size_t)pos * a.n + e] = v[k];
     }
     if (lane == 0) a.ncnt[e] = m;
     __syncwarp();
+}
+
+// The same list build by a whole CTA (every thread must call it with the same
+// e): the stencil entries are scanned in one load round (block_near_at), and
+// thread t checks gathered candidate t (at most 2 kMaxNbLocal <= kThreads).
+// The list equals warp_build's: the same candidates, repeats dropped, the
+// same order and the same capacity flags.
+template <typename T>
+__device__ void block_build(const KArgs<T>& a, int e) {
+    constexpr int cap = 2 * kMaxNbLocal;
+    static_assert(cap <= kThreads, "one candidate per thread");
+    __shared__ int s_c[cap];
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    block_near_at(a, e, a.pos_ref[2 * e], a.pos_ref[2 * e + 1], a.ecell[e], [&](int o) {
+        const int slot = atomicAdd(&s_n, 1);
+        if (slot < cap) s_c[slot] = o;
+    });  // ends with __syncthreads (or returns at once, before any, for an element without a cell)
+    __syncthreads();
+    const int found = s_n;
+    const int cnt = min(found, cap);
+    const int t = threadIdx.x;
+    const int v = (t < cnt) ? s_c[t] : -1;
+    bool keep = t < cnt;
+    if ((t & ~31) < cnt) {  // warp-uniform: warps holding candidates
+#pragma unroll 4
+        for (int j = 0; j < cnt; ++j) {
+            const int u = s_c[j];
+            keep = keep && !(j < t && u == v);
+        }
+    }
+    const int w = __syncthreads_count(keep);
+    const int split = __syncthreads_count(keep && v < e);  // kept indices below e
+    if (t < cnt && !keep) s_c[t] = -1;
+    __syncthreads();
+    if (t == 0) {
+        if (found > cap || w > a.max_nb) {
+            atomicMax(a.status, DEM_ERR_CAPACITY);
+            atomicOr((unsigned long long*)&a.stats[5], 2ull);  // a neighbour list overflowed
+        }
+        if (w > 16) atomicMax((unsigned long long*)&a.stats[1], (unsigned long long)w);
+    }
+    const int m = min(w, a.max_nb);
+    if (keep) {
+        int r = 0;
+#pragma unroll 4
+        for (int j = 0; j < cnt; ++j) {
+            const int u = s_c[j];
+            r += (u >= 0 && u < v) ? 1 : 0;
+        }
+        const int pos = (v > e) ? r - split : (w - split) + r;
+        if (pos < m) a.nbr[(size_t)pos * a.n + e] = v;
+    }
+    if (t == 0) a.ncnt[e] = m;
+    __syncthreads();  // the list is complete for the CTA; s_c / s_n are reused by the next call
 }
 
 // Queue bucket b for compaction at the next frame start.
@@ -670,6 +754,25 @@ __device__ __forceinline__ void lazy_escape_warp(const KArgs<T>& a, const T* kin
     });
     __syncwarp();
     if (lane == 0) {
+        mark_dirty(a, e, s_next, round_next);
+        rereference(a, e, px, py, c);
+    }
+}
+
+// The same lazy escape by a whole CTA (every thread must call it with the same
+// e), its stencil entries in one load round.
+template <typename T>
+__device__ __forceinline__ void lazy_escape_block(const KArgs<T>& a, const T* kin, int e, int s_next,
+                                                  unsigned round_next) {
+    const T px = kin[4 * (size_t)e], py = kin[4 * (size_t)e + 1];
+    const int2 c = (jfinite(px) && jfinite(py)) ? cell_of(a, px, py) : make_int2(INT_MIN, INT_MIN);
+    const double rx = (double)a.pos_ref[2 * e], ry = (double)a.pos_ref[2 * e + 1];
+    const bool had = isfinite(rx) && isfinite(ry) && a.ecell[e].x != INT_MIN;
+    block_near_at(a, e, px, py, c, [&](int o) {
+        if (!(had && list_holds(a, o, e, rx, ry))) mark_dirty(a, o, s_next, round_next);
+    });
+    __syncthreads();  // every thread is done with e's old reference
+    if (threadIdx.x == 0) {
         mark_dirty(a, e, s_next, round_next);
         rereference(a, e, px, py, c);
     }
@@ -1677,10 +1780,13 @@ __device__ __forceinline__ int force_element(const KArgs<T>& a, const Frame<T>& 
 
 // The same substep for one active element computed by a whole warp: lane j
 // takes bond slot j and contact candidate j (32 at a time), so all partner
-// gathers are in flight at once; the terms are then summed in slot / candidate
-// order through shuffles, exactly as force_element adds them.  For substeps
-// with few active elements, where one element's chain of dependent gathers
-// decides the phase's length.  Every lane returns the escape code.
+// gathers are in flight at once; the terms then go through the warp's slice of
+// shared memory, and every lane sums them in slot / candidate order, exactly as
+// force_element adds them (a select keeps the sum unchanged for a slot without
+// a term, so the loop has no branch and its reads pipeline).  The element's own
+// loads for the integration are issued first, beside the gathers.  For
+// substeps with few active elements, where one element's chain of dependent
+// loads decides the phase's length.  Every lane returns the escape code.
 template <typename T>
 __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame<T>& F, const ForceCtx<T>& cx,
                                                    int e) {
@@ -1690,10 +1796,18 @@ __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame
     const int lane = threadIdx.x & 31;
     const T *kin = cx.kin, *kvin = cx.kvin;
     const bool h15 = a.fc.h15 != 0;
+    __shared__ T s_terms[kThreads / 32][6 * 32];
+    T* wt = s_terms[threadIdx.x >> 5];
     const V4 ke = ld4(kin, e);
     const V2 ve = ld2(kvin, e);
     const int s0 = a.boff[e], s1 = a.boff[e + 1];
     const int nc = a.ncnt[e];
+    // the integration's own loads (no other warp writes these during the phase)
+    const V4 ec = ld4(a.econ, e);
+    const V2 w = ld2(F.vw, e);
+    const T sub = F.dst.sub[e];
+    const V2 so = ld2(a.soi, e);
+    const T av = cx.ain[e], rot = cx.rin[e];
     const int nbe = s1 - s0;
     const int m = max(nbe, nc);
     T fbx = T(0), fby = T(0), mb = T(0);
@@ -1719,37 +1833,43 @@ __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame
         T tx = T(0), ty = T(0), hm = T(0);
         const bool eis = e < o;
         const bool cv = (o >= 0) && contact_term(a.fc, h15, ke, ve, ko, vo, eis, tx, ty, hm);
-        unsigned bm = __ballot_sync(full, bv);
+        const unsigned bm = __ballot_sync(full, bv);
         const unsigned rm = __ballot_sync(full, bv && r.o < 0);
-        unsigned cm = __ballot_sync(full, cv);
+        const unsigned cm = __ballot_sync(full, cv);
         const unsigned em = __ballot_sync(full, cv && eis);
-        while (bm) {  // warp-uniform trip count
-            const int l = __ffs(bm) - 1;
-            bm &= bm - 1;
-            const T x = __shfl_sync(full, bfx, l), y = __shfl_sync(full, bfy, l), c = __shfl_sync(full, bcr, l);
-            if ((rm >> l) & 1u) {
-                fbx -= x;
-                fby -= y;
-                mb -= c;
-            } else {
-                fbx += x;
-                fby += y;
-                mb += c;
-            }
+        wt[lane] = bfx;
+        wt[32 + lane] = bfy;
+        wt[64 + lane] = bcr;
+        wt[96 + lane] = tx;
+        wt[128 + lane] = ty;
+        wt[160 + lane] = hm;
+        __syncwarp();
+        const int nbp = min(32, nbe - j0), ncp = min(32, nc - j0);  // warp-uniform
+#pragma unroll 4
+        for (int l = 0; l < nbp; ++l) {
+            const T x = wt[l], y = wt[32 + l], c = wt[64 + l];
+            const bool on = (bm >> l) & 1u, neg = (rm >> l) & 1u;
+            const T sx = neg ? fbx - x : fbx + x;
+            const T sy = neg ? fby - y : fby + y;
+            const T sc = neg ? mb - c : mb + c;
+            fbx = on ? sx : fbx;
+            fby = on ? sy : fby;
+            mb = on ? sc : mb;
         }
-        while (cm) {
-            const int l = __ffs(cm) - 1;
-            cm &= cm - 1;
-            const T x = __shfl_sync(full, tx, l), y = __shfl_sync(full, ty, l), h = __shfl_sync(full, hm, l);
-            fix += x;
-            fiy += y;
-            mi = ((em >> l) & 1u) ? mi + h : mi - h;
+#pragma unroll 4
+        for (int l = 0; l < ncp; ++l) {
+            const T x = wt[96 + l], y = wt[128 + l], h = wt[160 + l];
+            const bool on = (cm >> l) & 1u;
+            const T sx = fix + x, sy = fiy + y;
+            const T sm = ((em >> l) & 1u) ? mi + h : mi - h;
+            fix = on ? sx : fix;
+            fiy = on ? sy : fiy;
+            mi = on ? sm : mi;
         }
+        __syncwarp();  // the next pass overwrites the terms
     }
     int esc = 0;
-    if (lane == 0)
-        esc = integrate_element(a, F, cx, e, ke, ve, ld4(a.econ, e), ld2(F.vw, e), F.dst.sub[e], ld2(a.soi, e),
-                                cx.ain[e], cx.rin[e], fbx, fby, mb, fix, fiy, mi);
+    if (lane == 0) esc = integrate_element(a, F, cx, e, ke, ve, ec, w, sub, so, av, rot, fbx, fby, mb, fix, fiy, mi);
     return __shfl_sync(full, esc, 0);
 }
 
@@ -1763,13 +1883,36 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     int* lazy_ctr = &a.lazy_cnt[s + 1];
     const int warp = gtid >> 5, nwarps = gsz >> 5, lane = threadIdx.x & 31;
     const int nd = has_dirty ? *((volatile int*)&a.dirty_cnt[s]) : 0;
-    if (has_dirty) {
-        // elements whose list this round invalidated: one warp rebuilds the list,
-        // then lane 0 computes the element (the main loop below skips them)
+    if (has_dirty && gtid == 0) atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)nd);
+    // The special items of this substep: elements whose list this round
+    // invalidated (rebuilt, then computed, here; the element loop below skips
+    // them), or the lazy escapes.  A few take a CTA each, so that a stencil scan
+    // is one load round, on CTAs that then take no element work; many take a
+    // warp each.
+    const int nspecial = has_dirty ? nd : n_lazy;
+    const bool cta_items = nspecial > 0 && a.mark_split != DEM_SPLIT_WARP &&
+                           nspecial <= (int)gridDim.x / (a.mark_split == DEM_SPLIT_CTA ? 2 : 4);
+    if (cta_items) {
+        if ((int)blockIdx.x < nspecial) {  // uniform over the CTA
+            if (has_dirty) {
+                const int e = a.dirty_list[blockIdx.x];
+                block_build(a, e);
+                if (threadIdx.x < 32) {
+                    // a frozen element's substep buffers and output are written for the frame
+                    const int code = cx.act[e] ? force_element_warp(a, F, cx, e) : 0;
+                    if (lane == 0 && code == 2) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
+                    if (lane == 0 && code == 1) a.lazy_list[atomicAdd(lazy_ctr, 1)] = e;
+                }
+            } else {
+                lazy_escape_block(a, cx.kin, a.lazy_list[blockIdx.x], s + 1, round + 1u);
+            }
+            return;
+        }
+    } else if (has_dirty) {
+        // one warp rebuilds the list, then computes the element
         __shared__ int sbuf[kThreads / 32][2 * kMaxNbLocal];
         __shared__ int scnt[kThreads / 32];
         const int wl = threadIdx.x >> 5;
-        if (gtid == 0) atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)nd);
         for (int q = warp; q < nd; q += nwarps) {
             const int e = a.dirty_list[q];
             warp_build(a, e, sbuf[wl], &scnt[wl]);
@@ -1785,9 +1928,8 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     }
     // The warps that rebuilt a list (or took a lazy escape) above take no share
     // of the element loop (while enough warps remain), so they do not finish
-    // the phase last.
-    const int nspecial = has_dirty ? nd : n_lazy;
-    const int skip = (nspecial < nwarps / 2) ? nspecial : 0;
+    // the phase last; with a CTA per item, those CTAs' warps.
+    const int skip = cta_items ? nspecial * (kThreads / 32) : ((nspecial < nwarps / 2) ? nspecial : 0);
     if (warp < skip) return;
     // Only active elements move (frozen ones were carried over by phase_reduce).
     // Chunks of 32 active elements: every warp starts with one chunk of its own,
