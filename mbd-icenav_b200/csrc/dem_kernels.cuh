@@ -1845,26 +1845,47 @@ __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame
         wt[160 + lane] = hm;
         __syncwarp();
         const int nbp = min(32, nbe - j0), ncp = min(32, nc - j0);  // warp-uniform
-#pragma unroll 4
-        for (int l = 0; l < nbp; ++l) {
-            const T x = wt[l], y = wt[32 + l], c = wt[64 + l];
-            const bool on = (bm >> l) & 1u, neg = (rm >> l) & 1u;
-            const T sx = neg ? fbx - x : fbx + x;
-            const T sy = neg ? fby - y : fby + y;
-            const T sc = neg ? mb - c : mb + c;
-            fbx = on ? sx : fbx;
-            fby = on ? sy : fby;
-            mb = on ? sc : mb;
+        // four terms per step: their twelve reads first, then the four sums in order
+        for (int l0 = 0; l0 < nbp; l0 += 4) {
+            T x[4], y[4], c[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int l = min(l0 + u, 31);
+                x[u] = wt[l];
+                y[u] = wt[32 + l];
+                c[u] = wt[64 + l];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int l = (l0 + u) & 31;
+                const bool on = (l0 + u < nbp) && ((bm >> l) & 1u), neg = (rm >> l) & 1u;
+                const T sx = neg ? fbx - x[u] : fbx + x[u];
+                const T sy = neg ? fby - y[u] : fby + y[u];
+                const T sc = neg ? mb - c[u] : mb + c[u];
+                fbx = on ? sx : fbx;
+                fby = on ? sy : fby;
+                mb = on ? sc : mb;
+            }
         }
-#pragma unroll 4
-        for (int l = 0; l < ncp; ++l) {
-            const T x = wt[96 + l], y = wt[128 + l], h = wt[160 + l];
-            const bool on = (cm >> l) & 1u;
-            const T sx = fix + x, sy = fiy + y;
-            const T sm = ((em >> l) & 1u) ? mi + h : mi - h;
-            fix = on ? sx : fix;
-            fiy = on ? sy : fiy;
-            mi = on ? sm : mi;
+        for (int l0 = 0; l0 < ncp; l0 += 4) {
+            T x[4], y[4], h[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int l = min(l0 + u, 31);
+                x[u] = wt[96 + l];
+                y[u] = wt[128 + l];
+                h[u] = wt[160 + l];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int l = (l0 + u) & 31;
+                const bool on = (l0 + u < ncp) && ((cm >> l) & 1u);
+                const T sx = fix + x[u], sy = fiy + y[u];
+                const T sm = ((em >> l) & 1u) ? mi + h[u] : mi - h[u];
+                fix = on ? sx : fix;
+                fiy = on ? sy : fiy;
+                mi = on ? sm : mi;
+            }
         }
         __syncwarp();  // the next pass overwrites the terms
     }
@@ -1874,15 +1895,15 @@ __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame
 }
 
 template <typename T>
-__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigned round, bool has_dirty,
-                            int n_lazy) {
+__device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigned round, int nd, int n_lazy,
+                            int na) {
     const ForceCtx<T> cx = force_ctx(a, F, s);
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
     int* esc_ctr = (int*)&a.esc_cnt[s + 1];
     int* lazy_ctr = &a.lazy_cnt[s + 1];
     const int warp = gtid >> 5, nwarps = gsz >> 5, lane = threadIdx.x & 31;
-    const int nd = has_dirty ? *((volatile int*)&a.dirty_cnt[s]) : 0;
+    const bool has_dirty = nd > 0;
     if (has_dirty && gtid == 0) atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)nd);
     // The special items of this substep: elements whose list this round
     // invalidated (rebuilt, then computed, here; the element loop below skips
@@ -1935,7 +1956,6 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     // Chunks of 32 active elements: every warp starts with one chunk of its own,
     // then takes further chunks from a counter (the next grab is issued before
     // the current chunk is computed), so uneven chunks do not leave warps idle.
-    const int na = *((volatile int*)a.act_cnt);
     const int nw2 = nwarps - skip;
     if (a.force_split == DEM_SPLIT_WARP || (a.force_split == DEM_SPLIT_AUTO && na <= 2 * nw2)) {
         // at most two active elements per warp: a warp per element
@@ -2277,9 +2297,11 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
                 phase_build_all(a);
             } else {
                 // lists to rebuild: this round's marks (escape phase, or the lazy
-                // escapes of the previous substep)
+                // escapes of the previous substep); the counters are read
+                // together, before any branch on them
                 const int nd = *((volatile int*)&a.dirty_cnt[s]);
-                phase_force(a, F, s, round, !all && nd > 0, (cnt == 0u) ? n_lazy : 0);
+                const int na = *((volatile int*)a.act_cnt);
+                phase_force(a, F, s, round, all ? 0 : nd, (cnt == 0u) ? n_lazy : 0, na);
             }
         }
         // a barrier after every phase but the last; with profiling on, after the
