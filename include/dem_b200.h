@@ -238,7 +238,10 @@ int dem_set_launch_mode(DemHandle* h, int32_t mode);
  * DEM_SPLIT_AUTO (a warp per active element when at most two fall to each warp,
  * else a thread per element), DEM_SPLIT_THREAD or DEM_SPLIT_WARP.  mark_split,
  * for the escape rounds: DEM_SPLIT_AUTO (a CTA per escaped element when they fit
- * one per CTA, else a warp each), DEM_SPLIT_CTA or DEM_SPLIT_WARP. */
+ * one per CTA, else a warp each), DEM_SPLIT_CTA or DEM_SPLIT_WARP.  mark_split
+ * also sets the unit of a force phase's list rebuilds and lazy escapes:
+ * DEM_SPLIT_AUTO (a CTA each when they are at most a quarter of the CTAs, else
+ * a warp each), DEM_SPLIT_CTA (a CTA each up to half the CTAs) or DEM_SPLIT_WARP. */
 #define DEM_SPLIT_AUTO 0
 #define DEM_SPLIT_THREAD 1
 #define DEM_SPLIT_CTA 1
