@@ -68,3 +68,53 @@ def test_single_rank_needs_no_process_group():
     assert bench.retry_verdict(0, False, 1, dev) == 0
     assert bench.retry_verdict(3, True, 1, dev) == 1
     assert bench.retry_verdict(4, False, 1, dev) == 2
+
+
+def _ranked_main(rank, world, port, out):
+    """bench.run_ranked, the bench's own rank entry, with a CPU body: each rank
+    times a different replica; rank 0 alone prints the line."""
+    import io
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, ROOT)
+    import bench
+    buf = io.StringIO()
+
+    def body(r, w):
+        secs = bench.max_over_ranks(0.5 * (r + 1), w, torch.device("cpu"))
+        return {"rank": r, "n_gpus": w, "seconds": secs}
+
+    line = bench.run_ranked(body, rank, world, backend="gloo", out=buf)
+    out[rank] = (line, buf.getvalue(), dist.is_initialized())
+
+
+def test_bench_rank_entry_two_gloo_ranks():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_ranked_main, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
+        res = dict(out)
+    assert sorted(res) == [0, 1]
+    for r in range(world):
+        line, printed, still_joined = res[r]
+        assert line["seconds"] == pytest.approx(1.0)  # the slower rank's time on both
+        assert not still_joined  # the group is left
+        assert (printed != "") == (r == 0)  # one JSON line, from rank 0
+    import json
+    assert json.loads(res[0][1]) == {"rank": 0, "n_gpus": 2, "seconds": 1.0}
+
+
+def test_gpus_flag_resolves_world_size():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.resolve_world(1, {}) == (0, 1, False)
+    assert bench.resolve_world(4, {}) == (0, 1, True)  # relaunch under torchrun
+    assert bench.resolve_world(2, {"WORLD_SIZE": "2", "RANK": "1"}) == (1, 2, False)
+    with pytest.raises(SystemExit):
+        bench.resolve_world(8, {"WORLD_SIZE": "1"})  # would time one GPU as eight
+    with pytest.raises(SystemExit):
+        bench.resolve_world(0, {})
+    cmd = bench.torchrun_command(4, 29511, ["--steps", "20"])
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
+    assert cmd[-3].endswith("bench.py") and cmd[-2:] == ["--steps", "20"]
