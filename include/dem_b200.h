@@ -270,6 +270,22 @@ int dem_get_phase_times(DemHandle* h, int64_t* pairs, int32_t max_pairs, int32_t
  * One-shot; DEM_ERR_INVALID in phased mode or for phase < 0. */
 int dem_debug_fail_barrier(DemHandle* h, int32_t phase);
 
+/* Contact-set recording, a parity aid (no reference counterpart).  With
+ * `pairs` not NULL, every later call on this handle records each ice–ice pair
+ * whose contact term a force phase computed — the pairs with overlap > 0 and
+ * distance > 1e-6 (jax_simulation.py:127-131) among each active element's
+ * candidates — as int32 pairs {e, o} seen from the active element e (a pair
+ * of two active elements appears twice, once from each), at most `capacity`
+ * pairs; *count (device uint32, zeroed at the start of every call) gets the
+ * total, which exceeds capacity if pairs were dropped.  After substep s of
+ * frame f of a call, marks[f * n_ice_steps + s] gets the number of pairs
+ * recorded so far (for f * n_ice_steps + s < max_marks), so the pairs of one
+ * substep are pairs[marks[m-1] .. marks[m]).  Records of one substep come in
+ * no fixed order.  All arrays are device arrays owned by the caller;
+ * pairs = NULL turns recording off.  Results of the step are unchanged. */
+int dem_debug_record_contacts(DemHandle* h, int32_t* pairs, int32_t capacity, int32_t* marks, int32_t max_marks,
+                              uint32_t* count);
+
 /* Copy the last error message (NUL-terminated) into buf. */
 int dem_get_error(DemHandle* h, char* buf, size_t len);
 
@@ -337,6 +353,30 @@ int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const i
                       const DemRolloutCostParams* params, const void* masses, const void* vel0,
                       const void* vel1, double* out, void* stream);
 
+/* Per-rollout ice terms after dem_rollout_segment (no reference counterpart
+ * as a whole): for every system q of n_systems, out[q] (Q,2) double =
+ * [hull impulse: the sum over the segment's steps of J_hist[t, q], the
+ * frame's |F_ice_on_ship| dt (J_cumul_incr, jax_simulation.py:692-697), in
+ * step order; bonds broken: the bonds b in [bond_start[q], bond_start[q+1])
+ * with intact0[b] set and intact1[b] clear].  J_hist (H, Q) of `dtype`;
+ * bond_start (Q+1) int32 or NULL (no bond count); intact0 / intact1 (n_bonds)
+ * the segment's input and output bond_intact.  All device arrays. */
+int dem_rollout_ice_terms(int32_t dtype, int32_t n_systems, int32_t horizon, const void* J_hist,
+                          const int32_t* bond_start, const uint8_t* intact0, const uint8_t* intact1, double* out,
+                          void* stream);
+
+/* The planners' rigid-ship rollout (jax_mbd_planner.py:51-122 rolls the
+ * 3-DOF ship out over a static costmap): for each of n_rollouts candidates,
+ * `horizon` steps of the vessel update of dem_rollout_segment (tau = u,
+ * ship_euler_step_jax and the velocity clip, jax_vessel_dynamics.py:54-84,
+ * :233-243) with no ice load.  eta0, nu0 (Q,3); controls (H,Q,3) body-frame
+ * [X, Y, N]; v_water_ship (H,Q,2) or NULL; eta_hist (H,Q,3) gets the poses
+ * after each step, nu_out (Q,3) (or NULL) the final velocity.  Arrays are
+ * device arrays of `dtype`; params supplies dt, D3, M3inv and the clip. */
+int dem_ship_rollout(const DemParams* params, int32_t dtype, int32_t n_rollouts, int32_t horizon, const void* eta0,
+                     const void* nu0, const void* controls, const void* v_water_ship, void* eta_hist, void* nu_out,
+                     void* stream);
+
 /* Largest n accepted by dem_ship_contact_noalloc. */
 #define DEM_CONTACT_NOALLOC_MAX_ELEMENTS 262144
 
@@ -357,9 +397,12 @@ int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const i
  * Scratch: one static device array of 1 MiB + 256 bytes per device (held by
  * every device that loads the library until the process exits), hence the
  * limit n <= DEM_CONTACT_NOALLOC_MAX_ELEMENTS; larger n returns
- * DEM_ERR_CAPACITY before any work.  The first call on a device looks up that
- * array's device address (once per device): make that first call before any
- * stream capture on the device.  Every call on a device shares the array, so
+ * DEM_ERR_CAPACITY before any work.  Every call made outside stream capture
+ * looks up that array's device address on the current device (so a device
+ * reset leaves no stale address); a call inside a capture uses the address
+ * of the last call outside capture on that device, so make one call before
+ * any stream capture on the device, and again after a device reset (a first
+ * call inside a capture returns DEM_ERR_INVALID).  Every call on a device shares the array, so
  * calls that overlap on the GPU (other streams, other host threads) race on
  * it: serialise them.  Returns DEM_ERR_INVALID for bad arguments and
  * DEM_ERR_CUDA if a launch fails. */

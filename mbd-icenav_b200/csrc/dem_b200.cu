@@ -104,6 +104,11 @@ struct DemHandle {
     std::vector<int> sys_start_h;  // (nsys + 1) element offsets
     void* sprow = nullptr;     // (6,) setpoint row of dem_frame_step
     unsigned* bar = nullptr;
+    // contact-set recording (dem_debug_record_contacts; caller-owned device arrays)
+    int2* crec = nullptr;
+    unsigned* crec_cnt = nullptr;
+    int crec_cap = 0, crec_max_marks = 0;
+    int* crec_marks = nullptr;
     int* status = nullptr;
     long long* stats = nullptr;
     int* host_status = nullptr;  // pinned
@@ -428,6 +433,12 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.bar = h->bar;
     a.status = h->status;
     a.stats = h->stats;
+    a.crec = h->crec;
+    a.crec_cnt = h->crec_cnt;
+    a.crec_cap = h->crec_cap;
+    a.crec_marks = h->crec_marks;
+    a.crec_max_marks = h->crec_max_marks;
+    if (h->crec) CUDA_TRY(h, cudaMemsetAsync(h->crec_cnt, 0, sizeof(unsigned), stream));
 
     // per-call scratch reset (the kernel keeps it clean between frames)
     // per-call counters (escapes, rebuilds, work, lazy escapes, barrier, near
@@ -469,6 +480,41 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
         }
     }
     return DEM_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// The planners' rigid-ship rollout (jax_mbd_planner.py:51-122 rolls the
+// 3-DOF ship out alone): per candidate, H steps of the frame step's vessel
+// update driven by its body-frame control with no ice load, exactly the ship
+// part of a dem_rollout_segment frame whose ice exerts nothing.
+template <typename T>
+__global__ void ship_rollout_kernel(const DemParams P, int Q, int H, const T* __restrict__ eta0,
+                                    const T* __restrict__ nu0, const T* __restrict__ u,
+                                    const T* __restrict__ vws, T* __restrict__ eta_hist, T* __restrict__ nu_out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Q) return;
+    T eta[3], nu[3], na[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, ei[3] = {T(0), T(0), T(0)};
+    for (int i = 0; i < 3; ++i) {
+        eta[i] = eta0[3 * q + i];
+        nu[i] = nu0[3 * q + i];
+    }
+    const T zero3[3] = {T(0), T(0), T(0)};
+    const T zero2[2] = {T(0), T(0)};
+    for (int t = 0; t < H; ++t) {
+        T eo[3], no[3], nao[6], eio[3];
+        const T* w = vws ? vws + ((size_t)t * Q + q) * 2 : zero2;
+        dem::ship_step<T>(P, eta, nu, na, ei, zero3, zero3, zero3, w, eo, no, nao, eio, u + ((size_t)t * Q + q) * 3);
+        for (int i = 0; i < 3; ++i) {
+            eta[i] = eo[i];
+            nu[i] = no[i];
+            eta_hist[((size_t)t * Q + q) * 3 + i] = eo[i];
+        }
+    }
+    if (nu_out)
+        for (int i = 0; i < 3; ++i) nu_out[3 * q + i] = nu[i];
 }
 
 }  // namespace
@@ -959,6 +1005,47 @@ int dem_get_error(DemHandle* h, char* buf, size_t len) {
     return DEM_OK;
 }
 
+int dem_ship_rollout(const DemParams* params, int32_t dtype, int32_t n_rollouts, int32_t horizon, const void* eta0,
+                     const void* nu0, const void* controls, const void* v_water_ship, void* eta_hist, void* nu_out,
+                     void* stream) {
+    if (!params || (dtype != DEM_F32 && dtype != DEM_F64) || n_rollouts < 1 || horizon < 1 || !eta0 || !nu0 ||
+        !controls || !eta_hist)
+        return DEM_ERR_INVALID;
+    const int blocks = (n_rollouts + 127) / 128;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == DEM_F32)
+        ship_rollout_kernel<float><<<blocks, 128, 0, st>>>(*params, n_rollouts, horizon, (const float*)eta0,
+                                                           (const float*)nu0, (const float*)controls,
+                                                           (const float*)v_water_ship, (float*)eta_hist,
+                                                           (float*)nu_out);
+    else
+        ship_rollout_kernel<double><<<blocks, 128, 0, st>>>(*params, n_rollouts, horizon, (const double*)eta0,
+                                                            (const double*)nu0, (const double*)controls,
+                                                            (const double*)v_water_ship, (double*)eta_hist,
+                                                            (double*)nu_out);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}
+
+int dem_debug_record_contacts(DemHandle* h, int32_t* pairs, int32_t capacity, int32_t* marks, int32_t max_marks,
+                              uint32_t* count) {
+    if (!h) return DEM_ERR_INVALID;
+    if (!pairs) {
+        h->crec = nullptr;
+        h->crec_cnt = nullptr;
+        h->crec_marks = nullptr;
+        h->crec_cap = h->crec_max_marks = 0;
+        return DEM_OK;
+    }
+    if (capacity < 0 || max_marks < 0 || !count || (max_marks > 0 && !marks))
+        return set_err(h, DEM_ERR_INVALID, "dem_debug_record_contacts: bad arguments");
+    h->crec = reinterpret_cast<int2*>(pairs);
+    h->crec_cnt = count;
+    h->crec_cap = capacity;
+    h->crec_marks = marks;
+    h->crec_max_marks = max_marks;
+    return DEM_OK;
+}
+
 int dem_destroy(DemHandle* h) {
     if (!h) return DEM_OK;
     cudaSetDevice(h->device);
@@ -1205,26 +1292,34 @@ extern "C" int dem_ship_contact_noalloc(int32_t dtype, int32_t n, int32_t max_v,
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return DEM_ERR_CUDA;
     if (dev < 0 || dev >= kNoAllocMaxDevices) return DEM_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    // Outside stream capture the address is looked up again on every call, so
+    // a device reset (which reloads the module at a new address) leaves no
+    // stale pointer; under capture, where the lookup may load the module, the
+    // address of the last call outside capture on this device is used.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return DEM_ERR_CUDA;
     NoAllocDevice d;
     {
-        // once per device, with that device current: the address of this
-        // device's copy of the static scratch array
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
         NoAllocDevice& slot = g_noalloc_dev[dev];
-        if (!slot.scratch) {
+        if (cap == cudaStreamCaptureStatusNone) {
+            // with this device current: the address of its copy of the static scratch array
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_contact_scratch) != cudaSuccess || !p) return DEM_ERR_CUDA;
+            slot.scratch = static_cast<unsigned char*>(p);
+        }
+        if (!slot.scratch) return DEM_ERR_INVALID;  // first call on this device inside a capture
+        if (slot.sm_count == 0) {
             int sm = 0;
             if (cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sm < 1)
                 return DEM_ERR_CUDA;
             slot.sm_count = sm;
-            slot.scratch = static_cast<unsigned char*>(p);
         }
         d = slot;
     }
     double t_samp[dem::kMaxEdgeSamples] = {0};
     np_linspace(1.0 / (n_edge_samples + 1), (double)n_edge_samples / (n_edge_samples + 1), n_edge_samples, t_samp);
-    cudaStream_t st = (cudaStream_t)stream;
     int* near_cnt = reinterpret_cast<int*>(d.scratch);
     int* near_list = reinterpret_cast<int*>(d.scratch + kNoAllocListOffset);
     if (dtype == DEM_F32) {
