@@ -118,7 +118,7 @@ class DemRolloutCostParams(C.Structure):
 EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status",
            "dem_set_capacity", "dem_set_launch_mode", "dem_set_work_split", "dem_get_info", "dem_set_profiling",
            "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap", "dem_rollout_segment",
-           "dem_rollout_costs")
+           "dem_rollout_costs", "dem_debug_record_contacts", "dem_rollout_ice_terms", "dem_ship_rollout")
 
 _LIB = None
 
@@ -157,15 +157,43 @@ def load_library(path: str = None):
     lib.dem_get_error.argtypes = [H, C.c_char_p, C.c_size_t]
     lib.dem_destroy.argtypes = [H]
     lib.dem_debug_fail_barrier.argtypes = [H, _i]
+    lib.dem_debug_record_contacts.argtypes = [H, _vp, _i, _vp, _i, _vp]
+    lib.dem_rollout_ice_terms.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]
+    lib.dem_ship_rollout.argtypes = [C.POINTER(DemParams), _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     lib.dem_ke_costmap.argtypes = [_i, _i, _vp, _vp, _vp, _vp, C.POINTER(DemCostmapParams), _vp, _vp, _vp, _vp]
     lib.dem_rollout_costs.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, C.POINTER(DemRolloutCostParams), _vp,
                                       _vp, _vp, _vp, _vp]
     lib.dem_version.restype = C.c_char_p
+    _bind_surrogate(lib)
     for name in EXPORTS:
         if name != "dem_version":
             getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
+
+
+# surrogate kernels (include/surrogate_b200.h)
+SG_OK, SG_ERR_INVALID, SG_ERR_CUDA = 0, 1, 2
+SG_OUT_F32, SG_OUT_BF16 = 0, 1
+SG_EXPORTS = ("sg_gemm", "sg_im2col", "sg_col2im", "sg_transpose", "sg_colsum", "sg_adam", "sg_mse",
+              "sg_pack_rows", "sg_unpack_grad", "sg_to_bf16", "sg_gather_rows")
+
+
+def _bind_surrogate(lib):
+    f = C.c_float
+    lib.sg_gemm.argtypes = [_i, _i, _i, _vp, _i, _vp, _i, _vp, _i, _i, _vp, _i, _vp, _i, _vp, _vp]
+    lib.sg_im2col.argtypes = [_i, _i, _i, _i, _vp, _i, _vp, _vp]
+    lib.sg_col2im.argtypes = [_i, _i, _i, _i, _vp, _i, _vp, _vp, _vp]
+    lib.sg_transpose.argtypes = [_i, _i, _vp, _i, _vp, _i, _vp]
+    lib.sg_colsum.argtypes = [_i, _i, _vp, _i, _i, _vp, _vp]
+    lib.sg_adam.argtypes = [_i, _i, _vp, _vp, _vp, _vp, f, f, f, f, _i, _vp, _i, _vp, _i, _vp]
+    lib.sg_mse.argtypes = [_i, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp]
+    lib.sg_pack_rows.argtypes = [_i, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp]
+    lib.sg_unpack_grad.argtypes = [_i, _i, _vp, _i, _vp, _vp, _vp]
+    lib.sg_to_bf16.argtypes = [C.c_int64, _vp, _vp, _vp]
+    lib.sg_gather_rows.argtypes = [_i, C.c_int64, _vp, C.c_int64, _vp, _vp, C.c_int64, _vp]
+    for name in SG_EXPORTS:
+        getattr(lib, name).restype = C.c_int
 
 
 class DemError(RuntimeError):

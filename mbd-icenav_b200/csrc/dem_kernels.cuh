@@ -181,6 +181,14 @@ struct KArgs {
     T *h_pos, *h_rot, *h_eta, *h_sub, *h_J, *h_F;
     uint8_t* h_intact;
     unsigned* bar;        // [count, generation]
+    // contact-set recording (parity aid, off when crec is null): every pair
+    // whose contact term a force phase computes goes to crec as {e, o}, seen
+    // from the active element e; crec_marks[f * k_sub + s] = pairs recorded
+    // up to the end of substep s of frame f
+    int2* crec;
+    unsigned* crec_cnt;
+    int crec_cap, crec_max_marks;
+    int* crec_marks;
     int* status;
     long long* stats;     // [rounds, max list, max bucket, re-referenced, lists rebuilt, overflow flags]
 };
@@ -1600,6 +1608,14 @@ __device__ __forceinline__ bool contact_term(const ForceConst<T>& fc, bool h15, 
     return true;
 }
 
+// Contact-set recording (only when a.crec is set): one pair {e, o} whose
+// contact term element e's force computation added.
+template <typename T>
+__device__ __forceinline__ void record_contact(const KArgs<T>& a, int e, int o) {
+    const unsigned i = atomicAdd(a.crec_cnt, 1u);
+    if (i < (unsigned)a.crec_cap) a.crec[i] = make_int2(e, o);
+}
+
 // Escape code of element e at its new position: 2 = escaped past this substep's
 // threshold (processed before the next substep), 1 = lazily escaped (re-referenced
 // during the next force phase), 0 = neither.
@@ -1770,6 +1786,7 @@ __device__ __forceinline__ int force_element(const KArgs<T>& a, const Frame<T>& 
             const bool e_is_i = e < o;
             T tx, ty, hm;
             if (!contact_term(a.fc, h15, ke, ve, ko[j], vo[j], e_is_i, tx, ty, hm)) continue;
+            if (a.crec) record_contact(a, e, o);
             fix += tx;
             fiy += ty;
             mi = e_is_i ? mi + hm : mi - hm;
@@ -1833,6 +1850,7 @@ __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame
         T tx = T(0), ty = T(0), hm = T(0);
         const bool eis = e < o;
         const bool cv = (o >= 0) && contact_term(a.fc, h15, ke, ve, ko, vo, eis, tx, ty, hm);
+        if (cv && a.crec) record_contact(a, e, o);
         const unsigned bm = __ballot_sync(full, bv);
         const unsigned rm = __ballot_sync(full, bv && r.o < 0);
         const unsigned cm = __ballot_sync(full, cv);
@@ -2267,6 +2285,11 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
     for (int ph = ph_lo; ph < ph_hi; ++ph) {
         const int f = ph / per_frame;
         const int p = ph % per_frame;
+        if (a.crec && p >= 7 && (p - 7) % 3 == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+            // the force phase of substep (p - 7) / 3 has ended (barrier or launch boundary)
+            const int m = f * k + (p - 7) / 3;
+            if (m < a.crec_max_marks) a.crec_marks[m] = (int)*((volatile unsigned*)a.crec_cnt);
+        }
         Frame<T> F = make_frame(a, f);
         if (p == 0) {
             phase_cull(a, F);

@@ -209,3 +209,61 @@ extern "C" int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horiz
         return launch_costs<float>(c, system_start, eta0, eta_hist, controls, grid, masses, vel0, vel1, out, st);
     return launch_costs<double>(c, system_start, eta0, eta_hist, controls, grid, masses, vel0, vel1, out, st);
 }
+
+// ════════════════════════════════════════════════════════════════════════════
+// dem_rollout_ice_terms: per rollout, the hull impulse (sum over the steps of
+// the frame's J_cumul_incr = |F_ice_on_ship| dt, jax_simulation.py:692-697)
+// and the bonds its ship broke (intact at the start, broken at the end), one
+// CTA per rollout with fixed-order sums.
+// ════════════════════════════════════════════════════════════════════════════
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(kRcThreads) ice_terms_kernel(int Q, int H, const T* __restrict__ J_hist,
+                                                               const int* __restrict__ bond_start,
+                                                               const uint8_t* __restrict__ intact0,
+                                                               const uint8_t* __restrict__ intact1,
+                                                               double* __restrict__ out) {
+    __shared__ double s_imp[kRcThreads];
+    __shared__ long long s_brk[kRcThreads];
+    const int q = blockIdx.x;
+    double imp = 0.0;
+    for (int t = threadIdx.x; t < H; t += blockDim.x) imp += (double)J_hist[(size_t)t * Q + q];
+    long long brk = 0;
+    if (bond_start) {
+        for (int b = bond_start[q] + threadIdx.x; b < bond_start[q + 1]; b += blockDim.x)
+            brk += (intact0[b] != 0 && intact1[b] == 0) ? 1 : 0;
+    }
+    s_imp[threadIdx.x] = imp;
+    s_brk[threadIdx.x] = brk;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            s_imp[threadIdx.x] += s_imp[threadIdx.x + w];
+            s_brk[threadIdx.x] += s_brk[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * q] = s_imp[0];
+        out[2 * q + 1] = (double)s_brk[0];
+    }
+}
+
+}  // namespace
+
+extern "C" int dem_rollout_ice_terms(int32_t dtype, int32_t n_systems, int32_t horizon, const void* J_hist,
+                                     const int32_t* bond_start, const uint8_t* intact0, const uint8_t* intact1,
+                                     double* out, void* stream) {
+    if ((dtype != DEM_F32 && dtype != DEM_F64) || n_systems < 1 || horizon < 1 || !J_hist || !out)
+        return DEM_ERR_INVALID;
+    if (bond_start && (!intact0 || !intact1)) return DEM_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == DEM_F32)
+        ice_terms_kernel<float><<<n_systems, kRcThreads, 0, st>>>(n_systems, horizon, (const float*)J_hist, bond_start,
+                                                                  intact0, intact1, out);
+    else
+        ice_terms_kernel<double><<<n_systems, kRcThreads, 0, st>>>(n_systems, horizon, (const double*)J_hist,
+                                                                   bond_start, intact0, intact1, out);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}

@@ -239,6 +239,20 @@ class FrameStep:
         self._check(self.lib.dem_get_phase_times(self._h, buf, 4096, C.byref(cnt), C.byref(t0)))
         return [(int(buf[2 * i]), int(buf[2 * i + 1]) - int(t0.value)) for i in range(cnt.value)]
 
+    def record_contacts(self, capacity: int = 1 << 20, max_marks: int = 4096) -> "ContactRecorder":
+        """Record the ice-ice contact set of every later call (``dem_debug_record_contacts``):
+        the pairs whose contact term each substep's force phase computed.  Returns
+        the recorder; ``stop_recording`` turns it off."""
+        rec = ContactRecorder(self.device, capacity, max_marks)
+        self._check(self.lib.dem_debug_record_contacts(self._h, _ptr(rec.pairs), capacity, _ptr(rec.marks),
+                                                       max_marks, _ptr(rec.count)))
+        self._recorder = rec
+        return rec
+
+    def stop_recording(self):
+        self._check(self.lib.dem_debug_record_contacts(self._h, None, 0, None, 0, None))
+        self._recorder = None
+
     def close(self):
         if getattr(self, "_h", None):
             self.lib.dem_destroy(self._h)
@@ -412,6 +426,35 @@ class FrameStep:
         self._run(fn, C.byref(cin), C.byref(cout), C.byref(sin), C.byref(sout), K, _ptr(sp), _ptr(vw), _ptr(vws),
                   C.byref(chist) if chist is not None else None, self._stream(), check=check)
         return out, sh_out, hist
+
+
+class ContactRecorder:
+    """Device buffers of ``dem_debug_record_contacts`` and their readout."""
+
+    def __init__(self, device, capacity: int, max_marks: int):
+        torch = _tm()
+        self.pairs = torch.zeros((max(capacity, 1), 2), dtype=torch.int32, device=device)
+        self.marks = torch.zeros(max(max_marks, 1), dtype=torch.int32, device=device)
+        self.count = torch.zeros(1, dtype=torch.int32, device=device)  # read as uint32
+        self.capacity = capacity
+
+    def substeps(self, n_substeps: int):
+        """Pairs of each substep of the last call, as (i < j) sets: a list of
+        ``n_substeps`` sets of tuples, and the raw {e, o} records per substep."""
+        _tm().cuda.synchronize()
+        total = int(self.count.item()) & 0xFFFFFFFF
+        if total > self.capacity:
+            raise RuntimeError(f"contact recorder overflow: {total} pairs > capacity {self.capacity}")
+        marks = self.marks[:n_substeps].cpu().numpy().astype(np.int64)
+        pairs = self.pairs[:total].cpu().numpy().astype(np.int64)
+        sets, raw = [], []
+        lo = 0
+        for m in marks:
+            p = pairs[lo:m]
+            raw.append(p)
+            sets.append(set(zip(np.minimum(p[:, 0], p[:, 1]).tolist(), np.maximum(p[:, 0], p[:, 1]).tolist())))
+            lo = int(m)
+        return sets, raw
 
 
 def make_frame_step(static, cfg, ship_dyn, ship_length, ship_beam, n_ice_steps, dt, dt_ice,

@@ -175,6 +175,9 @@ class Oracle:
         self.B_mat = f(B_mat)
         self.pair_mode = pair_mode
         self.pair_margin = float(pair_margin)
+        # when a list: each substep appends its contact set, the pairs (i < j)
+        # with overlap > 0 and distance > 1e-6 (jax_simulation.py:127-131)
+        self.contact_log = None
         if pair_mode == "all":
             n = self.n
             self._all_i = np.repeat(np.arange(n), np.arange(n - 1, -1, -1))
@@ -261,8 +264,13 @@ class Oracle:
         moments = np.zeros(n, dt)
         pi, pj = pairs if pairs is not None else self.candidate_pairs(st.positions)
         if len(pi) == 0:
+            if self.contact_log is not None:
+                self.contact_log.append(set())
             return forces, moments
-        _, _, f_n, f_t, cross = self.contact_terms(st.positions, st.velocities, pi, pj)
+        _, overlap, f_n, f_t, cross = self.contact_terms(st.positions, st.velocities, pi, pj)
+        if self.contact_log is not None:
+            has = overlap > 0.0
+            self.contact_log.append(set(zip(pi[has].tolist(), pj[has].tolist())))
         np.add.at(forces, pi, -f_n + f_t)
         np.add.at(forces, pj, f_n - f_t)
         np.add.at(moments, pi, 0.5 * cross)

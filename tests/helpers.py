@@ -157,3 +157,103 @@ def to_np_state(st, ship):
     ice = OState(*[t.detach().cpu().numpy() for t in st])
     sh = OShip(*[t.detach().cpu().numpy() for t in ship])
     return ice, sh
+
+
+# ── per-element step comparison (fp32 parity at the stated tolerance) ───────
+
+STEP_REL = 1e-5  # per-step relative tolerance in fp32 (positions, velocities, forces, state)
+STEP_ULPS = 4    # absolute floor: this many fp32 rounding units of the quantity itself
+
+
+def ulp32(x):
+    """fp32 rounding unit (spacing) of |x|, as float64."""
+    return np.spacing(np.abs(np.asarray(x, np.float64)).astype(np.float32)).astype(np.float64)
+
+
+def step_ratio(got, want, before, rel=STEP_REL, ulps=STEP_ULPS):
+    """Per entry (per row for (m, 2) arrays): |got - want| / (rel |want - before| +
+    ulps ulp32(max(|want|, |before|))), the error against the step's own change
+    with a floor at fp32 rounding of the values.  Returns the array of ratios
+    (<= 1 passes) — 0 where both agree exactly."""
+    g = np.asarray(got, np.float64)
+    w = np.asarray(want, np.float64)
+    b = np.asarray(before, np.float64)
+    mag = np.maximum(np.abs(w), np.abs(b))
+    if g.ndim == 2:
+        err = np.sqrt(((g - w) ** 2).sum(1))
+        change = np.sqrt(((w - b) ** 2).sum(1))
+        floor = ulps * ulp32(mag.max(1))
+    else:
+        err = np.abs(g - w)
+        change = np.abs(w - b)
+        floor = ulps * ulp32(mag)
+    both_nan = np.isnan(g) & np.isnan(w)
+    if g.ndim == 2:
+        both_nan = both_nan.all(1)
+    err = np.where(both_nan, 0.0, err)
+    return err / (rel * change + floor)
+
+
+def assert_step_close(name, got, want, before, rel=STEP_REL, ulps=STEP_ULPS):
+    """Every entry within ``rel`` of its own step change (floor: fp32 rounding)."""
+    r = step_ratio(got, want, before, rel, ulps)
+    if r.size and not (np.nanmax(r) <= 1.0):
+        i = int(np.nanargmax(r))
+        raise AssertionError(f"{name}: entry {i} off by {np.nanmax(r):.3g}x the tolerance "
+                             f"(got {np.asarray(got)[i]}, want {np.asarray(want)[i]}, "
+                             f"before {np.asarray(before)[i]}); {int((r > 1).sum())} entries out")
+    return float(np.nanmax(r)) if r.size else 0.0
+
+
+ICE_FLOAT_FIELDS = ("positions", "velocities", "rotations", "angular_vels", "submergence", "bond_damage",
+                    "bond_delta_m_0", "bond_delta_m_max", "bond_delta_s")
+ICE_MASK_FIELDS = ("bond_intact", "elem_active", "dpdem_floe_eligible")
+SHIP_FIELDS = ("eta", "nu", "n_actual", "e_int")
+
+
+def assert_frame_matches(ice, ship, o_ice, o_ship, in_ice, in_ship, diag=None, o_diag=None, where=""):
+    """One frame from identical inputs, GPU vs oracle: every IceState and
+    ShipState field (masks bit-equal; floats per entry within the step
+    tolerance), and the diagnostics (contact mask, force magnitudes, ship
+    force).  Returns the worst ratio per field."""
+    worst = {}
+    for f in ICE_MASK_FIELDS:
+        np.testing.assert_array_equal(getattr(ice, f), getattr(o_ice, f), err_msg=f"{f} {where}")
+    for f in ICE_FLOAT_FIELDS:
+        worst[f] = assert_step_close(f"{f} {where}", getattr(ice, f), getattr(o_ice, f), getattr(in_ice, f))
+    for f in SHIP_FIELDS:
+        worst[f] = assert_step_close(f"ship {f} {where}", getattr(ship, f), getattr(o_ship, f),
+                                     getattr(in_ship, f))
+    if diag is not None:
+        gp = diag["pen_max"].detach().cpu().numpy()
+        np.testing.assert_array_equal(gp > 0, o_diag["pen_max"] > 0, err_msg=f"contact mask {where}")
+        z = np.zeros_like(o_diag["force_mag"])
+        worst["force_mag"] = assert_step_close(f"force_mag {where}", diag["force_mag"].detach().cpu().numpy(),
+                                               o_diag["force_mag"], z)
+        worst["pen_max"] = assert_step_close(f"pen_max {where}", gp, o_diag["pen_max"], np.zeros_like(gp))
+        worst["F_ice_on_ship"] = assert_step_close(f"F_ice_on_ship {where}",
+                                                   diag["F_ice_on_ship"].detach().cpu().numpy()[None],
+                                                   np.asarray(o_diag["F_ice_on_ship"])[None],
+                                                   np.zeros((1, 2)))
+    return worst
+
+
+def contact_sets_match(sets, raw, o_sets, active, where=""):
+    """GPU contact sets (per substep, recorded from active elements) against
+    the oracle's (all pairs): equal on the pairs with an active end, and every
+    pair of two active elements recorded from both ends."""
+    assert len(sets) == len(o_sets), (len(sets), len(o_sets))
+    total = 0
+    for s, (g, o, r) in enumerate(zip(sets, o_sets, raw)):
+        o_act = {(i, j) for i, j in o if active[i] or active[j]}
+        missing, extra = o_act - g, g - o_act
+        assert not missing and not extra, (f"substep {s} {where}: {len(missing)} contacts missing "
+                                           f"(e.g. {sorted(missing)[:3]}), {len(extra)} extra "
+                                           f"(e.g. {sorted(extra)[:3]})")
+        both = {(i, j) for i, j in g if active[i] and active[j]}
+        seen = set(map(tuple, r.tolist()))
+        for i, j in both:
+            assert (i, j) in seen and (j, i) in seen, f"substep {s} {where}: pair {(i, j)} recorded from one end"
+        assert len(r) == len(g) + len(both), f"substep {s} {where}: repeated records"
+        total += len(g)
+    return total
