@@ -19,9 +19,9 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB_NAME = "libdem_b200.so"
 LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
 
-SOURCES = [os.path.join(CSRC, f) for f in ("dem_b200.cu", "dem_costmap.cu", "dem_rollout.cu")]
-DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("dem_kernels.cuh", "dem_math.cuh")] + [
-    os.path.join(INCLUDE, "dem_b200.h")]
+SOURCES = [os.path.join(CSRC, f) for f in ("dem_b200.cu", "dem_costmap.cu", "dem_rollout.cu", "sg_kernels.cu")]
+DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("dem_kernels.cuh", "dem_math.cuh", "sg_tc.cuh")] + [
+    os.path.join(INCLUDE, f) for f in ("dem_b200.h", "surrogate_b200.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

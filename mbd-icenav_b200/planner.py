@@ -1,0 +1,587 @@
+"""Model-based-diffusion planning with the DEM in the loop, plain and
+surrogate-screened.
+
+``mbd_plan`` mirrors the reference's ``run_mbd`` (``jax_mbd_planner.py:
+1314-1411``): a mean action sequence Ybar (H, 2) in normalised action space
+(surge force, yaw moment) is refined over ``n_diffuse - 1`` reverse diffusion
+steps; each step draws ``n_sample`` candidates Y0 = clip(Ybar + sigma_i eps),
+scores them with a cost batch, and moves Ybar to the softmax(-cost / T)
+weighted mean through the same score update.  Sway is held at zero (the
+surrogate's controls are (surge, yaw) per step).
+
+Two cost batches:
+
+* ``DemScorer`` — every candidate rolled out by the DEM (``dem_rollout_segment``,
+  one system per candidate, each its own copy of the ice window around the
+  start) and scored on the device: the reference planner's cost components
+  (``dem_rollout_costs``) plus the ice terms only the DEM gives (kinetic energy
+  transferred, hull impulse, bonds broken; ``dem_rollout_ice_terms``);
+* ``ScreenedScorer`` — the rigid-ship rollout (``dem_ship_rollout``) for the
+  planner's components plus the surrogate's prediction of the ice terms for
+  every candidate; the ``top_k`` best are then re-scored by the DEM and those
+  exact costs replace the predictions.  When the prediction error on them
+  (mean relative error of the total cost) exceeds ``max_rel_err``, the step
+  falls back to scoring every candidate with the DEM.
+
+The reference has no DEM rollout and no surrogate; its planners score
+rigid-ship rollouts on a static costmap.  Torch tensors hold the device
+buffers; the planner's bookkeeping (sampling, softmax, weighted mean) uses
+torch tensor ops as the reference uses jnp.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field as dc_field
+from types import SimpleNamespace
+from typing import List, Optional
+
+import numpy as np
+
+from . import _abi, rollouts, sg_ops, sim
+from . import surrogate as S
+from .config import DEFAULT_MATERIAL
+
+_torch = None
+
+
+def _tm():
+    global _torch
+    if _torch is None:
+        import torch
+        _torch = torch
+    return _torch
+
+
+# ─── cost ───────────────────────────────────────────────────────────────────
+@dataclass
+class CostWeights:
+    """J = costmap / normalizer * w_costmap + w_length * length + w_goal * goal
+    + w_jerk * jerk (the reference's weighted components, jax_mbd_planner.py:
+    668-717, with its planner defaults) + the DEM's ice terms."""
+    w_costmap: float = 1.0
+    costmap_normalizer: float = 1.0
+    w_length: float = 0.0
+    w_goal: float = 0.0
+    w_jerk: float = 0.0
+    w_ke: float = 1e-3       # per J of kinetic energy transferred to the ice
+    w_impulse: float = 1e-4  # per N s of hull impulse
+    w_bonds: float = 1.0     # per bond broken
+
+    def planner(self):
+        return (self.w_costmap / self.costmap_normalizer, self.w_length, self.w_goal, self.w_jerk)
+
+    def ice(self):
+        return (self.w_ke, self.w_impulse, self.w_bonds)
+
+
+@dataclass
+class MBDConfig:
+    horizon: int = 64
+    n_sample: int = 8192
+    n_diffuse: int = 17          # 16 reverse steps
+    temperature: float = 0.01    # config.py planning_jax_mbd_temperature
+    beta0: float = 1e-5
+    betaT: float = 0.05
+    init_surge_bias: float = 0.7
+    top_k: int = 64
+    max_rel_err: float = 0.05
+
+
+# ─── the scene a plan starts from ───────────────────────────────────────────
+@dataclass
+class PlanScene:
+    field: object
+    static: object           # NumPy static arrays of the whole field
+    ship_dyn: object         # NumPy ship dynamics arrays
+    eta0: np.ndarray
+    nu0: np.ndarray
+    window: np.ndarray       # field element indices within reach of every candidate
+    costmap: object          # JaxCostMapResult, device grid, centred on the start
+    patch: object            # (1, 64, 64, 1) bf16 normalised costmap patch around the start
+    goal: np.ndarray
+    params: object           # DemParams (vessel constants for the rigid rollout)
+    dtype: object
+    device: object
+
+
+PATCH_CELLS = S.PATCH
+COSTMAP_CELLS = 256
+RESOLUTION = 2.0
+
+
+def reach_radius(field, horizon: int, dt: float, v_max: float = 5.0) -> float:
+    """Distance from the start within which any candidate's hull can touch ice."""
+    return math.hypot(0.5 * field.ship_length, 0.5 * field.ship_beam) + v_max * horizon * dt + 5.0
+
+
+def make_scene(field, eta0, nu0=(2.0, 0.0, 0.0), horizon: int = 64, dtype=None, device="cuda",
+               patch_stats=(0.0, 1.0), static=None, ship_dyn=None) -> PlanScene:
+    torch = _tm()
+    from .config import get_default_simulation_config
+    from .costmap import build_costmap_jax
+    from .state import build_static_arrays, ship_dynamics_arrays
+    from .vessel import SupplyVessel
+    cfg = get_default_simulation_config()
+    dev = torch.device(device)
+    dtype = dtype or torch.float32
+    if static is None:
+        static = build_static_arrays(field.polygons, field.centroids, field.bonds, field.thicknesses,
+                                     field.parent_ids, cfg, DEFAULT_MATERIAL, 0.05)
+    if ship_dyn is None:
+        ship_dyn = ship_dynamics_arrays(field.ship_props, cfg, field.ship_length, field.ship_beam, field.hull_local)
+    eta0 = np.asarray(eta0, np.float64)
+    nu0 = np.asarray(nu0, np.float64)
+    R = reach_radius(field, horizon, field.dt)
+    d = np.linalg.norm(np.asarray(field.centroids, np.float64) - eta0[:2], axis=1)
+    window = np.nonzero(d < R)[0]
+    half = 0.5 * COSTMAP_CELLS * RESOLUTION - 20.0  # 256 cells with the builder's 20 m margin
+    cm, _ = build_costmap_jax(field.centroids, field.thicknesses, static.radii, eta0[0] - half, eta0[0] + half,
+                              eta0[1] - half, eta0[1] + half, resolution=RESOLUTION, ship_length=field.ship_length,
+                              ship_beam=field.ship_beam, masses=static.masses, device=dev, download=False)
+    c0 = (COSTMAP_CELLS - PATCH_CELLS) // 2
+    mean, std = patch_stats
+    patch32 = ((cm.grid[c0:c0 + PATCH_CELLS, c0:c0 + PATCH_CELLS] - mean) / std).contiguous()
+    patch = sg_ops.to_bf16(patch32).view(1, PATCH_CELLS, PATCH_CELLS, 1)
+    sv = SupplyVessel(mass=field.ship_props.mass, length=field.ship_length)
+    P = sim.build_params(cfg, ship_dyn, field.ship_length, field.ship_beam, field.n_ice_steps, field.dt,
+                         field.dt / field.n_ice_steps, False, sv.B, sv.T_n)
+    goal = eta0[:2] + 200.0 * np.array([math.cos(eta0[2]), math.sin(eta0[2])])
+    return PlanScene(field, static, ship_dyn, eta0, nu0, window, cm, patch, goal, P, dtype, dev)
+
+
+def shared_window_batch(scene: PlanScene, Q: int, **frame_kw) -> rollouts.RolloutBatch:
+    """Q systems, each its own copy of the scene's window (the candidates of one plan)."""
+    torch = _tm()
+    from .state import IceState, ShipState
+    from .vessel import SupplyVessel
+    from .config import get_default_simulation_config
+    f = scene.field
+    st = scene.static
+    w = np.asarray(scene.window, np.int64)
+    n_w = len(w)
+    local = -np.ones(st.masses.shape[0], np.int64)
+    local[w] = np.arange(n_w)
+    bi, bj = np.asarray(st.bond_i, np.int64), np.asarray(st.bond_j, np.int64)
+    keep = (local[bi] >= 0) & (local[bj] >= 0)
+    nb_w = int(keep.sum())
+    _, floe = np.unique(np.asarray(st.initial_floe_of)[w], return_inverse=True)
+    nf_w = int(floe.max()) + 1 if n_w else 0
+    tile = lambda a: np.concatenate([np.asarray(a)] * Q, axis=0)
+    bs = SimpleNamespace()
+    for k in rollouts._STATIC_ELEM:
+        setattr(bs, k, tile(np.asarray(getattr(st, k))[w]))
+    for k in rollouts._STATIC_BOND:
+        setattr(bs, k, tile(np.asarray(getattr(st, k))[keep]))
+    offs_e = (np.arange(Q, dtype=np.int64) * n_w)[:, None]
+    bs.bond_i = (local[bi[keep]][None, :] + offs_e).reshape(-1).astype(np.int32)
+    bs.bond_j = (local[bj[keep]][None, :] + offs_e).reshape(-1).astype(np.int32)
+    bs.initial_floe_of = (floe[None, :] + (np.arange(Q) * nf_w)[:, None]).reshape(-1).astype(np.int32)
+    bs.k_n, bs.k_s = float(st.k_n), float(st.k_s)
+    bs.pair_i = bs.pair_j = None
+    sys_start = np.arange(Q + 1, dtype=np.int64) * n_w
+    cfg = get_default_simulation_config()
+    sv = SupplyVessel(mass=f.ship_props.mass, length=f.ship_length)
+    sd_dev = rollouts.sim_ship_dyn(scene.ship_dyn, scene.dtype, scene.device)
+    fs = sim.make_frame_step(bs, cfg, sd_dev, f.ship_length, f.ship_beam, f.n_ice_steps, f.dt,
+                             f.dt / f.n_ice_steps, False, sv.B, sv.T_n, device=scene.device, dtype=scene.dtype,
+                             system_start=sys_start if Q > 1 else None, **frame_kw)
+    dev, d = fs.device, fs.dtype
+    n, nb, nf = fs.n, fs.n_bonds, fs.n_floes
+    pos = torch.as_tensor(np.asarray(f.centroids, np.float64)[w], dtype=d, device=dev).repeat(Q, 1)
+    z = lambda *s: torch.zeros(s, dtype=d, device=dev)
+    state = IceState(positions=pos, velocities=z(n, 2), rotations=z(n), angular_vels=z(n), submergence=z(n),
+                     bond_intact=torch.ones(nb, dtype=torch.bool, device=dev), bond_damage=z(nb),
+                     bond_delta_m_0=z(nb), bond_delta_m_max=z(nb), bond_delta_s=z(nb),
+                     elem_active=torch.zeros(n, dtype=torch.bool, device=dev),
+                     dpdem_floe_eligible=torch.zeros(nf, dtype=torch.bool, device=dev))
+    tq = lambda v: torch.as_tensor(np.tile(np.asarray(v, np.float64), (Q, 1)), dtype=d, device=dev)
+    ship = ShipState(eta=tq(scene.eta0), nu=tq(scene.nu0), n_actual=z(Q, 6), e_int=z(Q, 3))
+    if Q == 1:
+        ship = ShipState(*[t[0] for t in ship])
+    batch = rollouts.RolloutBatch(fs, [w] * Q, sys_start, torch.as_tensor(sys_start, dtype=torch.int32, device=dev),
+                                  state, ship)
+    batch.bond_start = torch.as_tensor(np.arange(Q + 1) * nb_w, dtype=torch.int32, device=dev)
+    return batch
+
+
+# ─── controls and features ──────────────────────────────────────────────────
+def physical_controls(Yn):
+    """(Q, H, 2) normalised (surge, yaw) in [-1, 1] -> (H, Q, 3) body-frame [X, 0, N]."""
+    torch = _tm()
+    c, s = rollouts.ACTION_CENTER, rollouts.ACTION_SCALE
+    X = c[0] + s[0] * Yn[..., 0]
+    N = c[2] + s[2] * Yn[..., 1]
+    return torch.stack([X, torch.zeros_like(X), N], -1).transpose(0, 1).contiguous()
+
+
+def features(scene: PlanScene, Yn):
+    """(Q, 6 + 2H) fp32 network inputs besides the patch: ship state [u/5, v/2,
+    r/0.1, cos psi, sin psi, 0] and the normalised controls, step by step."""
+    torch = _tm()
+    Q, H, _ = Yn.shape
+    e, v = scene.eta0, scene.nu0
+    ship = torch.tensor([v[0] / 5.0, v[1] / 2.0, v[2] / 0.1, math.cos(e[2]), math.sin(e[2]), 0.0],
+                        dtype=torch.float32, device=Yn.device)
+    return torch.cat([ship.expand(Q, S.N_SHIP), Yn.reshape(Q, 2 * H).float()], 1).contiguous()
+
+
+# ─── target transforms ──────────────────────────────────────────────────────
+TARGET_SCALE = (1e3, 1e3, 1.0)  # J, N s, bonds: log1p(x / scale) before standardising
+
+
+@dataclass
+class TargetStats:
+    mean: np.ndarray
+    std: np.ndarray
+
+    def forward(self, raw):
+        """raw (Q, 3) -> standardised log1p targets (torch, fp32)."""
+        torch = _tm()
+        sc = torch.tensor(TARGET_SCALE, dtype=torch.float64, device=raw.device)
+        t = torch.log1p(torch.clamp(raw.double(), min=0.0) / sc)
+        m = torch.as_tensor(self.mean, device=raw.device)
+        s = torch.as_tensor(self.std, device=raw.device)
+        return ((t - m) / s).float()
+
+    def inverse(self, pred):
+        torch = _tm()
+        sc = torch.tensor(TARGET_SCALE, dtype=torch.float64, device=pred.device)
+        m = torch.as_tensor(self.mean, device=pred.device)
+        s = torch.as_tensor(self.std, device=pred.device)
+        return torch.clamp(torch.expm1(pred.double() * s + m), min=0.0) * sc
+
+
+# ─── scorers ────────────────────────────────────────────────────────────────
+class DemScorer:
+    """Every candidate through the batched DEM."""
+
+    def __init__(self, scene: PlanScene, Q: int, weights: CostWeights, **frame_kw):
+        self.scene = scene
+        self.Q = Q
+        self.w = weights
+        self.batch = shared_window_batch(scene, Q, **frame_kw)
+        torch = _tm()
+        self.cost_out = torch.empty((Q, 5), dtype=torch.float64, device=scene.device)
+        self.ice_out = torch.empty((Q, 2), dtype=torch.float64, device=scene.device)
+        self.rollouts = 0
+
+    def terms(self, Yn):
+        """(Q, 7) float64: [costmap, length, goal, jerk, KE, impulse, bonds] of the candidates."""
+        torch = _tm()
+        sc = self.scene
+        u = physical_controls(Yn).to(sc.dtype)
+        res = rollouts.run(self.batch, u, history="ship", check=True)
+        comp = rollouts.costs(self.batch, res, sc.costmap, sc.goal, sc.field.ship_length, sc.field.ship_beam,
+                              out=self.cost_out)
+        fs = self.batch.frame_step
+        H = int(u.shape[0])
+        rc = fs.lib.dem_rollout_ice_terms(_abi.DEM_F64 if fs.dtype == torch.float64 else _abi.DEM_F32, self.Q, H,
+                                          res.history[5].data_ptr(), self.batch.bond_start.data_ptr(),
+                                          self.batch.state.bond_intact.data_ptr(),
+                                          res.state.bond_intact.data_ptr(), self.ice_out.data_ptr(),
+                                          fs._stream())
+        if rc != _abi.DEM_OK:
+            raise _abi.DemError(rc, "dem_rollout_ice_terms failed")
+        self.rollouts += self.Q
+        return torch.cat([comp[:, :4], comp[:, 4:5], self.ice_out], 1)
+
+    def total(self, terms):
+        torch = _tm()
+        w = torch.tensor(self.w.planner() + self.w.ice(), dtype=torch.float64, device=terms.device)
+        return terms @ w
+
+    def __call__(self, Yn):
+        return self.total(self.terms(Yn))
+
+
+class Surrogate:
+    """A trained ``SurrogateNet`` with its input and target normalisation."""
+
+    def __init__(self, net: S.SurrogateNet, stats: TargetStats, patch_stats=(0.0, 1.0)):
+        self.net = net
+        self.stats = stats
+        self.patch_stats = patch_stats
+
+    def predict(self, scene: PlanScene, Yn):
+        """(Q, 3) float64 predicted ice terms [KE, impulse, bonds] of the candidates."""
+        torch = _tm()
+        Q = int(Yn.shape[0])
+        enc = self.net.encode(scene.patch, tag="plan_enc")
+        rows = self.net._buf("plan_rows", (Q,), torch.int32)
+        rows.zero_()
+        out = self.net.head(enc, features(scene, Yn), enc_row=rows, tag="plan_head")
+        return self.stats.inverse(out[:, :S.N_OUT])
+
+
+def rigid_terms(scene: PlanScene, Yn, out=None):
+    """(Q, 4) float64 planner components of the rigid-ship paths (``dem_ship_rollout``)."""
+    torch = _tm()
+    lib = _abi.load_library()
+    Q, H, _ = Yn.shape
+    d = scene.dtype
+    u = physical_controls(Yn).to(d)
+    eta0 = torch.as_tensor(np.tile(scene.eta0, (Q, 1)), dtype=d, device=scene.device)
+    nu0 = torch.as_tensor(np.tile(scene.nu0, (Q, 1)), dtype=d, device=scene.device)
+    hist = torch.empty((H, Q, 3), dtype=d, device=scene.device)
+    import ctypes as C
+    rc = lib.dem_ship_rollout(C.byref(scene.params), _abi.DEM_F64 if d == torch.float64 else _abi.DEM_F32, Q, H,
+                              eta0.data_ptr(), nu0.data_ptr(), u.data_ptr(), None, hist.data_ptr(), None,
+                              C.c_void_p(torch.cuda.current_stream(scene.device).cuda_stream))
+    if rc != _abi.DEM_OK:
+        raise _abi.DemError(rc, "dem_ship_rollout failed")
+    comp = rollouts.path_costs(eta0, hist, u, scene.costmap, scene.goal, scene.field.ship_length,
+                               scene.field.ship_beam, out=out)
+    return comp[:, :4]
+
+
+class ScreenedScorer:
+    """Surrogate predictions for every candidate, the DEM for the best ``top_k``."""
+
+    def __init__(self, scene: PlanScene, surrogate: Surrogate, Q: int, weights: CostWeights, top_k: int = 64,
+                 max_rel_err: float = 0.05, **frame_kw):
+        self.scene = scene
+        self.sur = surrogate
+        self.w = weights
+        self.Q = Q
+        self.k = top_k
+        self.max_rel_err = max_rel_err
+        self.dem_k = DemScorer(scene, top_k, weights, **frame_kw)
+        self.dem_all = None
+        self.frame_kw = frame_kw
+        self.fallbacks = 0
+        self.rel_errs: List[float] = []
+        self.rollouts = 0
+
+    def __call__(self, Yn):
+        torch = _tm()
+        planner = rigid_terms(self.scene, Yn)
+        ice = self.sur.predict(self.scene, Yn)
+        wp = torch.tensor(self.w.planner(), dtype=torch.float64, device=Yn.device)
+        wi = torch.tensor(self.w.ice(), dtype=torch.float64, device=Yn.device)
+        pred = planner @ wp + ice @ wi
+        top = torch.topk(pred, self.k, largest=False).indices
+        exact = self.dem_k(Yn[top].contiguous())
+        rel = float(((pred[top] - exact).abs() / exact.abs().clamp(min=1e-9)).mean().item())
+        self.rel_errs.append(rel)
+        self.rollouts += self.k
+        if rel > self.max_rel_err:
+            # the surrogate is off on this population: the plain DEM scores all of it
+            if self.dem_all is None:
+                self.dem_all = DemScorer(self.scene, self.Q, self.w, **self.frame_kw)
+            self.fallbacks += 1
+            self.rollouts += self.Q
+            return self.dem_all(Yn)
+        cost = pred.clone()
+        cost[top] = exact
+        return cost
+
+
+# ─── MBD (jax_mbd_planner.py:1314-1411) ─────────────────────────────────────
+def mbd_plan(scorer, cfg: MBDConfig, device, seed: int = 0, Ybar_init=None):
+    """Reverse diffusion in normalised (surge, yaw) action space; returns
+    (Ybar (H, 2), per-step [mean cost, min cost])."""
+    torch = _tm()
+    H, Ns = cfg.horizon, cfg.n_sample
+    if Ybar_init is None:
+        Ybar = torch.zeros((H, 2), dtype=torch.float32, device=device)
+        Ybar[:, 0] = cfg.init_surge_bias
+    else:
+        Ybar = torch.clamp(torch.as_tensor(Ybar_init, dtype=torch.float32, device=device), -1.0, 1.0)
+    if cfg.n_diffuse <= 1:
+        return Ybar, []
+    betas = torch.linspace(cfg.beta0, cfg.betaT, cfg.n_diffuse, dtype=torch.float32, device=device)
+    alphas = 1.0 - betas
+    alphas_bar = torch.cumprod(alphas, 0)
+    sigmas = torch.sqrt(1.0 - alphas_bar)
+    gen = torch.Generator(device=device).manual_seed(seed)
+    metrics = []
+    i = cfg.n_diffuse - 1
+    for _ in range(cfg.n_diffuse - 1):
+        Yi = Ybar * torch.sqrt(alphas_bar[i])
+        eps = torch.randn((Ns, H, 2), generator=gen, dtype=torch.float32, device=device)
+        Y0s = torch.clamp(eps * sigmas[i] + Ybar, -1.0, 1.0)
+        costs = scorer(Y0s).float()
+        rews = -costs
+        logp0 = (rews - rews.max()) / cfg.temperature
+        weights = torch.softmax(logp0, 0)
+        Ybar_new = torch.einsum("n,nij->ij", weights, Y0s)
+        score = 1.0 / (1.0 - alphas_bar[i]) * (-Yi + torch.sqrt(alphas_bar[i]) * Ybar_new)
+        Yim1 = 1.0 / torch.sqrt(alphas[i]) * (Yi + (1.0 - alphas_bar[i]) * score)
+        i_prev = max(i - 1, 0)
+        Ybar = torch.clamp(Yim1 / torch.sqrt(alphas_bar[i_prev]), -1.0, 1.0)
+        metrics.append((costs.mean(), costs.min()))
+        i -= 1
+    return Ybar, [(float(a), float(b)) for a, b in metrics]
+
+
+def plan_cost(scene: PlanScene, Ybar, dem: DemScorer) -> float:
+    """The DEM cost of executing a plan (every system of ``dem`` runs it; the first is read)."""
+    Y = Ybar.unsqueeze(0).expand(dem.Q, -1, -1).contiguous()
+    return float(dem(Y)[0].item())
+
+
+# ─── training data: DEM rollouts from the batched-rollout generator ─────────
+def sample_starts(field, n: int, rng, horizon: int = 64, clearance: float = 2.0):
+    """Start poses in open water among the floes: heading along the field's
+    track +- 0.3 rad, no element within the hull box plus ``clearance``, and
+    ice within reach of the bow (a window of at least 20 elements)."""
+    cents = np.asarray(field.centroids, np.float64)
+    x0, x1, y0, y1 = field.domain
+    L, B = field.ship_length, field.ship_beam
+    R = reach_radius(field, horizon, field.dt)
+    from scipy.spatial import cKDTree
+    tree = cKDTree(cents)
+    out = []
+    tries = 0
+    base = float(field.trajectory[0][2])
+    while len(out) < n and tries < 200000:
+        tries += 1
+        x, y = rng.uniform(x0 + 20, x1 - 20), rng.uniform(y0 + 20, y1 - 20)
+        psi = base + rng.uniform(-0.3, 0.3)
+        c, s = math.cos(psi), math.sin(psi)
+        near = tree.query_ball_point([x, y], 0.5 * math.hypot(L, B) + clearance + 3.0)
+        ok = True
+        for k in near:
+            dx, dy = cents[k, 0] - x, cents[k, 1] - y
+            bx, by = c * dx + s * dy, -s * dx + c * dy
+            if abs(bx) < 0.5 * L + clearance and abs(by) < 0.5 * B + clearance:
+                ok = False
+                break
+        if not ok:
+            continue
+        if len(tree.query_ball_point([x, y], R)) < 20:
+            continue
+        out.append(np.array([x, y, psi]))
+    return out
+
+
+def sample_training_controls(rng, Q: int, H: int, device):
+    """(Q, H, 2) normalised controls: half Gaussian around the surge bias (sigma
+    0.3 of the maxima, the batched-rollout generator's spread), half uniform."""
+    torch = _tm()
+    g = rng.normal(0.0, 0.3, (Q, H, 2))
+    g[..., 0] += MBDConfig.init_surge_bias
+    u = rng.uniform(-1.0, 1.0, (Q, H, 2))
+    pick = rng.random(Q) < 0.5
+    y = np.where(pick[:, None, None], g, u)
+    return torch.as_tensor(np.clip(y, -1.0, 1.0), dtype=torch.float32, device=device)
+
+
+@dataclass
+class Dataset:
+    patches: object     # (S, 64, 64, 1) bf16, normalised
+    start_of: object    # (N,) int32 start index of each sample
+    extra: object       # (N, 6 + 2H) fp32
+    raw: object         # (N, 3) float64 ice terms [KE, impulse, bonds]
+    planner: object     # (N, 4) float64 planner components of the DEM paths
+    patch_stats: tuple
+    seconds: float = 0.0
+
+
+def generate_dataset(field, n_starts: int, per_start: int, horizon: int = 64, seed: int = 0, device="cuda",
+                     patch_stats=None, weights: Optional[CostWeights] = None, **frame_kw) -> Dataset:
+    """``n_starts`` x ``per_start`` DEM rollouts (one batched launch per start)."""
+    torch = _tm()
+    from .config import get_default_simulation_config
+    from .state import build_static_arrays, ship_dynamics_arrays
+    t0 = time.time()
+    rng = np.random.default_rng(seed)
+    cfg = get_default_simulation_config()
+    static = build_static_arrays(field.polygons, field.centroids, field.bonds, field.thicknesses, field.parent_ids,
+                                 cfg, DEFAULT_MATERIAL, 0.05)
+    sd = ship_dynamics_arrays(field.ship_props, cfg, field.ship_length, field.ship_beam, field.hull_local)
+    starts = sample_starts(field, n_starts, rng, horizon)
+    raw_patches, extras, raws, plans, start_of = [], [], [], [], []
+    w = weights or CostWeights()
+    for si, e0 in enumerate(starts):
+        nu0 = np.array([rng.uniform(1.0, 3.0), 0.0, 0.0])
+        sc = make_scene(field, e0, nu0, horizon, device=device, static=static, ship_dyn=sd)
+        c0 = (COSTMAP_CELLS - PATCH_CELLS) // 2
+        raw_patches.append(sc.costmap.grid[c0:c0 + PATCH_CELLS, c0:c0 + PATCH_CELLS].clone())
+        Yn = sample_training_controls(rng, per_start, horizon, sc.device)
+        dem = DemScorer(sc, per_start, w, **frame_kw)
+        terms = dem.terms(Yn)
+        extras.append(features(sc, Yn))
+        plans.append(terms[:, :4].clone())
+        raws.append(terms[:, 4:7].clone())
+        start_of.append(torch.full((per_start,), si, dtype=torch.int32, device=sc.device))
+        dem.batch.frame_step.close()
+        del dem
+    P = torch.stack(raw_patches)
+    if patch_stats is None:
+        patch_stats = (float(P.mean().item()), float(P.std().item()) or 1.0)
+    Pn = sg_ops.to_bf16(((P - patch_stats[0]) / patch_stats[1]).contiguous()).view(len(starts), PATCH_CELLS,
+                                                                                    PATCH_CELLS, 1)
+    torch.cuda.synchronize()
+    return Dataset(Pn, torch.cat(start_of), torch.cat(extras), torch.cat(raws), torch.cat(plans), patch_stats,
+                   time.time() - t0)
+
+
+def train_surrogate(data: Dataset, horizon: int = 64, epochs: int = 8, batch: int = 256, lr: float = 1e-3,
+                    seed: int = 0, holdout: float = 0.1, device="cuda"):
+    """Adam on fp32 master weights, BF16 tensor-core forward and backward;
+    returns (Surrogate, {"train_loss", "holdout_loss", "seconds", "steps"})."""
+    torch = _tm()
+    t0 = time.time()
+    dev = torch.device(device)
+    N = int(data.extra.shape[0])
+    raw = data.raw
+    # target statistics on the log1p transform
+    sc = torch.tensor(TARGET_SCALE, dtype=torch.float64, device=dev)
+    t = torch.log1p(torch.clamp(raw, min=0.0) / sc)
+    stats = TargetStats(t.mean(0).cpu().numpy(), np.maximum(t.std(0).cpu().numpy(), 1e-6))
+    tgt = stats.forward(raw).contiguous()
+    rng = np.random.default_rng(seed)
+    # hold out whole starts (unseen ice)
+    n_starts = int(data.patches.shape[0])
+    hold = set(rng.choice(n_starts, max(1, int(round(holdout * n_starts))), replace=False).tolist())
+    so = data.start_of.cpu().numpy()
+    train_idx = np.nonzero(~np.isin(so, list(hold)))[0]
+    hold_idx = np.nonzero(np.isin(so, list(hold)))[0]
+    net = S.SurrogateNet(horizon=horizon, device=dev, seed=seed)
+    Bz = batch
+    ext_b = torch.empty((Bz, data.extra.shape[1]), dtype=torch.float32, device=dev)
+    tgt_b = torch.empty((Bz, S.N_OUT), dtype=torch.float32, device=dev)
+    pat_b = torch.empty((Bz, PATCH_CELLS, PATCH_CELLS, 1), dtype=torch.bfloat16, device=dev)
+    grad = torch.empty((Bz, S.OUT_ROWS), dtype=torch.bfloat16, device=dev)
+    loss = torch.empty(1, dtype=torch.float32, device=dev)
+    steps = 0
+    losses = []
+    for ep in range(epochs):
+        perm = rng.permutation(train_idx)
+        for b0 in range(0, len(perm) - Bz + 1, Bz):
+            idx = torch.as_tensor(perm[b0:b0 + Bz], dtype=torch.int32, device=dev)
+            sidx = data.start_of[idx.long()]
+            sg_ops.gather_rows(data.extra, idx, ext_b)
+            sg_ops.gather_rows(tgt, idx, tgt_b)
+            sg_ops.gather_rows(data.patches.view(n_starts, -1), sidx, pat_b.view(Bz, -1))
+            out = net.forward(pat_b, ext_b, keep=True)
+            sg_ops.mse(out, tgt_b, S.N_OUT, grad, loss)
+            net.backward(grad)
+            net.adam_step(lr * (0.5 * (1 + math.cos(math.pi * ep / max(epochs, 1)))))
+            steps += 1
+        losses.append(float(loss.item()))
+    sg_ops.error_flag(dev).check()
+    sur = Surrogate(net, stats, data.patch_stats)
+    hl = holdout_error(sur, data, hold_idx, tgt) if len(hold_idx) else float("nan")
+    return sur, {"train_loss": losses, "holdout_loss": hl, "seconds": time.time() - t0, "steps": steps,
+                 "train_samples": int(len(train_idx)), "holdout_samples": int(len(hold_idx))}
+
+
+def holdout_error(sur: Surrogate, data: Dataset, idx, tgt) -> float:
+    """Mean squared error of the standardised targets on held-out samples."""
+    torch = _tm()
+    dev = data.extra.device
+    errs = []
+    B = 1024
+    for b0 in range(0, len(idx), B):
+        ii = torch.as_tensor(idx[b0:b0 + B], dtype=torch.int32, device=dev)
+        n = int(ii.shape[0])
+        ext = torch.empty((n, data.extra.shape[1]), dtype=torch.float32, device=dev)
+        sg_ops.gather_rows(data.extra, ii, ext)
+        pat = torch.empty((n, PATCH_CELLS, PATCH_CELLS, 1), dtype=torch.bfloat16, device=dev)
+        sg_ops.gather_rows(data.patches.view(data.patches.shape[0], -1), data.start_of[ii.long()], pat.view(n, -1))
+        out = sur.net.forward(pat, ext)
+        errs.append(((out[:, :S.N_OUT] - tgt[ii.long()]) ** 2).mean().item() * n)
+    return float(sum(errs) / len(idx))

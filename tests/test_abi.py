@@ -8,10 +8,10 @@ import pytest
 from conftest import ROOT
 
 
-def _declared():
-    src = open(os.path.join(ROOT, "include", "dem_b200.h")).read()
+def _declared(header="dem_b200.h", prefix="dem_"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(dem_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(rf"^\s*(?:int|const char\*)\s+({prefix}\w+)\s*\(", src, flags=re.M)))
 
 
 def test_header_declares_the_boundary():
@@ -29,6 +29,18 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, name), name
     assert set(_abi.EXPORTS) <= set(_declared())
     assert lib.dem_version is not None
+
+
+def test_library_exports_every_surrogate_symbol():
+    """The surrogate's kernels (include/surrogate_b200.h) live in the same library."""
+    from mbd_icenav_b200 import _abi, build
+    build.build_library()
+    lib = ctypes.CDLL(build.LIB_PATH)
+    names = _declared("surrogate_b200.h", "sg_")
+    assert "sg_gemm" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(_abi.SG_EXPORTS) == set(names)
 
 
 def test_struct_layout_matches_header():
