@@ -665,6 +665,125 @@ def run_rollouts(args, rank: int, world: int):
     return line
 
 
+SUR_METRIC = "MBD candidates scored/s (surrogate-screened)"
+SUR_UNIT = "rollouts/s"
+
+
+def run_surrogate(args, rank: int, world: int):
+    """Surrogate-screened MBD planning against the plain batched-DEM MBD: the
+    network is trained (untimed) on DEM rollouts of the medium field, then both
+    planners plan from held-out starts; a step is one plan (n_diffuse - 1
+    reverse steps of n_sample candidates).  value = candidates scored per
+    second by the screened planner; the plain planner's rate and the relative
+    difference of the two plans' DEM costs are reported beside it."""
+    import numpy as np
+    import torch
+    _pkg()
+    from mbd_icenav_b200 import planner, sg_ops, surrogate as S
+    device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(device)
+    field = load_field("medium", args.seed)
+    H = args.horizon
+    t0 = time.time()
+    data = planner.generate_dataset(field, n_starts=args.sur_starts, per_start=args.sur_per_start, horizon=H,
+                                    seed=args.seed + 100 * rank, device=device)
+    gen_s = time.time() - t0
+    sur, info = planner.train_surrogate(data, horizon=H, epochs=args.sur_epochs, batch=256, device=device,
+                                        seed=args.seed)
+    cfg = planner.MBDConfig(horizon=H, n_sample=args.sur_samples, n_diffuse=args.sur_iters + 1,
+                            top_k=args.sur_top_k)
+    w = planner.CostWeights()
+    rng = np.random.default_rng(args.seed + 7777)
+    starts = planner.sample_starts(field, args.steps + args.warmup, rng, H)
+    stream = torch.cuda.current_stream(device)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    rows = []
+    with ClockSampler(device.index) as clk:
+        for si, e0 in enumerate(starts):
+            sc = planner.make_scene(field, e0, (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats)
+            plain = planner.DemScorer(sc, cfg.n_sample, w)
+            scr = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err)
+            (Yp, _), tp = timed(lambda: planner.mbd_plan(plain, cfg, device, seed=si))
+            n_fb0 = scr.fallbacks
+            (Ys, _), ts = timed(lambda: planner.mbd_plan(scr, cfg, device, seed=si))
+            cp = planner.plan_cost(sc, Yp, scr.dem_k)
+            cs = planner.plan_cost(sc, Ys, scr.dem_k)
+            if si >= args.warmup:
+                rows.append({"plain_s": tp, "screened_s": ts, "plain_cost": cp, "screened_cost": cs,
+                             "rel_cost_err": abs(cs - cp) / max(abs(cp), 1e-9), "fallbacks": scr.fallbacks - n_fb0,
+                             "topk_rel_err_mean": float(np.mean(scr.rel_errs)), "window": int(len(sc.window))})
+            plain.batch.frame_step.close()
+            scr.dem_k.batch.frame_step.close()
+            if scr.dem_all is not None:
+                scr.dem_all.batch.frame_step.close()
+            del plain, scr
+    # tensor-pipe figure: the network forward on one plan's population (8192 rows), timed alone
+    sc = planner.make_scene(field, starts[-1], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats)
+    Yn = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.5, -1, 1)
+    ext = planner.features(sc, Yn)
+    pat = sc.patch.expand(cfg.n_sample, -1, -1, -1).contiguous()
+    for _ in range(3):
+        sur.net.forward(pat, ext)
+    _, t_fwd = timed(lambda: [sur.net.forward(pat, ext) for _ in range(10)])
+    fl = S.flops_per_sample(H)
+    tflops = 10 * cfg.n_sample * (fl["encoder"] + fl["mlp"]) / t_fwd / 1e12
+    sg_ops.error_flag(device).check()
+    if rank != 0:
+        return None
+    K = len(rows)
+    cand = cfg.n_sample * cfg.n_diffuse - cfg.n_sample  # candidates scored per plan
+    ts = sum(r["screened_s"] for r in rows) / K
+    tp = sum(r["plain_s"] for r in rows) / K
+    ts_max = max_over_ranks(ts, world, device)
+    tp_max = max_over_ranks(tp, world, device)
+    value = world * cand / ts_max
+    plain_rate = world * cand / tp_max
+    errs = [r["rel_cost_err"] for r in rows]
+    peak_tf = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak_tf = float(json.load(fh)["bf16_tflops"])
+        peak_kind = "measured"
+    except Exception:
+        peak_tf, peak_kind = 1590.0, "fallback"
+    line = {
+        "metric": SUR_METRIC, "value": value, "unit": SUR_UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": 1e3 * ts_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 DEM, bf16 surrogate (fp32 accumulate)",
+        "data": "synthetic (seeded medium field; training tuples from the DEM's own batched rollouts)",
+        "config": {"workload": f"MBD {cfg.n_sample} samples x {cfg.n_diffuse - 1} reverse steps, horizon {H} x "
+                               f"10 substeps, top {cfg.top_k} re-scored by the DEM, fallback above "
+                               f"{cfg.max_rel_err:.0%} held-out error",
+                   "plain_dem_rollouts_per_s": plain_rate, "speedup_vs_plain_dem": value / plain_rate,
+                   "plan_rel_cost_err": errs, "plan_rel_cost_err_max": max(errs),
+                   "plans_within_5pct": int(sum(e <= 0.05 for e in errs)), "plans": rows,
+                   "train": {"samples": info["train_samples"], "holdout_samples": info["holdout_samples"],
+                             "epochs": args.sur_epochs, "steps": info["steps"], "seconds": info["seconds"],
+                             "holdout_mse_std_units": info["holdout_loss"], "train_loss": info["train_loss"],
+                             "data_seconds": gen_s, "starts": args.sur_starts, "per_start": args.sur_per_start},
+                   "network": {"params": sur.net.n_params(), "flops_per_sample_fwd": fl},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": tflops / peak_tf, "peak_kind": f"{peak_kind} bf16 dense",
+                     "what": f"surrogate forward on {cfg.n_sample} rows (per-sample encoder), 10 launches timed",
+                     "traffic": None},
+        "e2e": {"value": value, "unit": SUR_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
+                "note": "plans read their controls from device buffers; the plan's cost comes back"},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    return line
+
+
 def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_run: int = 1):
     """Per-phase device time of a few frames (profiling switch of the library).
     ``run()`` replaces the default one-frame scan (``frames`` calls of it, each
@@ -775,7 +894,9 @@ def run_reference(args):
     import multiprocessing as mp
     import numpy as np
     _pkg()
-    if args.config == "rollouts":
+    if args.config in ("rollouts", "surrogate"):
+        # the CPU reference rate of scoring candidates: the oracle port rolling
+        # candidates out on the host cores (the reference has no surrogate)
         return run_reference_rollouts(args)
     field = load_field(args.config, args.seed)
     cores = len(os.sched_getaffinity(0))
@@ -851,7 +972,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["large", "medium", "small", "rollouts"], default="large",
+    ap.add_argument("--config", choices=["large", "medium", "small", "rollouts", "surrogate"], default="large",
                     help="plain-DEM field, or batched planner rollouts on windows of the medium field")
     ap.add_argument("--rollouts", type=int, default=2048, help="candidates per batch (--config rollouts)")
     ap.add_argument("--horizon", type=int, default=64, help="control steps per candidate (--config rollouts)")
@@ -868,6 +989,12 @@ def main():
                     help="element numbering: as generated (by floe) or Morton order of centroids")
     ap.add_argument("--phase-times", action="store_true",
                     help="after the run, time one profiled frame per phase (device clock) to stderr")
+    ap.add_argument("--sur-starts", type=int, default=48, help="training starts (--config surrogate)")
+    ap.add_argument("--sur-per-start", type=int, default=2048, help="DEM rollouts per training start")
+    ap.add_argument("--sur-epochs", type=int, default=6)
+    ap.add_argument("--sur-samples", type=int, default=8192, help="MBD samples per reverse step")
+    ap.add_argument("--sur-iters", type=int, default=16, help="MBD reverse steps per plan")
+    ap.add_argument("--sur-top-k", type=int, default=64, help="candidates re-scored by the DEM per step")
     ap.add_argument("--all-active", action="store_true",
                     help="every element active from the start (the force path on the whole field)")
     args = ap.parse_args()
@@ -881,7 +1008,7 @@ def main():
             return 0
         print(json.dumps(run_reference(args)), flush=True)
         return 0
-    body = run_rollouts if args.config == "rollouts" else run_ours
+    body = {"rollouts": run_rollouts, "surrogate": run_surrogate}.get(args.config, run_ours)
     run_ranked(lambda r, w: body(args, r, w), rank, world, backend="nccl")
     return 0
 

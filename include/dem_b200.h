@@ -306,15 +306,19 @@ typedef struct DemCostmapParams {
     double ship_speed, ship_mass, ke_cost_scale;
     int32_t dilate_half;           /* square max window of 2h+1 cells; 0 = no dilation  */
     int32_t has_masses;            /* 0: masses = pi r^2 h 920 (jax_costmap.py:257-259) */
+    double ice_resistance_weight;  /* > 0: SIC modulation grid * SIC^w (:271-284)       */
+    void* sic_scratch;             /* device, rows * cols doubles when the weight is > 0 */
 } DemCostmapParams;
 
-/* Replaces the device work of build_costmap_jax (jax_costmap.py:179-331; with
- * ice_resistance_weight = 0): the KE collision costmap of the ice elements
+/* Replaces the device work of build_costmap_jax (jax_costmap.py:179-331): the KE collision costmap of the ice elements
  * (centroids (n,2), radii, thicknesses, masses (n,) of `dtype`; masses may be
  * NULL when has_masses = 0, thicknesses when it is 1) into grid (rows, cols)
- * float32, row-major.  tmp (rows, cols) float32 is needed when dilate_half > 0;
- * flag is one device int32 of scratch.  All pointers are device pointers;
- * `stream` is a cudaStream_t.  Bit-exact with the reference's float32 grid. */
+ * float32, row-major, with the SIC modulation when params->ice_resistance_weight
+ * > 0.  tmp (rows, cols) float32 is needed when dilate_half > 0; flag is one
+ * device int32 of scratch.  All pointers are device pointers; `stream` is a
+ * cudaStream_t.  Bit-exact with the reference's float32 grid (for a SIC weight
+ * other than 1 the reference's float32 power may differ by one unit in the
+ * last place from the device's, which rounds a double power once). */
 int dem_ke_costmap(int32_t dtype, int32_t n, const void* centroids, const void* radii,
                    const void* thicknesses, const void* masses, const DemCostmapParams* params,
                    float* grid, float* tmp, int32_t* flag, void* stream);

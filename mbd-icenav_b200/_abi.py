@@ -105,7 +105,7 @@ class DemCostmapParams(C.Structure):
     _fields_ = [("x_origin", _d), ("y_origin", _d), ("resolution", _d), ("rows", _i), ("cols", _i),
                 ("base_cost", _d), ("collision_cost", _d), ("obs_cost_buffer_factor", _d),
                 ("ship_speed", _d), ("ship_mass", _d), ("ke_cost_scale", _d),
-                ("dilate_half", _i), ("has_masses", _i)]
+                ("dilate_half", _i), ("has_masses", _i), ("ice_resistance_weight", _d), ("sic_scratch", _vp)]
 
 
 class DemRolloutCostParams(C.Structure):

@@ -8,8 +8,9 @@ Inputs may be NumPy arrays, torch tensors or anything exposing ``__dlpack__``
 (a JAX array, a live ``IceState`` field); ``result.grid`` keeps the grid on the
 device, and ``download=False`` skips the copy into ``result.cost_map``.
 
-Not built: the SIC modulation (``ice_resistance_weight > 0``, ``:271-284``),
-which the reference runs on the host with SciPy.
+The SIC modulation (``ice_resistance_weight > 0``, ``:271-284``), which the
+reference runs on the host with SciPy's box filter, runs on the device in the
+same float64 operation order.
 """
 from __future__ import annotations
 
@@ -69,8 +70,8 @@ def build_costmap_jax(centroids, thicknesses, radii, x_min: float, x_max: float,
                       masses=None, device=None, download: bool = True) -> Tuple[JaxCostMapResult, dict]:
     """KE collision costmap of the ice elements (``jax_costmap.py:179-331``)."""
     import torch
-    if ice_resistance_weight > 0.0:
-        raise NotImplementedError("SIC modulation (ice_resistance_weight > 0) is not built")
+    if not ice_resistance_weight >= 0.0:
+        raise ValueError("ice_resistance_weight must be >= 0")
     lib = _abi.load_library()
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     # grid geometry in double, as the reference (jax_costmap.py:237-244)
@@ -98,7 +99,12 @@ def build_costmap_jax(centroids, thicknesses, radii, x_min: float, x_max: float,
                               base_cost=base_cost, collision_cost=collision_cost,
                               obs_cost_buffer_factor=obs_cost_buffer_factor, ship_speed=ship_speed,
                               ship_mass=ship_mass, ke_cost_scale=ke_cost_scale, dilate_half=half,
-                              has_masses=1 if masses is not None else 0)
+                              has_masses=1 if masses is not None else 0,
+                              ice_resistance_weight=float(ice_resistance_weight))
+    sic = None
+    if ice_resistance_weight > 0.0:
+        sic = torch.empty(rows * cols, dtype=torch.float64, device=dev)
+        P.sic_scratch = sic.data_ptr()
     grid = torch.empty((rows, cols), dtype=torch.float32, device=dev)
     tmp = torch.empty((rows, cols), dtype=torch.float32, device=dev) if half > 0 else None
     flag = torch.empty(1, dtype=torch.int32, device=dev)

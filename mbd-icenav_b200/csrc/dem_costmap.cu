@@ -10,6 +10,8 @@
 //   * an element whose contribution the reference would make NaN everywhere
 //     (NaN centroid, non-finite radius, NaN constant) makes the grid NaN, as
 //     jnp.max over the stacked contributions does;
+//   * the SIC modulation grid * SIC^weight when ice_resistance_weight > 0
+//     (:271-284), SIC a float64 box mean of the ice-covered cells;
 //   * the open-water floor max(grid, base_cost) (:286);
 //   * the ship-footprint dilation: a (2h+1)^2 max window over the edge-padded
 //     grid (:142-176), as a row pass and a column pass (exact for a max).
@@ -91,6 +93,52 @@ __global__ void __launch_bounds__(kCmThreads) cm_paint_kernel(CmArgs c, const T*
     }
 }
 
+// SIC modulation (jax_costmap.py:271-284): SIC = box mean of the ice-covered
+// cells (grid > 0) over a k x k window with mirror padding, as SciPy's
+// uniform_filter computes it in float64 (along axis 0, then axis 1, each a
+// running sum: the first window summed in order, then + (entering - leaving)),
+// then grid *= max(float(clip(SIC, 0, 1)), 1e-6f)^weight.  One thread per
+// column for the first pass, one per row for the second (which also scales).
+__device__ __forceinline__ int mirror(int p, int len) { return p < 0 ? -p - 1 : (p >= len ? 2 * len - p - 1 : p); }
+
+__global__ void cm_sic_cols_kernel(const float* __restrict__ grid, double* __restrict__ a, int rows, int cols, int k) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const int s1 = k / 2;
+    auto occ = [&](int p) -> double { return grid[(size_t)mirror(p, rows) * cols + c] > 0.0f ? 1.0 : 0.0; };
+    double tmp = 0.0;
+    for (int l = 0; l < k; ++l) tmp += occ(l - s1);
+    a[c] = tmp / (double)k;
+    for (int i = 1; i < rows; ++i) {
+        tmp += occ(i + k - 1 - s1) - occ(i - 1 - s1);
+        a[(size_t)i * cols + c] = tmp / (double)k;
+    }
+}
+
+__global__ void cm_sic_rows_kernel(float* __restrict__ grid, const double* __restrict__ a, int rows, int cols, int k,
+                                   double weight) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const int s1 = k / 2;
+    const double* line = a + (size_t)r * cols;
+    float* g = grid + (size_t)r * cols;
+    auto scale = [&](int i, double s) {
+        const float sf = (float)dem::jclip(s, 0.0, 1.0);
+        const float safe = dem::jmax(sf, 1e-6f);
+        // the power in double, rounded once (exact for weight 1)
+        const float pw = (weight == 1.0) ? safe : (float)pow((double)safe, weight);
+        g[i] = g[i] * pw;
+    };
+    double tmp = 0.0;
+    for (int l = 0; l < k; ++l) tmp += line[mirror(l - s1, cols)];
+    // the sums read the separate array `a`, so the grid row is scaled in place
+    scale(0, tmp / (double)k);
+    for (int i = 1; i < cols; ++i) {
+        tmp += line[mirror(i + k - 1 - s1, cols)] - line[mirror(i - 1 - s1, cols)];
+        scale(i, tmp / (double)k);
+    }
+}
+
 // NaN poisoning, then the open-water floor (a NaN-propagating maximum); with
 // no element at all, the open-water cost itself (jax_costmap.py:288-289)
 __global__ void cm_floor_kernel(float* grid, size_t cells, float base, const int* poison, int empty) {
@@ -142,6 +190,14 @@ int launch_costmap(int32_t n, const void* cents, const void* radii, const void* 
                                                           (const T*)masses, (unsigned*)grid, (int*)poison);
         if (cudaGetLastError() != cudaSuccess) return DEM_ERR_CUDA;
     }
+    if (n > 0 && p->ice_resistance_weight > 0.0) {
+        const int k = std::min(31, (std::min(p->rows, p->cols) / 4) | 1);  // odd (jax_costmap.py:274-276)
+        double* a = reinterpret_cast<double*>(p->sic_scratch);
+        cm_sic_cols_kernel<<<(p->cols + 127) / 128, 128, 0, st>>>(grid, a, p->rows, p->cols, k);
+        cm_sic_rows_kernel<<<(p->rows + 127) / 128, 128, 0, st>>>(grid, a, p->rows, p->cols, k,
+                                                                 p->ice_resistance_weight);
+        if (cudaGetLastError() != cudaSuccess) return DEM_ERR_CUDA;
+    }
     const int eblocks = (int)std::min<size_t>((cells + kCmThreads - 1) / kCmThreads, (size_t)65535);
     cm_floor_kernel<<<eblocks, kCmThreads, 0, st>>>(grid, cells, (float)p->base_cost, (const int*)poison, n == 0);
     if (cudaGetLastError() != cudaSuccess) return DEM_ERR_CUDA;
@@ -162,6 +218,8 @@ extern "C" int dem_ke_costmap(int32_t dtype, int32_t n, const void* centroids, c
     if (p->rows < 1 || p->cols < 1 || !(p->resolution > 0.0) || p->dilate_half < 0) return DEM_ERR_INVALID;
     if ((long long)p->rows * p->cols >= (1LL << 31)) return DEM_ERR_INVALID;
     if (p->dilate_half > 0 && !tmp) return DEM_ERR_INVALID;
+    if (!(p->ice_resistance_weight >= 0.0) || (p->ice_resistance_weight > 0.0 && !p->sic_scratch))
+        return DEM_ERR_INVALID;
     if (n > 0 && (!centroids || !radii || (p->has_masses ? !masses : !thicknesses))) return DEM_ERR_INVALID;
     cudaStream_t st = (cudaStream_t)stream;
     if (dtype == DEM_F32) return launch_costmap<float>(n, centroids, radii, thicknesses, masses, p, grid, tmp, flag, st);

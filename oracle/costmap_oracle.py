@@ -6,7 +6,9 @@ is computed in float64 and clipped to float32 (``:256-268``); the rasteriser
 works on float32 arrays, with its float arguments (origin, resolution, buffer
 factor) entering as weak scalars, i.e. rounded to float32 where they meet the
 float32 arrays (``:99-139``); the open-water floor is a float32 maximum
-(``:286``); the ship-footprint dilation is a square max window over an
+(``:286``); the SIC modulation (``:271-284``) is a float64 box mean of the
+ice-covered cells as SciPy's ``uniform_filter`` accumulates it, then a
+float32 power; the ship-footprint dilation is a square max window over an
 edge-padded grid (``:87-95``, ``:142-176``, ``:292-298``).  Pinned by
 ``tests/test_costmap.py`` against ``tests/golden/costmap_golden.npz``.
 """
@@ -80,11 +82,52 @@ def dilate(grid, half: int) -> np.ndarray:
     return np.maximum(win.max(axis=(2, 3)), np.float32(-np.inf)).astype(np.float32)
 
 
+def sic_window(rows: int, cols: int) -> int:
+    """Box size of the SIC estimate: odd, at most 31 cells (jax_costmap.py:274-276)."""
+    k = min(31, (min(rows, cols) // 4) | 1)
+    return k + 1 if k % 2 == 0 else k
+
+
+def box_mean_1d(line: np.ndarray, size: int) -> np.ndarray:
+    """Mean over a centred window of ``size`` (``size // 2`` before, the rest
+    after) with mirror padding at the ends (d c b a | a b c d | d c b a), as a
+    running sum in float64: the first window summed in order, then each step
+    adds (entering - leaving).  This is the order in which SciPy's
+    ``uniform_filter1d`` accumulates (checked bit for bit against it)."""
+    s1 = size // 2
+    s2 = size - s1 - 1
+    ext = np.pad(np.asarray(line, np.float64), (s1, s2), mode="symmetric")
+    out = np.empty(len(line), np.float64)
+    tmp = 0.0
+    for k in range(size):
+        tmp += ext[k]
+    out[0] = tmp / size
+    for i in range(1, len(line)):
+        tmp += ext[i + size - 1] - ext[i - 1]
+        out[i] = tmp / size
+    return out
+
+
+def sic_modulate(grid: np.ndarray, weight: float) -> np.ndarray:
+    """grid * SIC^weight, SIC the local fraction of ice-covered cells
+    (jax_costmap.py:271-284): a box mean of (grid > 0) along axis 0, then
+    axis 1 (scipy.ndimage.uniform_filter, mode "reflect"), clipped to [0, 1],
+    float32, floored at 1e-6, raised to ``weight`` in float32."""
+    rows, cols = grid.shape
+    k = sic_window(rows, cols)
+    occ = (grid > 0.0).astype(np.float64)
+    a = np.stack([box_mean_1d(occ[:, c], k) for c in range(cols)], 1)
+    sic = np.stack([box_mean_1d(a[r, :], k) for r in range(rows)], 0)
+    sic = np.clip(sic, 0.0, 1.0).astype(np.float32)
+    sic_safe = np.maximum(sic, 1e-6)
+    return grid * np.power(sic_safe, weight)
+
+
 def build_costmap(centroids, thicknesses, radii, x_min, x_max, y_min, y_max, *, resolution=2.0, margin=20.0,
                   base_cost=0.1, collision_cost=5.0, obs_cost_buffer_factor=0.1, ship_length=None,
                   ship_beam=None, planning_clearance_margin=0.0, ship_speed=4.0, ship_mass=23e6,
-                  ke_cost_scale=1e-6, masses=None):
-    """``build_costmap_jax`` without SIC modulation (jax_costmap.py:179-331); returns (grid, geometry)."""
+                  ke_cost_scale=1e-6, masses=None, ice_resistance_weight=0.0):
+    """``build_costmap_jax`` (jax_costmap.py:179-331); returns (grid, geometry)."""
     x0, y0, width, height, rows, cols = grid_geometry(x_min, x_max, y_min, y_max, resolution, margin)
     n = len(centroids)
     if n > 0:
@@ -93,6 +136,8 @@ def build_costmap(centroids, thicknesses, radii, x_min, x_max, y_min, y_max, *, 
                 * ICE_DENSITY_APPROX
         kw = ke_constants(masses, collision_cost, ship_speed, ship_mass, ke_cost_scale)
         grid = rasterize(centroids, radii, kw, x0, y0, resolution, rows, cols, obs_cost_buffer_factor)
+        if ice_resistance_weight > 0.0:
+            grid = sic_modulate(grid, ice_resistance_weight)
         grid = np.maximum(grid, np.float32(base_cost))
     else:
         grid = np.full((rows, cols), float(base_cost), np.float32)

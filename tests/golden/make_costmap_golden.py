@@ -21,7 +21,10 @@ Cases (inputs and the resulting grid are stored per case in
 * ``window`` : the 500-element medium-field window of the DEM goldens, with its
                reference-built radii / thicknesses / masses, through
                ``build_costmap_jax_from_ice_state``;
-* ``nan``    : one element with a NaN centroid (the whole grid becomes NaN).
+* ``nan``    : one element with a NaN centroid (the whole grid becomes NaN);
+* ``sic1``   : the ``rand`` elements with the SIC modulation at weight 1.0;
+* ``sic_half``: the same elements, masses from the disk formula, 1 m cells, no
+               ship, SIC modulation at weight 0.5.
 """
 from __future__ import annotations
 
@@ -38,7 +41,7 @@ sys.path.insert(0, HERE)
 
 CASE_KEYS = ("x_min", "x_max", "y_min", "y_max", "resolution", "margin", "base_cost", "collision_cost",
              "obs_cost_buffer_factor", "ship_length", "ship_beam", "planning_clearance_margin",
-             "ship_speed", "ship_mass", "ke_cost_scale")
+             "ship_speed", "ship_mass", "ke_cost_scale", "ice_resistance_weight")
 
 
 def _load_costmap(ref_root: str):
@@ -59,7 +62,8 @@ def _cases():
     masses = np.pi * radii ** 2 * thick * 900.0 * rng.uniform(0.8, 1.2, n)
     base = dict(x_min=0.0, x_max=120.0, y_min=0.0, y_max=200.0, resolution=2.0, margin=20.0, base_cost=0.1,
                 collision_cost=5.0, obs_cost_buffer_factor=0.1, ship_length=60.0, ship_beam=12.0,
-                planning_clearance_margin=0.0, ship_speed=4.0, ship_mass=23e6, ke_cost_scale=1e-6)
+                planning_clearance_margin=0.0, ship_speed=4.0, ship_mass=23e6, ke_cost_scale=1e-6,
+                ice_resistance_weight=0.0)
     yield "rand", cents, radii, thick, masses, dict(base)
     yield "nomass", cents, radii, thick, None, dict(base, resolution=1.5, obs_cost_buffer_factor=0.3,
                                                     ship_length=None, ship_beam=None, margin=10.0)
@@ -74,6 +78,10 @@ def _cases():
     c2 = cents.copy()
     c2[5] = np.nan
     yield "nan", c2, radii, thick, masses, dict(base, ship_length=None, ship_beam=None)
+    # SIC modulation: the weight of the reference's own test (test_jax_ke_cost.py:381), and a fractional one
+    yield "sic1", cents, radii, thick, masses, dict(base, ice_resistance_weight=1.0)
+    yield "sic_half", cents, radii, thick, None, dict(base, ice_resistance_weight=0.5, ship_length=None,
+                                                      ship_beam=None, resolution=1.0)
 
 
 def main():

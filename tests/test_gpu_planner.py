@@ -1,0 +1,130 @@
+"""The planner pieces on the GPU: the rigid-ship rollout against the oracle's
+vessel step, the per-rollout ice terms, shared-window candidate batches, and
+the surrogate-screened MBD step (top-k re-scoring and the fallback)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+
+
+@pytest.fixture(scope="module")
+def medium():
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    return bench.load_field("medium", 0)
+
+
+def _scene(field, eta0=None, dtype=torch.float64):
+    from mbd_icenav_b200 import planner, rollouts
+    e0 = rollouts.ice_edge_pose(field) if eta0 is None else eta0
+    return planner.make_scene(field, e0, (2.0, 0.0, 0.0), horizon=16, dtype=dtype, device=DEV)
+
+
+def test_ship_rollout_matches_oracle_vessel_step(medium):
+    """dem_ship_rollout = the control-driven vessel step with no ice load
+    (jax_vessel_dynamics.py:54-84, :233-243), step by step, float64."""
+    from mbd_icenav_b200 import planner
+    from oracle.dem_oracle import ship_step
+    sc = _scene(medium)
+    rng = np.random.default_rng(0)
+    Q, H = 5, 16
+    Yn = torch.as_tensor(rng.uniform(-1, 1, (Q, H, 2)), dtype=torch.float32, device=DEV)
+    u = planner.physical_controls(Yn).double()
+    comp = planner.rigid_terms(sc, Yn)  # runs dem_ship_rollout
+    import ctypes as C
+    from mbd_icenav_b200 import _abi
+    lib = _abi.load_library()
+    eta0 = torch.as_tensor(np.tile(sc.eta0, (Q, 1)), dtype=torch.float64, device=DEV)
+    nu0 = torch.as_tensor(np.tile(sc.nu0, (Q, 1)), dtype=torch.float64, device=DEV)
+    hist = torch.empty((H, Q, 3), dtype=torch.float64, device=DEV)
+    assert lib.dem_ship_rollout(C.byref(sc.params), _abi.DEM_F64, Q, H, eta0.data_ptr(), nu0.data_ptr(),
+                                u.data_ptr(), None, hist.data_ptr(), None, None) == 0
+    torch.cuda.synchronize()
+    P = sc.params
+    M3inv = np.array(P.M3inv[:]).reshape(3, 3)
+    D3 = np.array(P.D3[:]).reshape(3, 3)
+    un = u.cpu().numpy()
+    for q in range(Q):
+        eta, nu = sc.eta0.copy(), sc.nu0.copy()
+        na, ei = np.zeros(6), np.zeros(3)
+        for t in range(H):
+            eta, nu, na, ei = ship_step(eta, nu, na, ei, np.zeros(3), np.zeros(3), np.zeros(3), M3inv, D3,
+                                        np.zeros((3, 3)), np.zeros((3, 3)), np.zeros((3, 3)), np.zeros((6, 3)),
+                                        np.ones(6), np.zeros((3, 6)), 1.0, P.dt, np.zeros(2), False,
+                                        (P.vc_surge, P.vc_sway, P.vc_yaw), np.float64, u_ctrl=un[t, q])
+            np.testing.assert_allclose(hist[t, q].cpu().numpy(), eta, rtol=1e-12, atol=1e-9)
+    assert torch.isfinite(comp).all()
+
+
+def test_shared_window_candidates_equal_their_runs_alone_and_ice_terms(medium):
+    """Each candidate of a shared-window batch equals the same candidate run as
+    a batch of one, bit for bit; the ice terms are the sums they name."""
+    from mbd_icenav_b200 import planner, rollouts
+    sc = _scene(medium, dtype=torch.float32)
+    w = planner.CostWeights()
+    Q = 6
+    rng = np.random.default_rng(1)
+    Yn = torch.as_tensor(np.clip(rng.normal(0.7, 0.4, (Q, 16, 2)), -1, 1), dtype=torch.float32, device=DEV)
+    dem = planner.DemScorer(sc, Q, w)
+    terms = dem.terms(Yn)
+    u = planner.physical_controls(Yn).to(torch.float32)
+    res = rollouts.run(dem.batch, u, history="ship")
+    J = res.history[5]  # (H, Q)
+    assert torch.allclose(terms[:, 5], J.double().sum(0), rtol=1e-12, atol=0)
+    nb = int(dem.batch.bond_start[1].item())
+    broken = (dem.batch.state.bond_intact & ~res.state.bond_intact).view(Q, nb).sum(1).double()
+    assert torch.equal(terms[:, 6], broken)
+    assert (terms[:, 4] >= 0).all() and terms[:, 4].max() > 0, "the candidates must push ice"
+    for q in (0, Q - 1):
+        one = planner.DemScorer(sc, 1, w)
+        t1 = one.terms(Yn[q:q + 1].contiguous())
+        assert torch.equal(t1[0], terms[q]), q
+        one.batch.frame_step.close()
+    dem.batch.frame_step.close()
+
+
+def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
+    """A surrogate-screened cost batch: the top_k candidates get their exact DEM
+    costs, the rest the prediction; with max_rel_err = 0 every step falls back
+    to the DEM for all candidates (equal to the plain DEM batch)."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from mbd_icenav_b200 import planner
+    field = bench.load_field("medium", 0)
+    data = planner.generate_dataset(field, n_starts=3, per_start=256, horizon=16, seed=2, device=DEV)
+    assert data.extra.shape == (768, 6 + 32) and torch.isfinite(data.raw).all()
+    sur, info = planner.train_surrogate(data, horizon=16, epochs=2, batch=128, device=DEV)
+    assert np.isfinite(info["train_loss"][-1])
+    sc = planner.make_scene(field, planner.sample_starts(field, 1, np.random.default_rng(9), 16)[0],
+                            (2.0, 0.0, 0.0), horizon=16, device=DEV, patch_stats=data.patch_stats)
+    w = planner.CostWeights()
+    Q, k = 256, 16
+    rng = np.random.default_rng(3)
+    Yn = torch.as_tensor(np.clip(rng.normal(0.7, 0.5, (Q, 16, 2)), -1, 1), dtype=torch.float32, device=DEV)
+    plain = planner.DemScorer(sc, Q, w)
+    exact = plain(Yn)
+    scr = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, max_rel_err=float("inf"))
+    cost = scr(Yn)
+    pred_ice = sur.predict(sc, Yn)
+    pred = planner.rigid_terms(sc, Yn) @ torch.tensor(w.planner(), dtype=torch.float64, device=DEV) + \
+        pred_ice @ torch.tensor(w.ice(), dtype=torch.float64, device=DEV)
+    top = torch.topk(pred, k, largest=False).indices
+    assert torch.allclose(cost[top], exact[top], rtol=0, atol=0)
+    rest = torch.ones(Q, dtype=torch.bool, device=DEV)
+    rest[top] = False
+    assert torch.allclose(cost[rest], pred[rest])
+    fb = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, max_rel_err=0.0)
+    assert torch.equal(fb(Yn), exact) and fb.fallbacks == 1
+    # a short plan runs end to end with both cost batches
+    cfg = planner.MBDConfig(horizon=16, n_sample=Q, n_diffuse=3, top_k=k)
+    Yp, m1 = planner.mbd_plan(plain, cfg, DEV, seed=0)
+    Ys, m2 = planner.mbd_plan(scr, cfg, DEV, seed=0)
+    assert Yp.shape == (16, 2) and Ys.shape == (16, 2) and len(m1) == len(m2) == 2
+    assert np.isfinite(planner.plan_cost(sc, Ys, scr.dem_k))
