@@ -544,6 +544,10 @@ def run_rollouts(args, rank: int, world: int):
 
     for _ in range(W):
         step(u_d, check=True)
+    # the work split of this batch shape, picked by timing every choice (all
+    # give identical results); untimed
+    from mbd_icenav_b200 import autotune
+    split, split_ms = autotune.tune(fs, lambda: rollouts.run(b, u_d, vw, history="ship", check=False))
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
@@ -642,6 +646,7 @@ def run_rollouts(args, rank: int, world: int):
                    "max_neighbors": fs.params.max_neighbors, "bucket_capacity": fs.params.bucket_capacity,
                    "skin_m": fs.params.skin,
                    "active_elements": [act0[0], act1[0]], "bonds_with_active_end": [act0[1], act1[1]],
+                   "work_split": split, "work_split_ms": split_ms,
                    "mean_transferred_ke_J": float(c[:, 4].mean()),
                    "rollouts_touching_ice": int((c[:, 4] > 0).sum())},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -712,6 +717,10 @@ def run_surrogate(args, rank: int, world: int):
             sc = planner.make_scene(field, e0, (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats)
             plain = planner.DemScorer(sc, cfg.n_sample, w)
             scr = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err)
+            # untimed: each DEM batch's work split, tuned on candidates like a plan's
+            Yt = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.7, -1, 1)
+            split_plain, _ = plain.autotune(Yt)
+            split_k, _ = scr.dem_k.autotune(Yt[:cfg.top_k].contiguous())
             (Yp, _), tp = timed(lambda: planner.mbd_plan(plain, cfg, device, seed=si))
             n_fb0 = scr.fallbacks
             (Ys, _), ts = timed(lambda: planner.mbd_plan(scr, cfg, device, seed=si))
@@ -720,7 +729,8 @@ def run_surrogate(args, rank: int, world: int):
             if si >= args.warmup:
                 rows.append({"plain_s": tp, "screened_s": ts, "plain_cost": cp, "screened_cost": cs,
                              "rel_cost_err": abs(cs - cp) / max(abs(cp), 1e-9), "fallbacks": scr.fallbacks - n_fb0,
-                             "topk_rel_err_mean": float(np.mean(scr.rel_errs)), "window": int(len(sc.window))})
+                             "topk_rel_err_mean": float(np.mean(scr.rel_errs)), "window": int(len(sc.window)),
+                             "work_split": [split_plain, split_k]})
             plain.batch.frame_step.close()
             scr.dem_k.batch.frame_step.close()
             if scr.dem_all is not None:

@@ -286,6 +286,13 @@ class DemScorer:
         self.rollouts += self.Q
         return torch.cat([comp[:, :4], comp[:, 4:5], self.ice_out], 1)
 
+    def autotune(self, Yn):
+        """Pick this batch's work split by timing it on candidates Yn (every
+        choice gives identical results); returns (choice, {choice: ms})."""
+        from . import autotune
+        u = physical_controls(Yn).to(self.scene.dtype)
+        return autotune.tune(self.batch.frame_step, lambda: rollouts.run(self.batch, u, history="ship", check=False))
+
     def total(self, terms):
         torch = _tm()
         w = torch.tensor(self.w.planner() + self.w.ice(), dtype=torch.float64, device=terms.device)

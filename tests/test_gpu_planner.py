@@ -128,3 +128,26 @@ def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
     Ys, m2 = planner.mbd_plan(scr, cfg, DEV, seed=0)
     assert Yp.shape == (16, 2) and Ys.shape == (16, 2) and len(m1) == len(m2) == 2
     assert np.isfinite(planner.plan_cost(sc, Ys, scr.dem_k))
+
+
+def test_autotune_picks_the_fastest_split_and_caches_it(medium):
+    """The work-split autotuner times every choice on the batch, sets the
+    fastest, and sets the cached choice for the same bucket without timing;
+    the batch's results do not depend on the choice."""
+    from mbd_icenav_b200 import autotune, planner, rollouts
+    sc = _scene(medium, dtype=torch.float32)
+    w = planner.CostWeights()
+    Q = 32
+    rng = np.random.default_rng(5)
+    Yn = torch.as_tensor(np.clip(rng.normal(0.7, 0.4, (Q, 16, 2)), -1, 1), dtype=torch.float32, device=DEV)
+    dem = planner.DemScorer(sc, Q, w)
+    ref = dem.terms(Yn)
+    best, times = dem.autotune(Yn)
+    assert set(times) == {c[0] for c in autotune.CHOICES} and best == min(times, key=times.get)
+    assert torch.equal(dem.terms(Yn), ref)
+    again, t2 = dem.autotune(Yn)
+    assert again == best and t2 == {}
+    for name, _, _ in autotune.CHOICES:
+        autotune.apply(dem.batch.frame_step, name)
+        assert torch.equal(dem.terms(Yn), ref), name
+    dem.batch.frame_step.close()
