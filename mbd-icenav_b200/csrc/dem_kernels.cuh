@@ -1495,19 +1495,24 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
 // Positions are packed with radii as {x, y, r} (one 16-byte load per neighbour,
 // velocities only for overlapping pairs) and bond slots are 16-byte records;
 // the loads of a batch are issued before any of them is used.
-// Contact distances and every predicate are computed unfused (-fmad=false);
-// force values use explicit fma where the reference's products are summed.
+// Every operation is unfused (-fmad=false) and in the reference's order, with
+// divisions where it divides, so that fp32 forces round as NumPy's fp32
+// evaluation of the same expressions does.
 #ifndef DEM_KBATCH
 #define DEM_KBATCH 2
 #endif
 constexpr int kBatch = DEM_KBATCH;  // bond slots / contact candidates whose loads are issued together
 
 
-__device__ __forceinline__ float jfma(float a, float b, float c) { return fmaf(a, b, c); }
-// correctly rounded reciprocal (force directions; predicates never use it)
-__device__ __forceinline__ float jrcp(float a) { return __frcp_rn(a); }
-__device__ __forceinline__ double jrcp(double a) { return __drcp_rn(a); }
-__device__ __forceinline__ double jfma(double a, double b, double c) { return fma(a, b, c); }
+// overlap^1.5 of the Hertz law, as the reference's power of an fp32 array: in
+// float the product o * sqrt(o) is formed in double and rounded once, which
+// gives the correctly rounded power (the value the C library's powf returns
+// but for its rare last-place misses); in double as is
+__device__ __forceinline__ float hertz15(float o) {
+    const double od = (double)o;
+    return (float)(od * sqrt(od));
+}
+__device__ __forceinline__ double hertz15(double o) { return o * sqrt(o); }
 
 // Constants and substep buffers of one force phase.
 template <typename T>
@@ -1557,11 +1562,11 @@ __device__ __forceinline__ void bond_term(const SlotRec<T>& r, typename vec2_of<
     const T dx = role_j ? ex - kb.x : kb.x - ex;
     const T dy = role_j ? ey - kb.y : kb.y - ey;
     const T dist = jsqrt(dx * dx + dy * dy);
-    const T inv = jrcp(jmax(dist, T(1e-10)));
+    const T dsafe = jmax(dist, T(1e-10));
     const T fmag = r.stiff * (dist - r.rest) * r.omd;
-    fx = (dx * inv) * fmag;
-    fy = (dy * inv) * fmag;
-    cr = T(0.5) * jfma(dx, fy, -(dy * fx));
+    fx = (dx / dsafe) * fmag;  // bond_dir * f_mag (jax_simulation.py:76-96)
+    fy = (dy / dsafe) * fmag;
+    cr = T(0.5) * (dx * fy - dy * fx);
 }
 
 // Ice-ice contact term (jax_simulation.py:111-164) of element e (kinematics
@@ -1585,23 +1590,24 @@ __device__ __forceinline__ bool contact_term(const ForceConst<T>& fc, bool h15, 
     const T dist = jsqrt(d2);
     const T overlap = jmax(min_dist - dist, T(0));
     if (!((dist > T(1e-6)) && (overlap > T(0)))) return false;
-    const T inv = jrcp(dist);
-    const T ux = dx * inv, uy = dy * inv;
-    const T fn = fc.hf * (h15 ? overlap * jsqrt(overlap) : jpow(overlap, fc.hexp));
+    // direction = d / max(dist, 1e-10); here dist > 1e-6 (jax_simulation.py:133-136)
+    const T ux = dx / dist, uy = dy / dist;
+    const T fn = fc.hf * (h15 ? hertz15(overlap) : jpow(overlap, fc.hexp));
     const T fnx = ux * fn, fny = uy * fn;
     const T vrx = e_is_i ? vo.x - ve.x : ve.x - vo.x;
     const T vry = e_is_i ? vo.y - ve.y : ve.y - vo.y;
-    const T vdot = jfma(vrx, ux, vry * uy);
-    const T vtx = jfma(-vdot, ux, vrx), vty = jfma(-vdot, uy, vry);
+    // tangential relative velocity and kinetic friction (jax_simulation.py:139-149)
+    const T vdot = vrx * ux + vry * uy;
+    const T vtx = vrx - vdot * ux, vty = vry - vdot * uy;
     const T vtm = jsqrt(vtx * vtx + vty * vty);
     T ftx = T(0), fty = T(0);
     if (vtm > T(1e-6)) {
-        const T ftm = jmin(fc.mu * fn, fc.fcap) * jrcp(vtm);
-        ftx = -vtx * ftm;
-        fty = -vty * ftm;
+        const T ftm = jmin(fc.mu * fn, fc.fcap);
+        ftx = (-vtx / vtm) * ftm;  // t_hat * f_t_mag
+        fty = (-vty / vtm) * ftm;
     }
     const T oix = -fnx - ftx, oiy = -fny - fty;
-    const T cr = -jfma(dx, oiy, -(dy * oix));
+    const T cr = -(dx * oiy - dy * oix);
     tx = e_is_i ? ftx - fnx : fnx - ftx;
     ty = e_is_i ? fty - fny : fny - fty;
     hm = T(0.5) * cr;
@@ -1644,9 +1650,10 @@ __device__ __forceinline__ int integrate_element(const KArgs<T>& a, const Frame<
     const T vm = jsqrt(vrx * vrx + vry * vry);
     T fdx, fdy;
     if (vm > T(1e-6)) {
-        const T q = a.fc.c_drag * a_drag * vm;  // (v/|v|) * c A |v|^2
-        fdx = vrx * q;
-        fdy = vry * q;
+        // (v / |v|) * (c A |v|^2), evaluated as the reference writes it
+        const T q = (a.fc.c_drag * a_drag) * (vm * vm);
+        fdx = (vrx / vm) * q;
+        fdy = (vry / vm) * q;
     } else {
         const T cl = a.fc.c_drag * a_drag * a.fc.lin;
         fdx = cl * vrx;

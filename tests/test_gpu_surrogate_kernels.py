@@ -110,8 +110,8 @@ def test_im2col_gemm_is_conv2d_and_col2im_is_its_adjoint(C):
     Bn_, CK, L = cols_t.shape
     perm = cols_t.reshape(Bn_, C, 9, L).permute(0, 3, 2, 1).reshape(Bn_ * L, 9 * C)  # (ky, kx, c) order
     (perm * dcols[:, :9 * C]).sum().backward()
-    np.testing.assert_allclose(dX.float().cpu().numpy(), Xr.grad.permute(0, 2, 3, 1).to(torch.bfloat16).float()
-                               .cpu().numpy(), rtol=1.0 / 128, atol=1e-6)
+    np.testing.assert_allclose(dX.float().cpu().numpy(), Xr.grad.to(torch.bfloat16).float().cpu().numpy(),
+                               rtol=1.0 / 128, atol=1e-6)
     assert abs(lhs - rhs) <= 1e-2 * max(abs(lhs), 1.0)
 
 
@@ -188,8 +188,35 @@ def test_mse_and_row_packing():
                        .to(torch.bfloat16))
 
 
+class _RoundBF16(torch.autograd.Function):
+    """Identity rounded to bf16 in both directions: the network's kernels store
+    every activation and every activation gradient as bf16."""
+
+    @staticmethod
+    def forward(ctx, x):
+        return x.to(torch.bfloat16).float()
+
+    @staticmethod
+    def backward(ctx, g):
+        return g.to(torch.bfloat16).float()
+
+
+class _GradBF16(torch.autograd.Function):
+    """Identity forward, gradient rounded to bf16 (the loss gradient the MSE kernel stores)."""
+
+    @staticmethod
+    def forward(ctx, x):
+        return x.clone()
+
+    @staticmethod
+    def backward(ctx, g):
+        return g.to(torch.bfloat16).float()
+
+
 def _torch_reference(net, patches, extra):
-    """The same network in plain fp32 PyTorch (autograd) on the kernels' bf16 weights."""
+    """The same network in plain fp32 PyTorch (autograd, no TF32) on the kernels'
+    bf16 weights, rounding activations and their gradients to bf16 where the
+    kernels store them."""
     from mbd_icenav_b200 import surrogate as S
     params = []
     x = patches.float().permute(0, 3, 1, 2)
@@ -197,7 +224,7 @@ def _torch_reference(net, patches, extra):
         w = layer.w.float()[:, :9 * cin].reshape(cout, 3, 3, cin).permute(0, 3, 1, 2).clone().requires_grad_(True)
         b = layer.b.clone().requires_grad_(True)
         params.append((w, b))
-        x = torch.relu(torch.nn.functional.conv2d(x, w, b, stride=2, padding=1))
+        x = _RoundBF16.apply(torch.relu(torch.nn.functional.conv2d(x, w, b, stride=2, padding=1)))
     enc = x.permute(0, 2, 3, 1).reshape(x.shape[0], -1)
     h = torch.cat([enc, extra, torch.zeros((enc.shape[0], net.xdim - enc.shape[1] - extra.shape[1]), device=DEV)], 1)
     for li, layer in enumerate(net.fc):
@@ -206,15 +233,16 @@ def _torch_reference(net, patches, extra):
         params.append((w, b))
         h = h @ w.T + b
         if li < len(net.fc) - 1:
-            h = torch.relu(h)
-    return h, params
+            h = _RoundBF16.apply(torch.relu(h))
+    return _GradBF16.apply(h), params
 
 
 def test_network_forward_and_gradients_match_torch_autograd():
     """Forward outputs and every layer's weight / bias gradients of the bf16
     tensor-core network against fp32 autograd on the same bf16 weights and
-    inputs.  The kernels round activations to bf16 between layers, so the
-    check is on relative norms (2 %) and direction (cosine > 0.999)."""
+    inputs, rounding where the kernels round.  What remains is the fp32
+    summation order and the bf16 roundings it can flip: relative norms within
+    2 % and direction (cosine) above 0.999 for every layer."""
     from mbd_icenav_b200 import surrogate as S
     ops = _ops()
     R, H = 64, 64
@@ -230,7 +258,12 @@ def test_network_forward_and_gradients_match_torch_autograd():
     net.backward(grad)
     torch.cuda.synchronize()
     ops.error_flag(DEV).check()
-    ref_out, params = _torch_reference(net, patches, extra.to(torch.bfloat16).float())
+    tf32 = (torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32)
+    torch.backends.cudnn.allow_tf32 = torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        ref_out, params = _torch_reference(net, patches, extra.to(torch.bfloat16).float())
+    finally:
+        torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32 = tf32
     rl = ((ref_out[:, :S.N_OUT] - tgt) ** 2).mean()
     rl.backward()
     o = out[:, :S.N_OUT]
