@@ -67,6 +67,8 @@ struct DemHandle {
     int* counters = nullptr;  // block holding the per-call counters below
     size_t counters_bytes = 0;
     unsigned* bstamp = nullptr;  // (nb) frame stamps of bonds with an active end
+    int* fb_list = nullptr;      // (nb) the frame's bonds with an active end
+    int* fb_cnt = nullptr;
     int* act_cnt = nullptr;
     int* slot_owner = nullptr;
     unsigned* esc_cnt = nullptr;
@@ -361,6 +363,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.lazy_list = h->lazy_list;
     a.lazy_cnt = h->lazy_cnt;
     a.bstamp = h->bstamp;
+    a.fb_list = h->fb_list;
+    a.fb_cnt = h->fb_cnt;
     a.act_cnt = h->act_cnt;
     a.slot_owner = h->slot_owner;
     a.esc_cnt = h->esc_cnt;
@@ -693,6 +697,8 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->lazy_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bstamp, sizeof(unsigned) * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fb_list, sizeof(int) * std::max(nb, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->fb_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     {

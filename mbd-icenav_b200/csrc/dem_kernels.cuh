@@ -159,6 +159,8 @@ struct KArgs {
     int* work_cnt;      // (k_sub + 2) element chunks handed out dynamically, per substep
     int* act_list;      // (n) elements active this frame (built by phase_reduce)
     unsigned* bstamp;   // (nb) frame stamp of the bonds with an active end (set by phase_reduce)
+    int* fb_list;       // (nb) the frame's bonds with an active end, each once (phase_reduce)
+    int* fb_cnt;        // (1) entries of fb_list
     int* act_cnt;       // (1) entries of act_list
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
     int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
@@ -253,12 +255,18 @@ __device__ bool grid_barrier(const KArgs<T>& a) {
         // of one barrier sum to 2^31, so bit 31 of the word flips exactly when the
         // last CTA arrives, and the word needs no reset between barriers
         const unsigned inc = (blockIdx.x == 0) ? 0x80000000u - (gridDim.x - 1u) : 1u;
-        __threadfence();
-        const unsigned old = atomicAdd(a.bar, inc);
+        // the arrival is a release at GPU scope (cumulative over the CTA's writes
+        // ordered before it by __syncthreads), the polls are acquires: the
+        // pattern orders every CTA's phase writes before every CTA's next phase
+        const unsigned old = atom_add_release_u32(a.bar, inc);
         int ok = 1;
-        const unsigned long long t0 = globaltimer_ns();
-        while (((ld_acquire_u32(a.bar) ^ old) & 0x80000000u) == 0u) {
-            if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+        unsigned long long t0 = 0;
+        for (unsigned it = 0; ((ld_acquire_u32(a.bar) ^ old) & 0x80000000u) == 0u; ++it) {
+            if ((it & 63u) != 0u) continue;  // the time limit is read every 64 polls
+            const unsigned long long t = globaltimer_ns();
+            if (it == 0) {
+                t0 = t;
+            } else if (t - t0 > kBarrierLimitNs) {
                 // a CTA that gives up returns; every other CTA's wait then ends
                 // at its own limit, so the launch always finishes
                 atomicMax(a.status, DEM_ERR_TIMEOUT);
@@ -266,7 +274,6 @@ __device__ bool grid_barrier(const KArgs<T>& a) {
                 break;
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -950,7 +957,10 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
     const T reach = a.hull_r * T(1.0001) + T(1e-3);
     // nothing reads the grid in this phase: drop stale entries queued last frame
     compact_buckets(a);
-    if (gtid == 0) *a.act_cnt = 0;  // read last by the previous frame's force phases
+    if (gtid == 0) {
+        *a.act_cnt = 0;  // read last by the previous frame's force phases
+        *a.fb_cnt = 0;   // read last by the previous frame's fracture
+    }
     // per-floe scratch of this frame (read last by the previous frame's fracture)
     for (int fl = gtid; fl < a.nf; fl += gsz) {
         a.fcoll[fl] = 0;
@@ -1461,8 +1471,9 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             const int2 ent0 = a.bslot[sl];
             const int2 ent1 = two ? a.bslot[sl + 1] : ent0;
             const int b0 = ent0.x & 0x7fffffff, b1 = ent1.x & 0x7fffffff;
-            a.bstamp[b0] = fstamp;  // the bond has an active end this frame
-            a.bstamp[b1] = fstamp;
+            // the bond has an active end this frame; the first stamper lists it
+            if (atomicExch(&a.bstamp[b0], fstamp) != fstamp) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b0;
+            if (two && atomicExch(&a.bstamp[b1], fstamp) != fstamp) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b1;
             const bool in0 = F.src.intact[b0] != 0, in1 = F.src.intact[b1] != 0;
             const bool sa0 = F.src.active[ent0.y] != 0, sa1 = F.src.active[ent1.y] != 0;
             const int fo0 = a.floe_of[ent0.y], fo1 = a.floe_of[ent1.y];
@@ -1920,6 +1931,52 @@ __device__ __forceinline__ int force_element_warp(const KArgs<T>& a, const Frame
 }
 
 template <typename T>
+__device__ __forceinline__ void copy4(const T* __restrict__ s, T* __restrict__ d, bool plus_zero);
+
+// Out of place (a frame that writes the caller's separate output), the state of
+// every bond is copied to the output during the substeps, a slice of the bond
+// groups of four per substep, by warps that have no element work there (the
+// substeps of a frame with few active elements leave most warps idle).  A
+// bond keeps its state unless it has an active end (jax_simulation.py:534-653:
+// with both ends frozen no gate opens and no collision breaks it), and the
+// fracture phase overwrites the copies of the bonds that have one.  The shear
+// displacement is copied as x + 0 and the intact flag as 0/1, as the update
+// itself would write them.  Warp `cw` of `ncw` copiers takes its share.
+template <typename T>
+__device__ __forceinline__ void copy_bond_slice(const KArgs<T>& a, const Frame<T>& F, int s, int cw, int ncw) {
+    const int ng = (a.nb + 3) >> 2;
+    const int g_lo = (int)((long long)ng * s / a.k_sub), g_hi = (int)((long long)ng * (s + 1) / a.k_sub);
+    auto al16 = [](const void* p) { return ((size_t)p & 15u) == 0; };
+    const bool vec = al16(F.src.ds) && al16(F.dst.ds) && al16(F.src.dmg) && al16(F.dst.dmg) && al16(F.src.dm0) &&
+                     al16(F.dst.dm0) && al16(F.src.dmmax) && al16(F.dst.dmmax) &&
+                     ((size_t)F.src.intact & 3u) == 0 && ((size_t)F.dst.intact & 3u) == 0;
+    for (int g = g_lo + cw * 32 + (threadIdx.x & 31); g < g_hi; g += ncw * 32) {
+        const int b0 = 4 * g;
+        const int cnt = min(4, a.nb - b0);
+        if (vec && cnt == 4) {
+            copy4<T>(F.src.ds + b0, F.dst.ds + b0, true);
+            copy4<T>(F.src.dmg + b0, F.dst.dmg + b0, false);
+            copy4<T>(F.src.dm0 + b0, F.dst.dm0 + b0, false);
+            copy4<T>(F.src.dmmax + b0, F.dst.dmmax + b0, false);
+            const unsigned raw = *reinterpret_cast<const unsigned*>(F.src.intact + b0);
+            unsigned in4 = 0u;
+            for (int k = 0; k < 4; ++k)
+                if ((raw >> (8 * k)) & 0xffu) in4 |= 1u << (8 * k);
+            *reinterpret_cast<unsigned*>(F.dst.intact + b0) = in4;
+        } else {
+            for (int k = 0; k < cnt; ++k) {
+                const int b = b0 + k;
+                F.dst.ds[b] = F.src.ds[b] + T(0);
+                F.dst.dmg[b] = F.src.dmg[b];
+                F.dst.dm0[b] = F.src.dm0[b];
+                F.dst.dmmax[b] = F.src.dmmax[b];
+                F.dst.intact[b] = F.src.intact[b] != 0 ? 1 : 0;
+            }
+        }
+    }
+}
+
+template <typename T>
 __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigned round, int nd, int n_lazy,
                             int na) {
     const ForceCtx<T> cx = force_ctx(a, F, s);
@@ -1982,6 +2039,7 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     // then takes further chunks from a counter (the next grab is issued before
     // the current chunk is computed), so uneven chunks do not leave warps idle.
     const int nw2 = nwarps - skip;
+    const bool copy_bonds = a.nb > 0 && F.src.ds != F.dst.ds;
     if (a.force_split == DEM_SPLIT_WARP || (a.force_split == DEM_SPLIT_AUTO && na <= 2 * nw2)) {
         // at most two active elements per warp: a warp per element
         for (int i = warp - skip; i < na; i += nw2) {
@@ -1990,6 +2048,16 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
             const int code = force_element_warp(a, F, cx, e);
             if (lane == 0 && code == 2) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
             if (lane == 0 && code == 1) a.lazy_list[atomicAdd(lazy_ctr, 1)] = e;
+        }
+        if (copy_bonds) {
+            // the warps without an element copy this substep's slice; when every
+            // warp has one, all of them copy after it
+            const int busy = min(na, nw2);
+            if (busy < nw2) {
+                if (warp - skip >= busy) copy_bond_slice(a, F, s, warp - skip - busy, nw2 - busy);
+            } else {
+                copy_bond_slice(a, F, s, warp - skip, nw2);
+            }
         }
         return;
     }
@@ -2010,6 +2078,7 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
         }
         c = __shfl_sync(0xffffffffu, next, 0);
     }
+    if (copy_bonds) copy_bond_slice(a, F, s, warp - skip, nw2);
 }
 
 // ─── bond damage (jax_bond_fracture.py:133-208) ─────────────────────────────
@@ -2184,74 +2253,15 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
     const unsigned fstamp = frame_stamp(a, F);
-    // Bonds in groups of four per thread.  A bond between two frozen elements
-    // keeps its state: neither end touches the ship (a touched element's floe is
-    // active this frame), so both contact forces are 0, no DPDEM gate opens and
-    // no collision breaks it; the update is then the copy of its state (shear
-    // displacement + 0, intact as 0/1).  Every bond of the group is copied first
-    // (16-byte accesses when all state arrays are aligned); then the bonds with an
-    // active end, which carry this frame's stamp (phase_reduce), take the full
-    // update and overwrite their copy.
-    auto al16 = [](const void* p) { return ((size_t)p & 15u) == 0; };
-    const bool vec = al16(F.src.ds) && al16(F.dst.ds) && al16(F.src.dmg) && al16(F.dst.dmg) && al16(F.src.dm0) &&
-                     al16(F.dst.dm0) && al16(F.src.dmmax) && al16(F.dst.dmmax) && al16(a.bstamp) &&
-                     ((size_t)F.src.intact & 3u) == 0 && ((size_t)F.dst.intact & 3u) == 0;
-    const int ng = (a.nb + 3) >> 2;
-    // updating in place (frames after the first of a call): bonds without an
-    // active end are already in place; only their history row is written
-    const bool inplace = F.src.ds == F.dst.ds;
-    for (int g = gtid; g < ng; g += gsz) {
-        const int b0 = 4 * g;
-        const int cnt = min(4, a.nb - b0);
-        unsigned st[4] = {0u, 0u, 0u, 0u};
-        unsigned in4 = 0u;
-        if (inplace) {
-            for (int k = 0; k < cnt; ++k) {
-                const int b = b0 + k;
-                if (a.bstamp[b] == fstamp) {
-                    fracture_bond(a, F, scale, b);
-                } else if (a.h_intact) {
-                    a.h_intact[(size_t)F.f * a.nb + b] = F.src.intact[b] != 0 ? 1 : 0;
-                }
-            }
-            continue;
-        }
-        if (vec && cnt == 4) {
-            const uint4 s4 = *reinterpret_cast<const uint4*>(a.bstamp + b0);
-            st[0] = s4.x;
-            st[1] = s4.y;
-            st[2] = s4.z;
-            st[3] = s4.w;
-            copy4<T>(F.src.ds + b0, F.dst.ds + b0, true);
-            copy4<T>(F.src.dmg + b0, F.dst.dmg + b0, false);
-            copy4<T>(F.src.dm0 + b0, F.dst.dm0 + b0, false);
-            copy4<T>(F.src.dmmax + b0, F.dst.dmmax + b0, false);
-            const unsigned raw = *reinterpret_cast<const unsigned*>(F.src.intact + b0);
-            for (int k = 0; k < 4; ++k)
-                if ((raw >> (8 * k)) & 0xffu) in4 |= 1u << (8 * k);
-            *reinterpret_cast<unsigned*>(F.dst.intact + b0) = in4;
-        } else {
-            for (int k = 0; k < cnt; ++k) {
-                const int b = b0 + k;
-                st[k] = a.bstamp[b];
-                F.dst.ds[b] = F.src.ds[b] + T(0);
-                F.dst.dmg[b] = F.src.dmg[b];
-                F.dst.dm0[b] = F.src.dm0[b];
-                F.dst.dmmax[b] = F.src.dmmax[b];
-                const unsigned v = F.src.intact[b] != 0 ? 1u : 0u;
-                F.dst.intact[b] = (uint8_t)v;
-                in4 |= v << (8 * k);
-            }
-        }
-        for (int k = 0; k < cnt; ++k) {
-            const int b = b0 + k;
-            if (st[k] == fstamp) {
-                fracture_bond(a, F, scale, b);
-            } else if (a.h_intact) {
-                a.h_intact[(size_t)F.f * a.nb + b] = (uint8_t)((in4 >> (8 * k)) & 1u);
-            }
-        }
-    }
+    // the bonds with an active end (listed by phase_reduce) take the full
+    // update; every other bond keeps its state, which the force phases have
+    // copied already when the frame writes a separate output, or which is in
+    // place; its history row is that state
+    const int nfb = *((volatile int*)a.fb_cnt);
+    for (int i = gtid; i < nfb; i += gsz) fracture_bond(a, F, scale, a.fb_list[i]);
+    if (a.h_intact)
+        for (int b = gtid; b < a.nb; b += gsz)
+            if (a.bstamp[b] != fstamp) a.h_intact[(size_t)F.f * a.nb + b] = F.src.intact[b] != 0 ? 1 : 0;
     for (int e = gtid; e < a.n; e += gsz) {
         if (a.h_pos) {
             typename vec2_of<T>::type p = ld2(F.dst.pos, e);
