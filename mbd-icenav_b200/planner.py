@@ -343,7 +343,15 @@ def rigid_terms(scene: PlanScene, Yn, out=None):
 
 
 class ScreenedScorer:
-    """Surrogate predictions for every candidate, the DEM for the best ``top_k``."""
+    """Surrogate predictions for every candidate, the DEM for the best ``top_k``.
+
+    Only the ``top_k`` candidates the surrogate ranks best are kept, with their
+    exact DEM costs; every other candidate gets +inf (weight 0 in the MBD
+    softmax), so that no cost the DEM has not checked can win a step.  The
+    check of each step is the relative regret of the surrogate's pick: the
+    exact cost of the candidate it ranks first against the best exact cost
+    among the ``top_k``.  Above ``max_rel_err`` the step falls back to scoring
+    every candidate with the plain DEM."""
 
     def __init__(self, scene: PlanScene, surrogate: Surrogate, Q: int, weights: CostWeights, top_k: int = 64,
                  max_rel_err: float = 0.05, **frame_kw):
@@ -357,29 +365,37 @@ class ScreenedScorer:
         self.dem_all = None
         self.frame_kw = frame_kw
         self.fallbacks = 0
-        self.rel_errs: List[float] = []
+        self.rel_errs: List[float] = []    # per step: the regret of the surrogate's pick
+        self.pred_errs: List[float] = []   # per step: mean relative error of the predicted totals (top_k)
         self.rollouts = 0
 
-    def __call__(self, Yn):
+    def predicted(self, Yn):
+        """(Q,) float64 predicted totals: rigid-path planner terms + predicted ice terms."""
         torch = _tm()
         planner = rigid_terms(self.scene, Yn)
         ice = self.sur.predict(self.scene, Yn)
         wp = torch.tensor(self.w.planner(), dtype=torch.float64, device=Yn.device)
         wi = torch.tensor(self.w.ice(), dtype=torch.float64, device=Yn.device)
-        pred = planner @ wp + ice @ wi
-        top = torch.topk(pred, self.k, largest=False).indices
+        return planner @ wp + ice @ wi
+
+    def __call__(self, Yn):
+        torch = _tm()
+        pred = self.predicted(Yn)
+        top = torch.topk(pred, self.k, largest=False).indices  # ascending: top[0] is the pick
         exact = self.dem_k(Yn[top].contiguous())
-        rel = float(((pred[top] - exact).abs() / exact.abs().clamp(min=1e-9)).mean().item())
+        best = exact.min()
+        rel = float(((exact[0] - best) / best.abs().clamp(min=1e-9)).item())
         self.rel_errs.append(rel)
+        self.pred_errs.append(float(((pred[top] - exact).abs() / exact.abs().clamp(min=1e-9)).mean().item()))
         self.rollouts += self.k
         if rel > self.max_rel_err:
-            # the surrogate is off on this population: the plain DEM scores all of it
+            # the surrogate's ranking is off on this population: the plain DEM scores all of it
             if self.dem_all is None:
                 self.dem_all = DemScorer(self.scene, self.Q, self.w, **self.frame_kw)
             self.fallbacks += 1
             self.rollouts += self.Q
             return self.dem_all(Yn)
-        cost = pred.clone()
+        cost = torch.full_like(pred, float("inf"))
         cost[top] = exact
         return cost
 
@@ -417,7 +433,8 @@ def mbd_plan(scorer, cfg: MBDConfig, device, seed: int = 0, Ybar_init=None):
         Yim1 = 1.0 / torch.sqrt(alphas[i]) * (Yi + (1.0 - alphas_bar[i]) * score)
         i_prev = max(i - 1, 0)
         Ybar = torch.clamp(Yim1 / torch.sqrt(alphas_bar[i_prev]), -1.0, 1.0)
-        metrics.append((costs.mean(), costs.min()))
+        fin = costs[torch.isfinite(costs)]  # a screened step leaves the unchecked candidates at +inf
+        metrics.append((fin.mean(), fin.min()))
         i -= 1
     return Ybar, [(float(a), float(b)) for a, b in metrics]
 
@@ -525,14 +542,29 @@ def generate_dataset(field, n_starts: int, per_start: int, horizon: int = 64, se
                    time.time() - t0)
 
 
+def mirror_rows(patches, extra):
+    """The mirror image of training rows about the ship's start axis, in place:
+    the patch flipped left-right (x about the ship), sway velocity, yaw rate,
+    cos(heading) and every yaw control negated.  The hull is symmetric, so the
+    mirrored scene has the same ice terms; the patch is centred on the ship."""
+    torch = _tm()
+    patches.copy_(torch.flip(patches, dims=[2]))
+    extra[:, 1] = -extra[:, 1]
+    extra[:, 2] = -extra[:, 2]
+    extra[:, 3] = -extra[:, 3]
+    extra[:, S.N_SHIP + 1::2] = -extra[:, S.N_SHIP + 1::2]
+
+
 def train_surrogate(data: Dataset, horizon: int = 64, epochs: int = 8, batch: int = 256, lr: float = 1e-3,
-                    seed: int = 0, holdout: float = 0.1, device="cuda"):
-    """Adam on fp32 master weights, BF16 tensor-core forward and backward;
-    returns (Surrogate, {"train_loss", "holdout_loss", "seconds", "steps"})."""
+                    seed: int = 0, holdout: float = 0.1, device="cuda", mirror: bool = True):
+    """Adam on fp32 master weights, BF16 tensor-core forward and backward.  Whole
+    starts are held out; half of every batch is mirrored (``mirror_rows``); the
+    weights of the epoch with the lowest held-out loss are kept.  Returns
+    (Surrogate, {"train_loss", "holdout_loss" (per epoch), "best_epoch",
+    "seconds", "steps", ...})."""
     torch = _tm()
     t0 = time.time()
     dev = torch.device(device)
-    N = int(data.extra.shape[0])
     raw = data.raw
     # target statistics on the log1p transform
     sc = torch.tensor(TARGET_SCALE, dtype=torch.float64, device=dev)
@@ -547,14 +579,17 @@ def train_surrogate(data: Dataset, horizon: int = 64, epochs: int = 8, batch: in
     train_idx = np.nonzero(~np.isin(so, list(hold)))[0]
     hold_idx = np.nonzero(np.isin(so, list(hold)))[0]
     net = S.SurrogateNet(horizon=horizon, device=dev, seed=seed)
+    sur = Surrogate(net, stats, data.patch_stats)
     Bz = batch
     ext_b = torch.empty((Bz, data.extra.shape[1]), dtype=torch.float32, device=dev)
     tgt_b = torch.empty((Bz, S.N_OUT), dtype=torch.float32, device=dev)
     pat_b = torch.empty((Bz, PATCH_CELLS, PATCH_CELLS, 1), dtype=torch.bfloat16, device=dev)
     grad = torch.empty((Bz, S.OUT_ROWS), dtype=torch.bfloat16, device=dev)
     loss = torch.empty(1, dtype=torch.float32, device=dev)
+    half = Bz // 2
     steps = 0
-    losses = []
+    losses, hlosses = [], []
+    best, best_ep, snap = float("inf"), -1, None
     for ep in range(epochs):
         perm = rng.permutation(train_idx)
         for b0 in range(0, len(perm) - Bz + 1, Bz):
@@ -563,16 +598,28 @@ def train_surrogate(data: Dataset, horizon: int = 64, epochs: int = 8, batch: in
             sg_ops.gather_rows(data.extra, idx, ext_b)
             sg_ops.gather_rows(tgt, idx, tgt_b)
             sg_ops.gather_rows(data.patches.view(n_starts, -1), sidx, pat_b.view(Bz, -1))
+            if mirror:
+                mirror_rows(pat_b[:half], ext_b[:half])
             out = net.forward(pat_b, ext_b, keep=True)
             sg_ops.mse(out, tgt_b, S.N_OUT, grad, loss)
             net.backward(grad)
             net.adam_step(lr * (0.5 * (1 + math.cos(math.pi * ep / max(epochs, 1)))))
             steps += 1
         losses.append(float(loss.item()))
+        hl = holdout_error(sur, data, hold_idx, tgt) if len(hold_idx) else float("nan")
+        hlosses.append(hl)
+        if hl < best:
+            best, best_ep = hl, ep
+            snap = [(p.p.clone(), p.b.clone()) for p in net.params()]
+    if snap is not None:
+        for layer, (pw, pb) in zip(net.params(), snap):
+            layer.p.copy_(pw)
+            layer.b.copy_(pb)
+            sg_ops.to_bf16(layer.p, out=layer.w)
+            sg_ops.transpose(layer.w, out=layer.wt)
     sg_ops.error_flag(dev).check()
-    sur = Surrogate(net, stats, data.patch_stats)
-    hl = holdout_error(sur, data, hold_idx, tgt) if len(hold_idx) else float("nan")
-    return sur, {"train_loss": losses, "holdout_loss": hl, "seconds": time.time() - t0, "steps": steps,
+    return sur, {"train_loss": losses, "holdout_loss": hlosses, "best_epoch": best_ep,
+                 "holdout_best": best, "seconds": time.time() - t0, "steps": steps,
                  "train_samples": int(len(train_idx)), "holdout_samples": int(len(hold_idx))}
 
 

@@ -4,7 +4,9 @@
   recorded field) and vs the float64 oracle (every IceState / ShipState field);
 * float32 single frames from identical input states vs the float32 oracle:
   every float field per entry within 1e-5 of its own change over the frame
-  (floor: fp32 rounding of the value), masks and the contact mask bit-equal;
+  (floor: fp32 rounding of the value, and twice the fp32 oracle's own error
+  against the float64 oracle from the same input), masks and the contact mask
+  bit-equal;
 * the ice-ice contact set of every substep bit-equal to the oracle's
   (overlap > 0 and distance > 1e-6, jax_simulation.py:127-131);
 * scan == frame loop and persistent == phased launches, bit for bit;
@@ -79,10 +81,14 @@ def test_f64_free_run_matches_reference(prefix, golden64):
 @pytest.mark.parametrize("prefix", ["hex", "small", "window"])
 def test_f32_single_frames_match_oracle(prefix, golden32):
     """Same fp32 input state -> one frame on GPU and in the fp32 oracle; every
-    field per entry within 1e-5 of its own change over the frame."""
+    field per entry within 1e-5 of its own change over the frame, or, where the
+    fp32 oracle itself is farther than that from the float64 oracle (a sum
+    that cancels, such as a torque whose normal-force terms balance), within
+    twice the fp32 oracle's own error."""
     g = golden32
     fs = gpu_frame_step(g, prefix, torch.float32)
     o = make_oracle(g, prefix, np.float32, pair_mode="grid")
+    o64 = make_oracle(g, prefix, np.float64, pair_mode="grid")  # the fp32 reference's own error
     st, sh = initial_state(g, prefix, np.float32)
     n_frames = g[f"{prefix}_pos"].shape[0]
     checked = 0
@@ -92,10 +98,14 @@ def test_f32_single_frames_match_oracle(prefix, golden32):
         c = lambda a: np.asarray(a, np.float64).astype(np.float32)
         o_st, o_sh, o_diag = o.frame_step(st, sh, c(sp), c(spn), c(vw), st.dpdem_floe_eligible, c(vws))
         if prefix != "small" or f % 5 == 0 or (o_diag["pen_max"] > 0).any():
+            d64 = lambda t: type(t)(*[np.asarray(a, np.float64) if np.asarray(a).dtype != bool else a for a in t])
+            o64_st, o64_sh, _ = o64.frame_step(d64(st), d64(sh), c(sp), c(spn), c(vw), st.dpdem_floe_eligible,
+                                               c(vws))
             gst, gsh = to_gpu_state(st, sh, torch.float32)
             r_st, r_sh, r_diag = _frame(fs, gst, gsh, g, prefix, f, torch.float32)
             ice, ship = to_np_state(r_st, r_sh)
-            w = assert_frame_matches(ice, ship, o_st, o_sh, st, sh, r_diag, o_diag, where=f"frame {f}")
+            w = assert_frame_matches(ice, ship, o_st, o_sh, st, sh, r_diag, o_diag, where=f"frame {f}",
+                                     o_ice64=o64_st, o_ship64=o64_sh)
             for k, v in w.items():
                 worst[k] = max(worst.get(k, 0.0), v)
             checked += 1

@@ -7,13 +7,15 @@ skin) first advances the field with the ship inside it, then one frame at a
 time is checked against the oracle from the identical fp32 state:
 
 * every IceState / ShipState field per entry within 1e-5 of its own change
-  over the frame (floor: fp32 rounding of the value), masks bit-equal;
+  over the frame (floor: fp32 rounding of the value, and twice the fp32
+  oracle's own error against the float64 oracle from the same input), masks
+  bit-equal;
 * the ice-ice contact set of every substep bit-equal to the oracle's
   all-pairs set (restated broad phase: exact, see the oracle's header);
 * the ship contact mask, force magnitudes and ship force.
 
 The medium field (12k elements, 0.2 m/s current) gets the same check.  The
-oracle's frame on the large field takes ~12 s on one core.
+oracle's frame on the large field takes ~12 s on one core (fp32 and fp64 each).
 """
 import os
 import sys
@@ -59,6 +61,7 @@ def _check_field(name, advance, frames):
     # advance with the ship in the field (the bench's own frames, one launch)
     st, sh, _ = fs.scan_segment(st, sh, sp[:advance], vw_row.expand(advance, n, 2).contiguous(), history=False)
     o = _oracle(field, np.float32)
+    o64 = _oracle(field, np.float64)  # the fp32 reference's own error, per entry
     rec = fs.record_contacts(capacity=1 << 22)
     vw_np = vw_row.cpu().numpy()
     sp_np = sp.cpu().numpy()
@@ -69,9 +72,13 @@ def _check_field(name, advance, frames):
         o_sh_in = OShip(*ship_in)
         o.contact_log = []
         o_st, o_sh, o_diag = o.frame_step(o_in, o_sh_in, sp_np[f, :3], sp_np[f, 3:], vw_np, o_in.dpdem_floe_eligible)
+        d64 = lambda t: type(t)(*[np.asarray(a, np.float64) if np.asarray(a).dtype != bool else a for a in t])
+        o64_st, o64_sh, _ = o64.frame_step(d64(o_in), d64(o_sh_in), sp_np[f, :3], sp_np[f, 3:], vw_np,
+                                           o_in.dpdem_floe_eligible)
         st, sh, diag = fs(st, sh, sp[f, :3], sp[f, 3:], vw_row.contiguous(), st.dpdem_floe_eligible)
         ice, ship = to_np_state(st, sh)
-        worst = assert_frame_matches(ice, ship, o_st, o_sh, o_in, o_sh_in, diag, o_diag, where=f"{name} frame {f}")
+        worst = assert_frame_matches(ice, ship, o_st, o_sh, o_in, o_sh_in, diag, o_diag, where=f"{name} frame {f}",
+                                     o_ice64=o64_st, o_ship64=o64_sh)
         sets, raw = rec.substeps(fs.n_ice_steps)
         n_contacts += contact_sets_match(sets, raw, o.contact_log, o_st.elem_active, where=f"{name} frame {f}")
         n_active.append(int(o_st.elem_active.sum()))

@@ -89,9 +89,11 @@ def test_shared_window_candidates_equal_their_runs_alone_and_ice_terms(medium):
 
 
 def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
-    """A surrogate-screened cost batch: the top_k candidates get their exact DEM
-    costs, the rest the prediction; with max_rel_err = 0 every step falls back
-    to the DEM for all candidates (equal to the plain DEM batch)."""
+    """A surrogate-screened cost batch: the top_k candidates the surrogate ranks
+    best get their exact DEM costs, every other candidate +inf (no unchecked
+    cost can win a step); the step's check is the regret of the surrogate's
+    pick; with a negative bound every step falls back to the DEM for all
+    candidates (equal to the plain DEM batch)."""
     import os
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -112,15 +114,15 @@ def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
     exact = plain(Yn)
     scr = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, max_rel_err=float("inf"))
     cost = scr(Yn)
-    pred_ice = sur.predict(sc, Yn)
-    pred = planner.rigid_terms(sc, Yn) @ torch.tensor(w.planner(), dtype=torch.float64, device=DEV) + \
-        pred_ice @ torch.tensor(w.ice(), dtype=torch.float64, device=DEV)
+    pred = scr.predicted(Yn)
     top = torch.topk(pred, k, largest=False).indices
-    assert torch.allclose(cost[top], exact[top], rtol=0, atol=0)
+    assert torch.equal(cost[top], exact[top])
     rest = torch.ones(Q, dtype=torch.bool, device=DEV)
     rest[top] = False
-    assert torch.allclose(cost[rest], pred[rest])
-    fb = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, max_rel_err=0.0)
+    assert torch.isinf(cost[rest]).all() and torch.isfinite(cost[top]).all()
+    regret = (exact[top[0]] - exact[top].min()) / exact[top].min().abs()
+    assert scr.rel_errs[-1] == pytest.approx(float(regret), rel=1e-12, abs=1e-15) and scr.fallbacks == 0
+    fb = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, max_rel_err=-1.0)
     assert torch.equal(fb(Yn), exact) and fb.fallbacks == 1
     # a short plan runs end to end with both cost batches
     cfg = planner.MBDConfig(horizon=16, n_sample=Q, n_diffuse=3, top_k=k)

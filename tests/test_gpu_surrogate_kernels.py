@@ -84,7 +84,8 @@ def test_gemm_repeated_calls_are_bit_identical():
 @pytest.mark.parametrize("C", [1, 32])
 def test_im2col_gemm_is_conv2d_and_col2im_is_its_adjoint(C):
     """3x3 stride-2 padding-1 convolution as im2col + GEMM equals torch's conv2d
-    (fp32, same bf16 values); col2im is the adjoint: <im2col(x), y> = <x, col2im(y)>."""
+    (fp32, same bf16 values); col2im is the adjoint of im2col: it equals the
+    gradient autograd takes through the same patches (then rounded to bf16)."""
     ops = _ops()
     g = torch.Generator().manual_seed(C)
     Bn, H, W, Co = 3, 16, 12, 24
@@ -102,8 +103,6 @@ def test_im2col_gemm_is_conv2d_and_col2im_is_its_adjoint(C):
     dcols = torch.randn(cols.shape, generator=g).to(DEV)
     dcols[:, 9 * C:] = 0
     dX = ops.col2im(dcols, (Bn, H, W, C), kpad)
-    lhs = (cols.float() * dcols).sum().item()
-    rhs = (X.float() * dX.float()).sum().item()
     # dX is rounded to bf16: compare against the fp32 adjoint computed by autograd
     Xr = X.float().clone().requires_grad_(True)
     cols_t = torch.nn.functional.unfold(Xr.permute(0, 3, 1, 2), 3, padding=1, stride=2)  # (B, C*9, L) in (c, ky, kx)
@@ -112,7 +111,6 @@ def test_im2col_gemm_is_conv2d_and_col2im_is_its_adjoint(C):
     (perm * dcols[:, :9 * C]).sum().backward()
     np.testing.assert_allclose(dX.float().cpu().numpy(), Xr.grad.to(torch.bfloat16).float().cpu().numpy(),
                                rtol=1.0 / 128, atol=1e-6)
-    assert abs(lhs - rhs) <= 1e-2 * max(abs(lhs), 1.0)
 
 
 def test_col2im_applies_relu_mask():
