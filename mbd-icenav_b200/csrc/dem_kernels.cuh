@@ -1471,9 +1471,7 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             const int2 ent0 = a.bslot[sl];
             const int2 ent1 = two ? a.bslot[sl + 1] : ent0;
             const int b0 = ent0.x & 0x7fffffff, b1 = ent1.x & 0x7fffffff;
-            // the bond has an active end this frame; the first stamper lists it
-            if (atomicExch(&a.bstamp[b0], fstamp) != fstamp) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b0;
-            if (two && atomicExch(&a.bstamp[b1], fstamp) != fstamp) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b1;
+
             const bool in0 = F.src.intact[b0] != 0, in1 = F.src.intact[b1] != 0;
             const bool sa0 = F.src.active[ent0.y] != 0, sa1 = F.src.active[ent1.y] != 0;
             const int fo0 = a.floe_of[ent0.y], fo1 = a.floe_of[ent1.y];
@@ -1482,6 +1480,12 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             const T k0 = a.slot_stiff[sl], k1 = two ? a.slot_stiff[sl + 1] : k0;
             const bool ao0 = sa0 || a.fcoll[fo0];
             const bool ao1 = sa1 || a.fcoll[fo1];
+            // the bond has an active end this frame; it is listed once, by its
+            // active end of lower index (e, unless the partner is active and lower)
+            a.bstamp[b0] = fstamp;
+            a.bstamp[b1] = fstamp;
+            if (!(ao0 && ent0.y < e)) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b0;
+            if (two && !(ao1 && ent1.y < e)) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b1;
             if (!in0 || (two && !in1)) a.crack[e] = 1;
             SlotRec<T> q;
             q.o = (ent0.x < 0) ? (int)((unsigned)ent0.y | 0x80000000u) : ent0.y;
