@@ -731,21 +731,24 @@ def run_surrogate(args, rank: int, world: int):
                              "rel_cost_err": abs(cs - cp) / max(abs(cp), 1e-9), "fallbacks": scr.fallbacks - n_fb0,
                              "topk_rel_err_mean": float(np.mean(scr.rel_errs)), "window": int(len(sc.window)),
                              "work_split": [split_plain, split_k]})
+                sys.stderr.write(f"plan {si}: {json.dumps(rows[-1])}\n")
             plain.batch.frame_step.close()
             scr.dem_k.batch.frame_step.close()
             if scr.dem_all is not None:
                 scr.dem_all.batch.frame_step.close()
             del plain, scr
-    # tensor-pipe figure: the network forward on one plan's population (8192 rows), timed alone
+    # tensor-pipe figure: the screening's own network work on one plan's
+    # population, the head over n_sample rows after one encoder pass, timed alone
     sc = planner.make_scene(field, starts[-1], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats)
     Yn = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.5, -1, 1)
     ext = planner.features(sc, Yn)
-    pat = sc.patch.expand(cfg.n_sample, -1, -1, -1).contiguous()
+    rows0 = torch.zeros(cfg.n_sample, dtype=torch.int32, device=device)
+    enc = sur.net.encode(sc.patch, tag="bench_enc")
     for _ in range(3):
-        sur.net.forward(pat, ext)
-    _, t_fwd = timed(lambda: [sur.net.forward(pat, ext) for _ in range(10)])
+        sur.net.head(enc, ext, enc_row=rows0, tag="bench_head")
+    _, t_fwd = timed(lambda: [sur.net.head(enc, ext, enc_row=rows0, tag="bench_head") for _ in range(20)])
     fl = S.flops_per_sample(H)
-    tflops = 10 * cfg.n_sample * (fl["encoder"] + fl["mlp"]) / t_fwd / 1e12
+    tflops = 20 * cfg.n_sample * fl["mlp"] / t_fwd / 1e12
     sg_ops.error_flag(device).check()
     if rank != 0:
         return None
@@ -784,7 +787,8 @@ def run_surrogate(args, rank: int, world: int):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": tflops / peak_tf, "peak_kind": f"{peak_kind} bf16 dense",
-                     "what": f"surrogate forward on {cfg.n_sample} rows (per-sample encoder), 10 launches timed",
+                     "what": f"surrogate head (3 x 512 MLP + output, bf16 tcgen05 GEMMs) on {cfg.n_sample} rows "
+                             f"after one encoder pass: the screening's network work per MBD step, 20 passes timed",
                      "traffic": None},
         "e2e": {"value": value, "unit": SUR_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
                 "note": "plans read their controls from device buffers; the plan's cost comes back"},
@@ -999,9 +1003,9 @@ def main():
                     help="element numbering: as generated (by floe) or Morton order of centroids")
     ap.add_argument("--phase-times", action="store_true",
                     help="after the run, time one profiled frame per phase (device clock) to stderr")
-    ap.add_argument("--sur-starts", type=int, default=48, help="training starts (--config surrogate)")
-    ap.add_argument("--sur-per-start", type=int, default=2048, help="DEM rollouts per training start")
-    ap.add_argument("--sur-epochs", type=int, default=6)
+    ap.add_argument("--sur-starts", type=int, default=1024, help="training starts (--config surrogate)")
+    ap.add_argument("--sur-per-start", type=int, default=256, help="DEM rollouts per training start")
+    ap.add_argument("--sur-epochs", type=int, default=10)
     ap.add_argument("--sur-samples", type=int, default=8192, help="MBD samples per reverse step")
     ap.add_argument("--sur-iters", type=int, default=16, help="MBD reverse steps per plan")
     ap.add_argument("--sur-top-k", type=int, default=64, help="candidates re-scored by the DEM per step")

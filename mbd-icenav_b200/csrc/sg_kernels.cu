@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(128, 1)
     auto empty = [&](int s) { return bar0 + 8u * (uint32_t)(kStages + s); };
     const uint32_t done = bar0 + 8u * (uint32_t)(2 * kStages);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;  // M tiles on x: no 65535 limit on M
     const int nk = (g.K + kBK - 1) / kBK;
 
     if (threadIdx.x == 0) {
@@ -213,7 +213,7 @@ int launch_gemm(const GemmArgs& g, const void* A, int lda, const void* B, int ld
         attr = cudaFuncSetAttribute(gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     });
     if (attr != cudaSuccess) return SG_ERR_CUDA;
-    dim3 grid((g.N + BN - 1) / BN, (g.M + kBM - 1) / kBM);
+    dim3 grid((g.M + kBM - 1) / kBM, (g.N + BN - 1) / BN);
     gemm_kernel<BN><<<grid, 128, smem, st>>>(ta, tb, g);
     return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
 }
@@ -431,7 +431,7 @@ int sg_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const v
     if (lda < K || ldb < K || (lda % 8) || (ldb % 8) || !aligned16(A) || !aligned16(B)) return SG_ERR_INVALID;
     if (ldd < N || (d_dtype != SG_OUT_F32 && d_dtype != SG_OUT_BF16)) return SG_ERR_INVALID;
     if (mask && ldm < N) return SG_ERR_INVALID;
-    if ((M + kBM - 1) / kBM > 65535) return SG_ERR_INVALID;
+    if ((N + 63) / 64 > 65535) return SG_ERR_INVALID;
     GemmArgs g{M, N, K, D, ldd, d_dtype == SG_OUT_BF16 ? 1 : 0, bias, relu ? 1 : 0,
                reinterpret_cast<const __nv_bfloat16*>(mask), ldm, err};
     cudaStream_t st = (cudaStream_t)stream;
