@@ -1,7 +1,7 @@
 // sg_kernels.cu — device kernels of the screening surrogate (include/surrogate_b200.h).
 //
 // The GEMM is the Blackwell tensor-core path: a 128 x BN output tile per CTA,
-// K consumed 64 bf16 at a time through a STAGES-deep ring of shared-memory
+// K consumed 64 bf16 at a time through a 6- or 8-deep ring of shared-memory
 // buffers that TMA fills (128-byte swizzled, the layout tcgen05 reads), one
 // elected thread issuing tcgen05.mma into an fp32 accumulator in tensor
 // memory, and all four warps reading it back (tcgen05.ld) for the fused
@@ -23,7 +23,11 @@ namespace {
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;  // bf16 per 128-byte swizzled row
-constexpr int kStages = 4;
+// stages of the operand ring: enough 64-deep K slices in flight to cover a
+// TMA round trip behind the MMAs of the slices before it (32 KB a stage at
+// BN = 128, 24 KB at BN = 64; both rings stay under 200 KB of shared memory)
+template <int BN>
+__host__ __device__ constexpr int stages_of() { return BN >= 128 ? 6 : 8; }
 
 struct GemmArgs {
     int M, N, K;
@@ -38,7 +42,7 @@ struct GemmArgs {
 
 template <int BN>
 constexpr size_t gemm_smem_bytes() {
-    return 1024 + (size_t)kStages * (kBM * kBK * 2 + BN * kBK * 2) + 256;
+    return 1024 + (size_t)stages_of<BN>() * (kBM * kBK * 2 + BN * kBK * 2) + 256;
 }
 
 template <int BN>
@@ -47,6 +51,7 @@ __global__ void __launch_bounds__(128, 1)
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                            ~static_cast<uintptr_t>(1023));
+    constexpr int kStages = stages_of<BN>();
     constexpr uint32_t kABytes = kBM * kBK * 2, kBBytes = BN * kBK * 2, kStage = kABytes + kBBytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * kStage);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);

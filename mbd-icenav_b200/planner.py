@@ -18,10 +18,10 @@ Two cost batches:
   transferred, hull impulse, bonds broken; ``dem_rollout_ice_terms``);
 * ``ScreenedScorer`` — the rigid-ship rollout (``dem_ship_rollout``) for the
   planner's components plus the surrogate's prediction of the ice terms for
-  every candidate; the ``top_k`` best are then re-scored by the DEM and those
-  exact costs replace the predictions.  When the prediction error on them
-  (mean relative error of the total cost) exceeds ``max_rel_err``, the step
-  falls back to scoring every candidate with the DEM.
+  every candidate; the ``top_k`` best and a random check set are re-scored by
+  the DEM and only they keep a cost.  When the check set beats the screened
+  best by more than ``max_rel_err``, the step falls back to scoring every
+  candidate with the DEM.
 
 The reference has no DEM rollout and no surrogate; its planners score
 rigid-ship rollouts on a static costmap.  Torch tensors hold the device
@@ -343,29 +343,35 @@ def rigid_terms(scene: PlanScene, Yn, out=None):
 
 
 class ScreenedScorer:
-    """Surrogate predictions for every candidate, the DEM for the best ``top_k``.
+    """Surrogate predictions for every candidate, the DEM for the best ``top_k``
+    and for ``n_check`` random others.
 
-    Only the ``top_k`` candidates the surrogate ranks best are kept, with their
-    exact DEM costs; every other candidate gets +inf (weight 0 in the MBD
-    softmax), so that no cost the DEM has not checked can win a step.  The
-    check of each step is the relative regret of the surrogate's pick: the
-    exact cost of the candidate it ranks first against the best exact cost
-    among the ``top_k``.  Above ``max_rel_err`` the step falls back to scoring
-    every candidate with the plain DEM."""
+    The ``top_k`` candidates the surrogate ranks best are rolled out by the DEM
+    together with ``n_check`` candidates drawn at random from the rest (the
+    held-out check).  Only these keep a cost, their exact DEM cost; every other
+    candidate gets +inf (weight 0 in the MBD softmax), so no cost the DEM has
+    not checked can win a step.  The check of a step is the relative amount by
+    which the best random candidate beats the best screened one (0 when it
+    does not): screening that misses better candidates than it keeps shows up
+    there.  Above ``max_rel_err`` the step falls back to scoring every
+    candidate with the plain DEM."""
 
     def __init__(self, scene: PlanScene, surrogate: Surrogate, Q: int, weights: CostWeights, top_k: int = 64,
-                 max_rel_err: float = 0.05, **frame_kw):
+                 max_rel_err: float = 0.05, n_check: int = 64, seed: int = 0, **frame_kw):
+        torch = _tm()
         self.scene = scene
         self.sur = surrogate
         self.w = weights
         self.Q = Q
         self.k = top_k
+        self.n_check = max(0, min(n_check, Q - top_k))
         self.max_rel_err = max_rel_err
-        self.dem_k = DemScorer(scene, top_k, weights, **frame_kw)
+        self.dem_k = DemScorer(scene, top_k + self.n_check, weights, **frame_kw)
         self.dem_all = None
         self.frame_kw = frame_kw
+        self.gen = torch.Generator(device=scene.device).manual_seed(seed)
         self.fallbacks = 0
-        self.rel_errs: List[float] = []    # per step: the regret of the surrogate's pick
+        self.rel_errs: List[float] = []    # per step: how much the best random candidate beats the screened best
         self.pred_errs: List[float] = []   # per step: mean relative error of the predicted totals (top_k)
         self.rollouts = 0
 
@@ -378,25 +384,37 @@ class ScreenedScorer:
         wi = torch.tensor(self.w.ice(), dtype=torch.float64, device=Yn.device)
         return planner @ wp + ice @ wi
 
+    def selection(self, pred):
+        """(screened top_k indices ascending by prediction, random check indices)."""
+        torch = _tm()
+        order = torch.argsort(pred)
+        top, rest = order[:self.k], order[self.k:]
+        pick = torch.randperm(rest.numel(), generator=self.gen, device=pred.device)[:self.n_check]
+        return top, rest[pick]
+
     def __call__(self, Yn):
         torch = _tm()
         pred = self.predicted(Yn)
-        top = torch.topk(pred, self.k, largest=False).indices  # ascending: top[0] is the pick
-        exact = self.dem_k(Yn[top].contiguous())
-        best = exact.min()
-        rel = float(((exact[0] - best) / best.abs().clamp(min=1e-9)).item())
-        self.rel_errs.append(rel)
-        self.pred_errs.append(float(((pred[top] - exact).abs() / exact.abs().clamp(min=1e-9)).mean().item()))
-        self.rollouts += self.k
-        if rel > self.max_rel_err:
-            # the surrogate's ranking is off on this population: the plain DEM scores all of it
+        top, chk = self.selection(pred)
+        idx = torch.cat([top, chk])
+        exact = self.dem_k(Yn[idx].contiguous())
+        e_top, e_chk = exact[:self.k], exact[self.k:]
+        best = e_top.min()
+        miss = 0.0
+        if self.n_check:
+            miss = float(((best - e_chk.min()) / e_chk.min().abs().clamp(min=1e-9)).clamp(min=0.0).item())
+        self.rel_errs.append(miss)
+        self.pred_errs.append(float(((pred[top] - e_top).abs() / e_top.abs().clamp(min=1e-9)).mean().item()))
+        self.rollouts += idx.numel()
+        if miss > self.max_rel_err:
+            # screening misses better candidates than it keeps: the plain DEM scores all of them
             if self.dem_all is None:
                 self.dem_all = DemScorer(self.scene, self.Q, self.w, **self.frame_kw)
             self.fallbacks += 1
             self.rollouts += self.Q
             return self.dem_all(Yn)
         cost = torch.full_like(pred, float("inf"))
-        cost[top] = exact
+        cost[idx] = exact
         return cost
 
 
