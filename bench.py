@@ -255,13 +255,19 @@ class DirectFrames:
     def state(self):
         return self.bufs[self.cur]
 
-    def frame(self, fr: int):
-        """Enqueue one frame with setpoint row ``fr``; returns the call's status."""
+    def frame(self, fr: int, io=None):
+        """Enqueue one frame with setpoint row ``fr``; returns the call's status.
+        ``io = (setpoints, v_water, history)``: the frame reads its setpoint row
+        and field from those device pointers instead and writes its history
+        rows through that ``DemHistory``."""
         C, a, b = self.C, self.cur, 1 - self.cur
+        if io is None:
+            sp, vw, hist = C.c_void_p(self.sp_base + fr * self.sp_row), self.vw_ptr, None
+        else:
+            sp, vw, hist = io[0], io[1], C.byref(io[2])
         rc = self.fs.lib.dem_scan_segment(self.fs._h, C.byref(self.c_ice[a]), C.byref(self.c_ice[b]),
-                                          C.byref(self.c_ship[a]), C.byref(self.c_ship[b]), 1,
-                                          C.c_void_p(self.sp_base + fr * self.sp_row), self.vw_ptr, None, None,
-                                          self.stream)
+                                          C.byref(self.c_ship[a]), C.byref(self.c_ship[b]), 1, sp, vw, None,
+                                          hist, self.stream)
         self.cur = b
         return rc
 
@@ -382,10 +388,11 @@ def run_ours(args, rank: int, world: int):
     total_max = frame_max * K
     value = world * n * N_SUB / frame_max
 
-    # end to end through the public API with host buffers: every step uploads
-    # its setpoint row and current field from pinned host memory and downloads
-    # its history rows, all inside the timed region.  A copy stream overlaps the
-    # upload of step i+1 and the download of step i-1 with step i (inputs are
+    # end to end through the C ABI with host buffers: every step uploads its
+    # setpoint row and current field from pinned host memory, runs one
+    # dem_scan_segment frame and downloads its history rows, all inside the
+    # timed region.  A copy stream overlaps the upload of step i+1 and the
+    # download of step i-1 with step i (inputs and history rows are
     # double-buffered on the device, results on the host).
     E = args.e2e_steps
     sp_h = sp_all[fr:fr + E2E_WARMUP + E2E_WINDOWS * E + 1].cpu().pin_memory()
@@ -394,20 +401,18 @@ def run_ours(args, rank: int, world: int):
     vw_d = [torch.empty_like(vw) for _ in range(2)]
     h2d = sp_d[0].numel() * sp_d[0].element_size() + vw_d[0].numel() * vw_d[0].element_size()
     copy = torch.cuda.Stream(device)
-    # one untimed step sizes the pinned result buffers
-    sp_d[0].copy_(sp_h[0:1])
-    vw_d[0].copy_(vw_h)
-    st, sh, hist = fs.scan_segment(st, sh, sp_d[0], vw_d[0], history=True, check=False)
-    outs_h = [[torch.empty(h.shape, dtype=h.dtype, pin_memory=True) for h in hist] for _ in range(2)]
-    d2h = sum(h.numel() * h.element_size() for h in hist)
-    del hist
+    import ctypes as C
+    hist_d = [fs.alloc_history(1) for _ in range(2)]
+    c_hist = [_abi_mod().DemHistory(*[C.c_void_p(int(t.data_ptr())) for t in h]) for h in hist_d]
+    io = [(C.c_void_p(int(sp_d[b].data_ptr())), C.c_void_p(int(vw_d[b].data_ptr())), c_hist[b]) for b in range(2)]
+    outs_h = [[torch.empty(h.shape, dtype=h.dtype, pin_memory=True) for h in hist_d[0]] for _ in range(2)]
+    d2h = sum(h.numel() * h.element_size() for h in hist_d[0])
     torch.cuda.synchronize()
     ev_in = [torch.cuda.Event() for _ in range(2)]
     ev_done = [torch.cuda.Event() for _ in range(2)]
 
     def e2e_steps(r0: int, count: int) -> float:
         """`count` steps on setpoint rows r0, r0 + 1, ...; returns their device time [s]."""
-        nonlocal st, sh
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -420,7 +425,9 @@ def run_ours(args, rank: int, world: int):
             b = i & 1
             flush.fill_(i & 0xFF)  # evict L2 before every step, as in the device-timed loop
             stream.wait_event(ev_in[b])
-            st, sh, hist = fs.scan_segment(st, sh, sp_d[b], vw_d[b], history=True, check=False)
+            rc_call = direct.frame(0, io[b])
+            if rc_call != 0:
+                raise RuntimeError(f"dem_scan_segment returned {rc_call}: {fs._error()}")
             ev_done[b].record(stream)
             with torch.cuda.stream(copy):
                 if i + 1 < count:
@@ -430,9 +437,8 @@ def run_ours(args, rank: int, world: int):
                     vw_d[1 - b].copy_(vw_h, non_blocking=True)
                     ev_in[1 - b].record(copy)
                 copy.wait_event(ev_done[b])
-                for hh, hd in zip(outs_h[b], hist):
+                for hh, hd in zip(outs_h[b], hist_d[b]):
                     hh.copy_(hd, non_blocking=True)
-                    hd.record_stream(copy)
         stream.wait_stream(copy)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -460,6 +466,7 @@ def run_ours(args, rank: int, world: int):
     info = fs.info()
     if args.phase_times and args.launch == "persistent":
         print_phase_times(fs, st, sh, sp_all[fr:fr + 1], vw)
+        print_phase_times(fs, st, sh, sp_all[fr:fr + 1], vw, flush=flush)
 
     if rank != 0:
         return None
@@ -497,7 +504,9 @@ def run_ours(args, rank: int, world: int):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": E,
                 "windows": [world * n * N_SUB * E / w for w in windows],
-                "value_of": f"median of {E2E_WINDOWS} consecutive timed windows of {E} steps"},
+                "value_of": f"median of {E2E_WINDOWS} consecutive timed windows of {E} steps",
+                "path": "pinned host rows -> device, one dem_scan_segment frame through the C ABI, history "
+                        "rows -> pinned host, per step"},
         "gpu_launches": K if args.launch == "persistent" else None,
         "clocks": clk.summary(),
     }
@@ -691,7 +700,7 @@ def run_surrogate(args, rank: int, world: int):
     H = args.horizon
     t0 = time.time()
     data = planner.generate_dataset(field, n_starts=args.sur_starts, per_start=args.sur_per_start, horizon=H,
-                                    seed=args.seed + 100 * rank, device=device)
+                                    seed=args.seed + 100 * rank, device=device, scenes=args.sur_scenes)
     gen_s = time.time() - t0
     sur, info = planner.train_surrogate(data, horizon=H, epochs=args.sur_epochs, batch=256, device=device,
                                         seed=args.seed)
@@ -699,7 +708,7 @@ def run_surrogate(args, rank: int, world: int):
                             top_k=args.sur_top_k)
     w = planner.CostWeights()
     rng = np.random.default_rng(args.seed + 7777)
-    starts = planner.sample_starts(field, args.steps + args.warmup, rng, H)
+    starts = planner.scene_starts(field, args.sur_scenes, args.steps + args.warmup, rng, H)
     stream = torch.cuda.current_stream(device)
 
     def timed(fn):
@@ -713,23 +722,30 @@ def run_surrogate(args, rank: int, world: int):
 
     rows = []
     with ClockSampler(device.index) as clk:
-        for si, e0 in enumerate(starts):
-            sc = planner.make_scene(field, e0, (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats)
+        for si, (e0, rem) in enumerate(starts):
+            sc = planner.make_scene(field, e0, (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats,
+                                    removed=rem)
             plain = planner.DemScorer(sc, cfg.n_sample, w)
             scr = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err,
-                                         n_check=cfg.top_k, seed=si)
+                                         n_check=args.sur_check, seed=si)
+            # the configuration's own top-64, for comparison
+            scr64 = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=64, max_rel_err=cfg.max_rel_err,
+                                           n_check=args.sur_check, seed=si)
             # untimed: each DEM batch's work split, tuned on candidates like a plan's
             Yt = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.7, -1, 1)
             split_plain, _ = plain.autotune(Yt)
             split_k, _ = scr.dem_k.autotune(Yt[:scr.dem_k.Q].contiguous())
+            scr64.dem_k.autotune(Yt[:scr64.dem_k.Q].contiguous())
             (Yp, _), tp = timed(lambda: planner.mbd_plan(plain, cfg, device, seed=si))
             n_fb0 = scr.fallbacks
             (Ys, _), ts = timed(lambda: planner.mbd_plan(scr, cfg, device, seed=si))
+            (Ys64, _), ts64 = timed(lambda: planner.mbd_plan(scr64, cfg, device, seed=si))
             # the plain planner again with other samples: its own spread of plan costs
             Yp2, _ = planner.mbd_plan(plain, cfg, device, seed=si + 1000)
             cp = planner.plan_cost(sc, Yp, scr.dem_k)
             cs = planner.plan_cost(sc, Ys, scr.dem_k)
             cp2 = planner.plan_cost(sc, Yp2, scr.dem_k)
+            cs64 = planner.plan_cost(sc, Ys64, scr.dem_k)
             if si >= args.warmup:
                 rows.append({"plain_s": tp, "screened_s": ts, "plain_cost": cp, "screened_cost": cs,
                              "plain_cost_other_seed": cp2,
@@ -738,18 +754,23 @@ def run_surrogate(args, rank: int, world: int):
                              "fallbacks": scr.fallbacks - n_fb0,
                              "check_miss_max": float(np.max(scr.rel_errs)),
                              "pred_rel_err_mean": float(np.mean(scr.pred_errs)), "window": int(len(sc.window)),
-                             "work_split": [split_plain, split_k]})
+                             "work_split": [split_plain, split_k],
+                             "top64": {"screened_s": ts64, "screened_cost": cs64,
+                                       "rel_cost_err": abs(cs64 - cp) / max(abs(cp), 1e-9),
+                                       "fallbacks": scr64.fallbacks, "check_miss_max": float(np.max(scr64.rel_errs))}})
                 sys.stderr.write(f"plan {si}: {json.dumps(rows[-1])}\n")
             plain.batch.frame_step.close()
-            scr.dem_k.batch.frame_step.close()
-            if scr.dem_all is not None:
-                scr.dem_all.batch.frame_step.close()
-            del plain, scr
+            for z in (scr, scr64):
+                z.dem_k.batch.frame_step.close()
+                if z.dem_all is not None:
+                    z.dem_all.batch.frame_step.close()
+            del plain, scr, scr64
     # tensor-pipe figure: the screening's own network work on one plan's
     # population, the head over n_sample rows after one encoder pass, timed alone
-    sc = planner.make_scene(field, starts[-1], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats)
+    sc = planner.make_scene(field, starts[-1][0], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats,
+                            removed=starts[-1][1])
     Yn = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.5, -1, 1)
-    ext = planner.features(sc, Yn)
+    ext = planner.features(sc, Yn, planner.rigid_path(sc, Yn)[1])
     rows0 = torch.zeros(cfg.n_sample, dtype=torch.int32, device=device)
     enc = sur.net.encode(sc.patch, tag="bench_enc")
     for _ in range(3):
@@ -780,10 +801,16 @@ def run_surrogate(args, rank: int, world: int):
         "metric": SUR_METRIC, "value": value, "unit": SUR_UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": 1e3 * ts_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 DEM, bf16 surrogate (fp32 accumulate)",
-        "data": "synthetic (seeded medium field; training tuples from the DEM's own batched rollouts)",
+        "data": f"synthetic (seeded medium field, {args.sur_scenes} starts; training tuples from the DEM's own "
+                "batched rollouts)",
         "config": {"workload": f"MBD {cfg.n_sample} samples x {cfg.n_diffuse - 1} reverse steps, horizon {H} x "
-                               f"10 substeps, top {cfg.top_k} + {cfg.top_k} random re-scored by the DEM, fallback "
-                               f"when the random ones beat the screened best by {cfg.max_rel_err:.0%}",
+                               f"10 substeps, top {cfg.top_k} + {args.sur_check} random re-scored by the DEM, "
+                               f"fallback when the random ones beat the screened best by {cfg.max_rel_err:.0%}",
+                   "top64": {"speedup_vs_plain_dem": tp / (sum(r["top64"]["screened_s"] for r in rows) / K),
+                             "plan_rel_cost_err": [r["top64"]["rel_cost_err"] for r in rows],
+                             "fallback_steps": [r["top64"]["fallbacks"] for r in rows],
+                             "note": "the same plans with only the 64 best-ranked candidates re-scored"},
+                   "scenes": args.sur_scenes, "windows": [r["window"] for r in rows],
                    "plain_dem_rollouts_per_s": plain_rate, "speedup_vs_plain_dem": value / plain_rate,
                    "plan_rel_cost_err": errs, "plan_rel_cost_err_max": max(errs),
                    "plans_within_5pct": int(sum(e <= 0.05 for e in errs)),
@@ -807,10 +834,11 @@ def run_surrogate(args, rank: int, world: int):
     return line
 
 
-def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_run: int = 1):
+def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_run: int = 1, flush=None):
     """Per-phase device time of a few frames (profiling switch of the library).
     ``run()`` replaces the default one-frame scan (``frames`` calls of it, each
-    ``frames_per_run`` frames long)."""
+    ``frames_per_run`` frames long); ``flush``, a buffer larger than L2, is
+    written before every call."""
     import collections
     import torch
     k = fs.n_ice_steps
@@ -820,7 +848,9 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_
     acc = collections.defaultdict(list)
     per_sub = collections.defaultdict(list)
     fs.set_profiling(True)
-    for _ in range(frames):
+    for i in range(frames):
+        if flush is not None:
+            flush.fill_(i & 0xFF)
         if run is None:
             st, sh, _ = fs.scan_segment(st, sh, sp, vw, history=False)
         else:
@@ -842,7 +872,7 @@ def print_phase_times(fs, st, sh, sp, vw, frames: int = 5, run=None, frames_per_
         s = sum(v) / frames
         tot += s
         sys.stderr.write(f"phase {nm:9s} {s:9.1f} us/frame  ({len(v) / frames:.1f} runs/frame)\n")
-    sys.stderr.write(f"phase total     {tot:9.1f} us/frame\n")
+    sys.stderr.write(f"phase total     {tot:9.1f} us/frame{' (L2 flushed before each call)' if flush is not None else ''}\n")
     for nm in ("escape", "force"):
         row = " ".join(f"{sum(per_sub[(nm, i)]) / max(len(per_sub[(nm, i)]), 1):6.1f}" for i in range(k))
         sys.stderr.write(f"phase {nm:9s} by substep (us per run): {row}\n")
@@ -1017,7 +1047,10 @@ def main():
     ap.add_argument("--sur-epochs", type=int, default=10)
     ap.add_argument("--sur-samples", type=int, default=8192, help="MBD samples per reverse step")
     ap.add_argument("--sur-iters", type=int, default=16, help="MBD reverse steps per plan")
-    ap.add_argument("--sur-top-k", type=int, default=64, help="candidates re-scored by the DEM per step")
+    ap.add_argument("--sur-top-k", type=int, default=512, help="best-ranked candidates re-scored by the DEM per step")
+    ap.add_argument("--sur-check", type=int, default=64, help="random held-out candidates re-scored per step")
+    ap.add_argument("--sur-scenes", choices=("channel", "open"), default="channel",
+                    help="plan starts: mid-transit in the pack with the ship's channel cleared, or open water")
     ap.add_argument("--all-active", action="store_true",
                     help="every element active from the start (the force path on the whole field)")
     args = ap.parse_args()

@@ -357,6 +357,17 @@ int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const i
                       const DemRolloutCostParams* params, const void* masses, const void* vel0,
                       const void* vel1, double* out, void* stream);
 
+/* Per-waypoint costmap values of pose paths (the waypoint term inside
+ * _make_raw_components_fn, jax_mbd_planner.py:569-665, before the trapezoid
+ * rule): out[q, t] (Q, H) float32 = the query (:128-168) at the hull centre
+ * and four box corners, maximum (the centre alone when ship_length or
+ * ship_beam is 0), of the pose eta_hist[t, q] (H, Q, 3) of `dtype`.  Only the
+ * costmap geometry, oob_penalty and the hull size of params are read; grid
+ * (rows, cols) float32.  Device arrays; 1 <= horizon <= 2000.  The screening
+ * surrogate reads these along each candidate's rigid-ship path. */
+int dem_rollout_waypoint_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const void* eta_hist,
+                               const float* grid, const DemRolloutCostParams* params, float* out, void* stream);
+
 /* Per-rollout ice terms after dem_rollout_segment (no reference counterpart
  * as a whole): for every system q of n_systems, out[q] (Q,2) double =
  * [hull impulse: the sum over the segment's steps of J_hist[t, q], the

@@ -478,6 +478,23 @@ __device__ __forceinline__ void warp_append(int* list, int* cnt, bool flag, int 
     if (flag) list[base + __popc(bal & ((1u << lane) - 1u))] = v;
 }
 
+// Two flagged values per lane, appended with one atomic per warp (the
+// frame's bond list: up to two slots per lane and step).
+__device__ __forceinline__ void warp_append2(int* list, int* cnt, bool f0, int v0, bool f1, int v1) {
+    const unsigned am = __activemask();
+    const unsigned bal0 = __ballot_sync(am, f0), bal1 = __ballot_sync(am, f1);
+    const int n0 = __popc(bal0), n = n0 + __popc(bal1);
+    if (!n) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(am) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(cnt, n);
+    base = __shfl_sync(am, base, leader);
+    const unsigned lt = (1u << lane) - 1u;
+    if (f0) list[base + __popc(bal0 & lt)] = v0;
+    if (f1) list[base + n0 + __popc(bal1 & lt)] = v1;
+}
+
 // Build element e's list (one warp): candidates are gathered in shared memory,
 // sorted and deduplicated, then stored so that indices above e come first
 // (ascending), then indices below e (ascending) — the order in which the
@@ -1361,6 +1378,51 @@ __device__ __forceinline__ T thrust_scale_of(const KArgs<T>& a, const double* to
     return (mag > mx) ? mx / jmax(mag, T(1e-6)) : T(1);
 }
 
+// Warps with at most this many active elements share each one's slots among
+// their lanes in phase_reduce.
+constexpr int kCoopSlots = 3;
+
+// The bond slot records of active element e by one lane: two slots per step,
+// their loads issued level by level (slot -> partner -> floe flag).  The bond
+// has an active end this frame; it is listed once, by its active end of lower
+// index (e, unless the partner is active and lower).
+template <typename T>
+__device__ __forceinline__ void slot_records_lane(const KArgs<T>& a, const Frame<T>& F, SlotRec<T>* rec, int e,
+                                                  unsigned fstamp) {
+    const int s0 = a.boff[e], s1 = a.boff[e + 1];
+    for (int sl = s0; sl < s1; sl += 2) {
+        const bool two = sl + 1 < s1;
+        const int2 ent0 = a.bslot[sl];
+        const int2 ent1 = two ? a.bslot[sl + 1] : ent0;
+        const int b0 = ent0.x & 0x7fffffff, b1 = ent1.x & 0x7fffffff;
+        const bool in0 = F.src.intact[b0] != 0, in1 = F.src.intact[b1] != 0;
+        const bool sa0 = F.src.active[ent0.y] != 0, sa1 = F.src.active[ent1.y] != 0;
+        const int fo0 = a.floe_of[ent0.y], fo1 = a.floe_of[ent1.y];
+        const T d0 = F.src.dmg[b0], d1 = F.src.dmg[b1];
+        const T r0 = a.slot_rest[sl], r1 = two ? a.slot_rest[sl + 1] : r0;
+        const T k0 = a.slot_stiff[sl], k1 = two ? a.slot_stiff[sl + 1] : k0;
+        const bool ao0 = sa0 || a.fcoll[fo0];
+        const bool ao1 = sa1 || a.fcoll[fo1];
+        a.bstamp[b0] = fstamp;
+        a.bstamp[b1] = fstamp;
+        warp_append2(a.fb_list, a.fb_cnt, !(ao0 && ent0.y < e), b0, two && !(ao1 && ent1.y < e), b1);
+        if (!in0 || (two && !in1)) a.crack[e] = 1;
+        SlotRec<T> q;
+        q.o = (ent0.x < 0) ? (int)((unsigned)ent0.y | 0x80000000u) : ent0.y;
+        q.rest = r0;
+        q.stiff = k0;
+        q.omd = (in0 && ao0) ? T(1) - d0 : T(-1);  // e is active: both ends must be
+        rec[sl] = q;
+        if (two) {
+            q.o = (ent1.x < 0) ? (int)((unsigned)ent1.y | 0x80000000u) : ent1.y;
+            q.rest = r1;
+            q.stiff = k1;
+            q.omd = (in1 && ao1) ? T(1) - d1 : T(-1);
+            rec[sl + 1] = q;
+        }
+    }
+}
+
 template <typename T>
 __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     typedef typename vec2_of<T>::type V2;
@@ -1430,75 +1492,80 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
     SlotRec<T>* rec = reinterpret_cast<SlotRec<T>*>(a.slotrec);
     typedef typename vec4_of<T>::type V4;
     const unsigned fstamp = frame_stamp(a, F);
-    for (int e = gtid; e < a.n; e += gsz) {
-        // activation (jax_simulation.py:498-509)
-        const bool was = F.src.active[e] != 0;
-        const bool ae = was || a.fcoll[a.floe_of[e]];
-        // after the first frame of a call, an element frozen before and after
-        // this frame's activation has its state, substep buffers and frame
-        // output in place already (the previous frame wrote them)
-        if (F.f >= 1 && !ae) continue;
-        F.dst.active[e] = ae ? 1 : 0;
-        // packed kinematics read by substep 0
-        const V2 p = ld2(F.src.pos, e), v = ld2(F.src.vel, e);
-        V4 k4;
-        k4.x = p.x;
-        k4.y = p.y;
-        k4.z = a.radii[e];
-        k4.w = a.r3[e];
-        reinterpret_cast<V4*>(a.kin[0])[e] = k4;
-        st2(a.kvel[0], e, v.x, v.y);
+    // lanes take consecutive elements; the loop bound is uniform over the warp,
+    // so that the warp can share the slot work of the active elements it finds
+    const int lane = threadIdx.x & 31;
+    for (int w0 = gtid - lane; w0 < a.n; w0 += gsz) {
+        const int e = w0 + lane;
+        bool ae = false;
+        if (e < a.n) {
+            // activation (jax_simulation.py:498-509)
+            const bool was = F.src.active[e] != 0;
+            ae = was || a.fcoll[a.floe_of[e]];
+            // after the first frame of a call, an element frozen before and
+            // after this frame's activation has its state, substep buffers and
+            // frame output in place already (the previous frame wrote them)
+            if (F.f == 0 || ae) {
+                F.dst.active[e] = ae ? 1 : 0;
+                // packed kinematics read by substep 0
+                const V2 p = ld2(F.src.pos, e), v = ld2(F.src.vel, e);
+                V4 k4;
+                k4.x = p.x;
+                k4.y = p.y;
+                k4.z = a.radii[e];
+                k4.w = a.r3[e];
+                reinterpret_cast<V4*>(a.kin[0])[e] = k4;
+                st2(a.kvel[0], e, v.x, v.y);
+                if (!ae) {
+                    // frozen for the whole frame, it keeps its state
+                    // (jax_simulation.py:257-262): both substep buffers and the
+                    // frame's output hold it now, and the substeps skip it
+                    reinterpret_cast<V4*>(a.kin[1])[e] = k4;
+                    st2(a.kvel[1], e, v.x, v.y);
+                    st2(F.dst.pos, e, p.x, p.y);
+                    st2(F.dst.vel, e, v.x, v.y);
+                    F.dst.rot[e] = F.src.rot[e];
+                    F.dst.avel[e] = F.src.avel[e];
+                }
+            }
+        }
         warp_append(a.act_list, a.act_cnt, ae, e);
-        if (!ae) {
-            // frozen for the whole frame, it keeps its state (jax_simulation.py:
-            // 257-262): both substep buffers and the frame's output hold it now,
-            // and the substeps skip the element
-            reinterpret_cast<V4*>(a.kin[1])[e] = k4;
-            st2(a.kvel[1], e, v.x, v.y);
-            st2(F.dst.pos, e, p.x, p.y);
-            st2(F.dst.vel, e, v.x, v.y);
-            F.dst.rot[e] = F.src.rot[e];
-            F.dst.avel[e] = F.src.avel[e];
+        // the bond slot records of the active elements for this frame (only
+        // active elements read them); crack front = the element touches a bond
+        // broken at frame start (read for bonds between two active elements).
+        // A warp with few active elements takes them one after another, each
+        // element's slots spread over the lanes; with more, every lane takes
+        // its own element's slots.
+        unsigned m = __ballot_sync(0xffffffffu, ae);
+        if (__popc(m) > kCoopSlots) {
+            if (ae) slot_records_lane(a, F, rec, e, fstamp);
             continue;
         }
-        // the bond slot records of an active element for this frame (only active
-        // elements read them); crack front = e touches a bond broken at frame
-        // start (read for bonds between two active elements only).  Two slots per
-        // step, their loads issued level by level (slot -> partner -> floe flag).
-        const int s0 = a.boff[e], s1 = a.boff[e + 1];
-        for (int sl = s0; sl < s1; sl += 2) {
-            const bool two = sl + 1 < s1;
-            const int2 ent0 = a.bslot[sl];
-            const int2 ent1 = two ? a.bslot[sl + 1] : ent0;
-            const int b0 = ent0.x & 0x7fffffff, b1 = ent1.x & 0x7fffffff;
-
-            const bool in0 = F.src.intact[b0] != 0, in1 = F.src.intact[b1] != 0;
-            const bool sa0 = F.src.active[ent0.y] != 0, sa1 = F.src.active[ent1.y] != 0;
-            const int fo0 = a.floe_of[ent0.y], fo1 = a.floe_of[ent1.y];
-            const T d0 = F.src.dmg[b0], d1 = F.src.dmg[b1];
-            const T r0 = a.slot_rest[sl], r1 = two ? a.slot_rest[sl + 1] : r0;
-            const T k0 = a.slot_stiff[sl], k1 = two ? a.slot_stiff[sl + 1] : k0;
-            const bool ao0 = sa0 || a.fcoll[fo0];
-            const bool ao1 = sa1 || a.fcoll[fo1];
-            // the bond has an active end this frame; it is listed once, by its
-            // active end of lower index (e, unless the partner is active and lower)
-            a.bstamp[b0] = fstamp;
-            a.bstamp[b1] = fstamp;
-            if (!(ao0 && ent0.y < e)) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b0;
-            if (two && !(ao1 && ent1.y < e)) a.fb_list[atomicAdd(a.fb_cnt, 1)] = b1;
-            if (!in0 || (two && !in1)) a.crack[e] = 1;
-            SlotRec<T> q;
-            q.o = (ent0.x < 0) ? (int)((unsigned)ent0.y | 0x80000000u) : ent0.y;
-            q.rest = r0;
-            q.stiff = k0;
-            q.omd = (in0 && ao0) ? T(1) - d0 : T(-1);  // e is active: both ends must be
-            rec[sl] = q;
-            if (two) {
-                q.o = (ent1.x < 0) ? (int)((unsigned)ent1.y | 0x80000000u) : ent1.y;
-                q.rest = r1;
-                q.stiff = k1;
-                q.omd = (in1 && ao1) ? T(1) - d1 : T(-1);
-                rec[sl + 1] = q;
+        while (m) {
+            const int ee = w0 + __ffs(m) - 1;
+            m &= m - 1;
+            const int s0 = a.boff[ee], s1 = a.boff[ee + 1];
+            for (int sl = s0 + lane; sl < s1; sl += 32) {
+                const int2 ent = a.bslot[sl];
+                const int b = ent.x & 0x7fffffff;
+                const bool in = F.src.intact[b] != 0;
+                const bool sa = F.src.active[ent.y] != 0;
+                const int fo = a.floe_of[ent.y];
+                const T d = F.src.dmg[b];
+                const T r = a.slot_rest[sl], k = a.slot_stiff[sl];
+                const bool ao = sa || a.fcoll[fo];
+                // the bond has an active end this frame; it is listed once, by
+                // its active end of lower index (ee, unless the partner is
+                // active and lower)
+                a.bstamp[b] = fstamp;
+                warp_append(a.fb_list, a.fb_cnt, !(ao && ent.y < ee), b);
+                if (!in) a.crack[ee] = 1;
+                SlotRec<T> q;
+                q.o = (ent.x < 0) ? (int)((unsigned)ent.y | 0x80000000u) : ent.y;
+                q.rest = r;
+                q.stiff = k;
+                q.omd = (in && ao) ? T(1) - d : T(-1);  // ee is active: both ends must be
+                rec[sl] = q;
             }
         }
     }
@@ -2262,7 +2329,14 @@ __device__ void phase_fracture(const KArgs<T>& a, const Frame<T>& F, T scale) {
     // copied already when the frame writes a separate output, or which is in
     // place; its history row is that state
     const int nfb = *((volatile int*)a.fb_cnt);
-    for (int i = gtid; i < nfb; i += gsz) fracture_bond(a, F, scale, a.fb_list[i]);
+    if ((long long)nfb * 4 > (long long)a.nb) {
+        // most bonds are listed: visit them in index order by their stamps,
+        // with coalesced bond loads (the list's order is the append order)
+        for (int b = gtid; b < a.nb; b += gsz)
+            if (a.bstamp[b] == fstamp) fracture_bond(a, F, scale, b);
+    } else {
+        for (int i = gtid; i < nfb; i += gsz) fracture_bond(a, F, scale, a.fb_list[i]);
+    }
     if (a.h_intact)
         for (int b = gtid; b < a.nb; b += gsz)
             if (a.bstamp[b] != fstamp) a.h_intact[(size_t)F.f * a.nb + b] = F.src.intact[b] != 0 ? 1 : 0;

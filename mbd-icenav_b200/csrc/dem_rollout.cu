@@ -51,6 +51,24 @@ __device__ __forceinline__ float query(const RcArgs& c, const float* __restrict_
     return val + oob;
 }
 
+// a waypoint's cost: the query at the hull centre and its four box corners,
+// maximum (NaN wins), or at the centre alone without a hull
+__device__ __forceinline__ float waypoint_cost(const RcArgs& c, const float* __restrict__ grid, float x, float y,
+                                               float psi) {
+    if (!c.use_hull) return query(c, grid, x, y);
+    const float cs = cosf(psi), sn = sinf(psi);
+    const float dxb[5] = {0.0f, c.hl, c.hl, -c.hl, -c.hl};
+    const float dyb[5] = {0.0f, c.hw, -c.hw, c.hw, -c.hw};
+    float w = 0.0f;
+    for (int k = 0; k < 5; ++k) {
+        const float wx = x + cs * dxb[k] - sn * dyb[k];
+        const float wy = y + sn * dxb[k] + cs * dyb[k];
+        const float v = query(c, grid, wx, wy);
+        w = (k == 0) ? v : max_nan(w, v);
+    }
+    return w;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kRcThreads) rollout_cost_kernel(RcArgs c, const int* __restrict__ sys_start,
                                                                   const T* __restrict__ eta0,
@@ -71,22 +89,7 @@ __global__ void __launch_bounds__(kRcThreads) rollout_cost_kernel(RcArgs c, cons
     for (int t = threadIdx.x; t < W; t += blockDim.x) {
         const T* p = (t == 0) ? eta0 + 3 * (size_t)q : eta_hist + 3 * ((size_t)(t - 1) * c.Q + q);
         const float x = (float)p[0], y = (float)p[1], psi = (float)p[2];
-        float w;
-        if (c.use_hull) {
-            const float cs = cosf(psi), sn = sinf(psi);
-            const float dxb[5] = {0.0f, c.hl, c.hl, -c.hl, -c.hl};
-            const float dyb[5] = {0.0f, c.hw, -c.hw, c.hw, -c.hw};
-            w = 0.0f;
-            for (int k = 0; k < 5; ++k) {
-                const float wx = x + cs * dxb[k] - sn * dyb[k];
-                const float wy = y + sn * dxb[k] + cs * dyb[k];
-                const float v = query(c, grid, wx, wy);
-                w = (k == 0) ? v : max_nan(w, v);
-            }
-        } else {
-            w = query(c, grid, x, y);
-        }
-        wp[t] = w;
+        wp[t] = waypoint_cost(c, grid, x, y, psi);
         tx[t] = x;
         ty[t] = y;
         dsc[t] = expf(-(float)t / c.tau);
@@ -154,6 +157,35 @@ __global__ void __launch_bounds__(kRcThreads) rollout_cost_kernel(RcArgs c, cons
     o[4] = s_ke[0];
 }
 
+// one thread per (step, rollout): out[q, t] = the cost of the pose after step t
+template <typename T>
+__global__ void __launch_bounds__(kRcThreads) waypoint_cost_kernel(RcArgs c, const T* __restrict__ eta_hist,
+                                                                   const float* __restrict__ grid,
+                                                                   float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)c.Q * c.H) return;
+    const int t = (int)(i / c.Q), q = (int)(i % c.Q);
+    const T* p = eta_hist + 3 * (size_t)i;
+    out[(size_t)q * c.H + t] = waypoint_cost(c, grid, (float)p[0], (float)p[1], (float)p[2]);
+}
+
+// the costmap geometry of the cost arguments, as the planner's float32 query sees it
+bool grid_args(const DemRolloutCostParams* p, RcArgs& c) {
+    if (p->rows < 1 || p->cols < 1 || (long long)p->rows * p->cols >= (1LL << 31) || !(p->resolution > 0.0))
+        return false;
+    c.rows = p->rows;
+    c.cols = p->cols;
+    c.use_hull = (p->ship_length > 0.0 && p->ship_beam > 0.0) ? 1 : 0;
+    // the planner's Python scalars meet float32 arrays: each is rounded to float
+    c.xo = (float)p->x_origin;
+    c.yo = (float)p->y_origin;
+    c.res = (float)p->resolution;
+    c.oob = (float)p->oob_penalty;
+    c.hl = (float)(p->ship_length / 2.0);
+    c.hw = (float)(p->ship_beam / 2.0);
+    return true;
+}
+
 template <typename T>
 int launch_costs(const RcArgs& c, const int32_t* sys_start, const void* eta0, const void* eta_hist,
                  const void* u, const float* grid, const void* masses, const void* v0, const void* v1, double* out,
@@ -173,29 +205,18 @@ extern "C" int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horiz
                                  const void* vel1, double* out, void* stream) {
     if (!p || !out || !eta0 || !eta_hist || !grid || (dtype != DEM_F32 && dtype != DEM_F64)) return DEM_ERR_INVALID;
     if (n_systems < 1 || horizon < 1 || horizon > kRcMaxHorizon) return DEM_ERR_INVALID;
-    if (p->rows < 1 || p->cols < 1 || (long long)p->rows * p->cols >= (1LL << 31) || !(p->resolution > 0.0))
-        return DEM_ERR_INVALID;
+    RcArgs c{};
+    if (!grid_args(p, c)) return DEM_ERR_INVALID;
     const bool has_ke = masses || vel0 || vel1;
     if (has_ke && (!masses || !vel0 || !vel1 || !system_start)) return DEM_ERR_INVALID;
     if (controls)
         for (int k = 0; k < 3; ++k)
             if (!(p->action_scale[k] != 0.0) || !std::isfinite(p->action_scale[k])) return DEM_ERR_INVALID;
-    RcArgs c{};
     c.Q = n_systems;
     c.H = horizon;
-    c.rows = p->rows;
-    c.cols = p->cols;
-    c.use_hull = (p->ship_length > 0.0 && p->ship_beam > 0.0) ? 1 : 0;
     c.has_truncate = p->has_truncate ? 1 : 0;
     c.has_jerk = controls ? 1 : 0;
     c.has_ke = has_ke ? 1 : 0;
-    // the planner's Python scalars meet float32 arrays: each is rounded to float
-    c.xo = (float)p->x_origin;
-    c.yo = (float)p->y_origin;
-    c.res = (float)p->resolution;
-    c.oob = (float)p->oob_penalty;
-    c.hl = (float)(p->ship_length / 2.0);
-    c.hw = (float)(p->ship_beam / 2.0);
     c.gx = (float)p->goal_x;
     c.gy = (float)p->goal_y;
     c.trunc_y = (float)p->truncate_y;
@@ -208,6 +229,25 @@ extern "C" int dem_rollout_costs(int32_t dtype, int32_t n_systems, int32_t horiz
     if (dtype == DEM_F32)
         return launch_costs<float>(c, system_start, eta0, eta_hist, controls, grid, masses, vel0, vel1, out, st);
     return launch_costs<double>(c, system_start, eta0, eta_hist, controls, grid, masses, vel0, vel1, out, st);
+}
+
+extern "C" int dem_rollout_waypoint_costs(int32_t dtype, int32_t n_systems, int32_t horizon, const void* eta_hist,
+                                          const float* grid, const DemRolloutCostParams* p, float* out,
+                                          void* stream) {
+    if (!p || !out || !eta_hist || !grid || (dtype != DEM_F32 && dtype != DEM_F64)) return DEM_ERR_INVALID;
+    if (n_systems < 1 || horizon < 1 || horizon > kRcMaxHorizon) return DEM_ERR_INVALID;
+    RcArgs c{};
+    if (!grid_args(p, c)) return DEM_ERR_INVALID;
+    c.Q = n_systems;
+    c.H = horizon;
+    const long long total = (long long)n_systems * horizon;
+    const unsigned blocks = (unsigned)((total + kRcThreads - 1) / kRcThreads);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == DEM_F32)
+        waypoint_cost_kernel<float><<<blocks, kRcThreads, 0, st>>>(c, (const float*)eta_hist, grid, out);
+    else
+        waypoint_cost_kernel<double><<<blocks, kRcThreads, 0, st>>>(c, (const double*)eta_hist, grid, out);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
 
 // ════════════════════════════════════════════════════════════════════════════

@@ -26,8 +26,14 @@ constexpr int kBK = 64;  // bf16 per 128-byte swizzled row
 // stages of the operand ring: enough 64-deep K slices in flight to cover a
 // TMA round trip behind the MMAs of the slices before it (32 KB a stage at
 // BN = 128, 24 KB at BN = 64; both rings stay under 200 KB of shared memory)
+#ifndef SG_STAGES_128
+#define SG_STAGES_128 6
+#endif
+#ifndef SG_BN_MAX
+#define SG_BN_MAX 128
+#endif
 template <int BN>
-__host__ __device__ constexpr int stages_of() { return BN >= 128 ? 6 : 8; }
+__host__ __device__ constexpr int stages_of() { return BN >= 256 ? 4 : BN >= 128 ? SG_STAGES_128 : 8; }
 
 struct GemmArgs {
     int M, N, K;
@@ -44,6 +50,10 @@ template <int BN>
 constexpr size_t gemm_smem_bytes() {
     return 1024 + (size_t)stages_of<BN>() * (kBM * kBK * 2 + BN * kBK * 2) + 256;
 }
+
+static_assert(gemm_smem_bytes<64>() <= 232448 && gemm_smem_bytes<128>() <= 232448 &&
+                  gemm_smem_bytes<256>() <= 232448,
+              "operand ring above the 227 KB of shared memory a CTA may use");
 
 template <int BN>
 __global__ void __launch_bounds__(128, 1)
@@ -440,7 +450,11 @@ int sg_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const v
     GemmArgs g{M, N, K, D, ldd, d_dtype == SG_OUT_BF16 ? 1 : 0, bias, relu ? 1 : 0,
                reinterpret_cast<const __nv_bfloat16*>(mask), ldm, err};
     cudaStream_t st = (cudaStream_t)stream;
-    return N <= 64 ? launch_gemm<64>(g, A, lda, B, ldb, st) : launch_gemm<128>(g, A, lda, B, ldb, st);
+    if (N <= 64) return launch_gemm<64>(g, A, lda, B, ldb, st);
+#if SG_BN_MAX >= 256
+    if (N >= 512) return launch_gemm<256>(g, A, lda, B, ldb, st);
+#endif
+    return launch_gemm<128>(g, A, lda, B, ldb, st);
 }
 
 int sg_im2col(int32_t B, int32_t H, int32_t W, int32_t C, const void* X, int32_t kpad, void* cols, void* stream) {

@@ -116,7 +116,12 @@ def reach_radius(field, horizon: int, dt: float, v_max: float = 5.0) -> float:
 
 
 def make_scene(field, eta0, nu0=(2.0, 0.0, 0.0), horizon: int = 64, dtype=None, device="cuda",
-               patch_stats=(0.0, 1.0), static=None, ship_dyn=None) -> PlanScene:
+               patch_stats=(0.0, 1.0), static=None, ship_dyn=None, removed=None) -> PlanScene:
+    """The plan's start: the window of elements any candidate can reach, the
+    costmap around the start and its normalised patch.  ``removed``: element
+    indices that are not in the scene (the channel a transiting ship has
+    cleared behind and around it); they are left out of the window and the
+    costmap."""
     torch = _tm()
     from .config import get_default_simulation_config
     from .costmap import build_costmap_jax
@@ -134,11 +139,18 @@ def make_scene(field, eta0, nu0=(2.0, 0.0, 0.0), horizon: int = 64, dtype=None, 
     nu0 = np.asarray(nu0, np.float64)
     R = reach_radius(field, horizon, field.dt)
     d = np.linalg.norm(np.asarray(field.centroids, np.float64) - eta0[:2], axis=1)
-    window = np.nonzero(d < R)[0]
+    present = np.ones(len(d), bool)
+    if removed is not None:
+        present[np.asarray(removed, np.int64)] = False
+    window = np.nonzero((d < R) & present)[0]
     half = 0.5 * COSTMAP_CELLS * RESOLUTION - 20.0  # 256 cells with the builder's 20 m margin
-    cm, _ = build_costmap_jax(field.centroids, field.thicknesses, static.radii, eta0[0] - half, eta0[0] + half,
-                              eta0[1] - half, eta0[1] + half, resolution=RESOLUTION, ship_length=field.ship_length,
-                              ship_beam=field.ship_beam, masses=static.masses, device=dev, download=False)
+    cents = np.asarray(field.centroids, np.float64)
+    near = present & (np.abs(cents[:, 0] - eta0[0]) < half + 60.0) & (np.abs(cents[:, 1] - eta0[1]) < half + 60.0)
+    thick = np.asarray(field.thicknesses, np.float64)
+    cm, _ = build_costmap_jax(cents[near], thick[near], np.asarray(static.radii)[near], eta0[0] - half,
+                              eta0[0] + half, eta0[1] - half, eta0[1] + half, resolution=RESOLUTION,
+                              ship_length=field.ship_length, ship_beam=field.ship_beam,
+                              masses=np.asarray(static.masses)[near], device=dev, download=False)
     c0 = (COSTMAP_CELLS - PATCH_CELLS) // 2
     mean, std = patch_stats
     patch32 = ((cm.grid[c0:c0 + PATCH_CELLS, c0:c0 + PATCH_CELLS] - mean) / std).contiguous()
@@ -215,15 +227,18 @@ def physical_controls(Yn):
     return torch.stack([X, torch.zeros_like(X), N], -1).transpose(0, 1).contiguous()
 
 
-def features(scene: PlanScene, Yn):
-    """(Q, 6 + 2H) fp32 network inputs besides the patch: ship state [u/5, v/2,
-    r/0.1, cos psi, sin psi, 0] and the normalised controls, step by step."""
+def features(scene: PlanScene, Yn, wcost):
+    """(Q, 6 + 3H) fp32 network inputs besides the patch: ship state [u/5, v/2,
+    r/0.1, cos psi, sin psi, 0], the normalised controls step by step, and
+    log1p of ``wcost`` (Q, H), the costmap value at each pose of the
+    candidate's rigid-ship path (``rigid_path``)."""
     torch = _tm()
     Q, H, _ = Yn.shape
     e, v = scene.eta0, scene.nu0
     ship = torch.tensor([v[0] / 5.0, v[1] / 2.0, v[2] / 0.1, math.cos(e[2]), math.sin(e[2]), 0.0],
                         dtype=torch.float32, device=Yn.device)
-    return torch.cat([ship.expand(Q, S.N_SHIP), Yn.reshape(Q, 2 * H).float()], 1).contiguous()
+    path = torch.log1p(torch.clamp(wcost.float(), min=0.0))
+    return torch.cat([ship.expand(Q, S.N_SHIP), Yn.reshape(Q, 2 * H).float(), path], 1).contiguous()
 
 
 # ─── target transforms ──────────────────────────────────────────────────────
@@ -310,19 +325,29 @@ class Surrogate:
         self.stats = stats
         self.patch_stats = patch_stats
 
-    def predict(self, scene: PlanScene, Yn):
-        """(Q, 3) float64 predicted ice terms [KE, impulse, bonds] of the candidates."""
+    def predict(self, scene: PlanScene, Yn, wcost=None):
+        """(Q, 3) float64 predicted ice terms [KE, impulse, bonds] of the
+        candidates; ``wcost`` (Q, H) from ``rigid_path`` (computed when None)."""
         torch = _tm()
         Q = int(Yn.shape[0])
+        if wcost is None:
+            _, wcost = rigid_path(scene, Yn)
         enc = self.net.encode(scene.patch, tag="plan_enc")
         rows = self.net._buf("plan_rows", (Q,), torch.int32)
         rows.zero_()
-        out = self.net.head(enc, features(scene, Yn), enc_row=rows, tag="plan_head")
+        out = self.net.head(enc, features(scene, Yn, wcost), enc_row=rows, tag="plan_head")
         return self.stats.inverse(out[:, :S.N_OUT])
 
 
 def rigid_terms(scene: PlanScene, Yn, out=None):
     """(Q, 4) float64 planner components of the rigid-ship paths (``dem_ship_rollout``)."""
+    return rigid_path(scene, Yn, out)[0]
+
+
+def rigid_path(scene: PlanScene, Yn, out=None):
+    """The candidates' rigid-ship paths (``dem_ship_rollout``): their (Q, 4)
+    float64 planner components and the (Q, H) float32 costmap value at each
+    pose (``dem_rollout_waypoint_costs``)."""
     torch = _tm()
     lib = _abi.load_library()
     Q, H, _ = Yn.shape
@@ -339,7 +364,8 @@ def rigid_terms(scene: PlanScene, Yn, out=None):
         raise _abi.DemError(rc, "dem_ship_rollout failed")
     comp = rollouts.path_costs(eta0, hist, u, scene.costmap, scene.goal, scene.field.ship_length,
                                scene.field.ship_beam, out=out)
-    return comp[:, :4]
+    wcost = rollouts.waypoint_costs(hist, scene.costmap, scene.field.ship_length, scene.field.ship_beam)
+    return comp[:, :4], wcost
 
 
 class ScreenedScorer:
@@ -378,8 +404,8 @@ class ScreenedScorer:
     def predicted(self, Yn):
         """(Q,) float64 predicted totals: rigid-path planner terms + predicted ice terms."""
         torch = _tm()
-        planner = rigid_terms(self.scene, Yn)
-        ice = self.sur.predict(self.scene, Yn)
+        planner, wcost = rigid_path(self.scene, Yn)
+        ice = self.sur.predict(self.scene, Yn, wcost)
         wp = torch.tensor(self.w.planner(), dtype=torch.float64, device=Yn.device)
         wi = torch.tensor(self.w.ice(), dtype=torch.float64, device=Yn.device)
         return planner @ wp + ice @ wi
@@ -498,6 +524,46 @@ def sample_starts(field, n: int, rng, horizon: int = 64, clearance: float = 2.0)
     return out
 
 
+def element_radii(field) -> np.ndarray:
+    """Largest centroid-to-vertex distance of each element's polygon."""
+    cents = np.asarray(field.centroids, np.float64)
+    return np.array([float(np.max(np.hypot(*(np.asarray(p, np.float64) - c).T))) for p, c in
+                     zip(field.polygons, cents)])
+
+
+def channel_starts(field, n: int, rng, horizon: int = 64, clearance: float = 2.0, channel: float = 100.0,
+                   radii=None):
+    """Mid-transit start poses inside the pack, each with the elements its
+    passage has cleared: the ship at a uniform position whose reach stays
+    inside the field's ice, heading along the field's track +- 0.3 rad, with
+    every element that overlaps the hull box plus ``clearance`` or the
+    ``channel`` metres of beam-wide lane behind the stern removed.  Returns
+    ``[(eta, removed_indices)]``; windows hold the full pack density."""
+    cents = np.asarray(field.centroids, np.float64)
+    radii = element_radii(field) if radii is None else np.asarray(radii, np.float64)
+    L, B = field.ship_length, field.ship_beam
+    R = reach_radius(field, horizon, field.dt)
+    lo, hi = cents.min(0) + R + 10.0, cents.max(0) - R - 10.0
+    if np.any(hi <= lo):
+        raise ValueError("the field's ice is smaller than one planning window")
+    from scipy.spatial import cKDTree
+    tree = cKDTree(cents)
+    rmax = float(radii.max())
+    base = float(field.trajectory[0][2])
+    out = []
+    for _ in range(n):
+        x, y = rng.uniform(lo[0], hi[0]), rng.uniform(lo[1], hi[1])
+        psi = base + rng.uniform(-0.3, 0.3)
+        c, s = math.cos(psi), math.sin(psi)
+        near = np.asarray(tree.query_ball_point([x, y], 0.5 * L + channel + B + clearance + rmax), np.int64)
+        dx, dy = cents[near, 0] - x, cents[near, 1] - y
+        bx, by = c * dx + s * dy, -s * dx + c * dy
+        r = radii[near] + clearance
+        gone = (bx < 0.5 * L + r) & (bx > -0.5 * L - channel - r) & (np.abs(by) < 0.5 * B + r)
+        out.append((np.array([x, y, psi]), near[gone]))
+    return out
+
+
 def sample_training_controls(rng, Q: int, H: int, device):
     """(Q, H, 2) normalised controls: half Gaussian around the surge bias (sigma
     0.3 of the maxima, the batched-rollout generator's spread), half uniform."""
@@ -514,16 +580,28 @@ def sample_training_controls(rng, Q: int, H: int, device):
 class Dataset:
     patches: object     # (S, 64, 64, 1) bf16, normalised
     start_of: object    # (N,) int32 start index of each sample
-    extra: object       # (N, 6 + 2H) fp32
+    extra: object       # (N, 6 + 3H) fp32 (``features``)
     raw: object         # (N, 3) float64 ice terms [KE, impulse, bonds]
     planner: object     # (N, 4) float64 planner components of the DEM paths
     patch_stats: tuple
     seconds: float = 0.0
 
 
+def scene_starts(field, kind: str, n: int, rng, horizon: int = 64):
+    """``n`` plan starts as ``[(eta, removed)]``: ``"open"`` water among the
+    floes (nothing removed) or mid-transit ``"channel"`` starts in the pack."""
+    if kind == "open":
+        return [(e, None) for e in sample_starts(field, n, rng, horizon)]
+    if kind == "channel":
+        return channel_starts(field, n, rng, horizon)
+    raise ValueError(f"unknown scene kind {kind!r}")
+
+
 def generate_dataset(field, n_starts: int, per_start: int, horizon: int = 64, seed: int = 0, device="cuda",
-                     patch_stats=None, weights: Optional[CostWeights] = None, **frame_kw) -> Dataset:
-    """``n_starts`` x ``per_start`` DEM rollouts (one batched launch per start)."""
+                     patch_stats=None, weights: Optional[CostWeights] = None, scenes: str = "open",
+                     **frame_kw) -> Dataset:
+    """``n_starts`` x ``per_start`` DEM rollouts (one batched launch per start)
+    from ``scenes`` starts (``scene_starts``)."""
     torch = _tm()
     from .config import get_default_simulation_config
     from .state import build_static_arrays, ship_dynamics_arrays
@@ -533,18 +611,18 @@ def generate_dataset(field, n_starts: int, per_start: int, horizon: int = 64, se
     static = build_static_arrays(field.polygons, field.centroids, field.bonds, field.thicknesses, field.parent_ids,
                                  cfg, DEFAULT_MATERIAL, 0.05)
     sd = ship_dynamics_arrays(field.ship_props, cfg, field.ship_length, field.ship_beam, field.hull_local)
-    starts = sample_starts(field, n_starts, rng, horizon)
+    starts = scene_starts(field, scenes, n_starts, rng, horizon)
     raw_patches, extras, raws, plans, start_of = [], [], [], [], []
     w = weights or CostWeights()
-    for si, e0 in enumerate(starts):
+    for si, (e0, rem) in enumerate(starts):
         nu0 = np.array([rng.uniform(1.0, 3.0), 0.0, 0.0])
-        sc = make_scene(field, e0, nu0, horizon, device=device, static=static, ship_dyn=sd)
+        sc = make_scene(field, e0, nu0, horizon, device=device, static=static, ship_dyn=sd, removed=rem)
         c0 = (COSTMAP_CELLS - PATCH_CELLS) // 2
         raw_patches.append(sc.costmap.grid[c0:c0 + PATCH_CELLS, c0:c0 + PATCH_CELLS].clone())
         Yn = sample_training_controls(rng, per_start, horizon, sc.device)
         dem = DemScorer(sc, per_start, w, **frame_kw)
         terms = dem.terms(Yn)
-        extras.append(features(sc, Yn))
+        extras.append(features(sc, Yn, rigid_path(sc, Yn)[1]))
         plans.append(terms[:, :4].clone())
         raws.append(terms[:, 4:7].clone())
         start_of.append(torch.full((per_start,), si, dtype=torch.int32, device=sc.device))
@@ -564,13 +642,15 @@ def mirror_rows(patches, extra):
     """The mirror image of training rows about the ship's start axis, in place:
     the patch flipped left-right (x about the ship), sway velocity, yaw rate,
     cos(heading) and every yaw control negated.  The hull is symmetric, so the
-    mirrored scene has the same ice terms; the patch is centred on the ship."""
+    mirrored scene has the same ice terms, and the mirrored path meets the
+    same costmap values; the patch is centred on the ship."""
     torch = _tm()
+    H = (int(extra.shape[1]) - S.N_SHIP) // S.N_STEP
     patches.copy_(torch.flip(patches, dims=[2]))
     extra[:, 1] = -extra[:, 1]
     extra[:, 2] = -extra[:, 2]
     extra[:, 3] = -extra[:, 3]
-    extra[:, S.N_SHIP + 1::2] = -extra[:, S.N_SHIP + 1::2]
+    extra[:, S.N_SHIP + 1:S.N_SHIP + 2 * H:2] = -extra[:, S.N_SHIP + 1:S.N_SHIP + 2 * H:2]
 
 
 def train_surrogate(data: Dataset, horizon: int = 64, epochs: int = 8, batch: int = 256, lr: float = 1e-3,

@@ -213,6 +213,49 @@ def costs(batch: RolloutBatch, result: RolloutResult, costmap, goal_xy, ship_len
                       out=out)
 
 
+def _device_grid(costmap):
+    import torch
+    grid = costmap.grid
+    if grid is None or not grid.is_cuda or grid.dtype != torch.float32:
+        raise ValueError("costmap.grid must be the float32 device grid")
+    return grid.contiguous()
+
+
+def _cost_params(costmap, oob_penalty, ship_length, ship_beam, goal_xy=(0.0, 0.0), action_center=ACTION_CENTER,
+                 action_scale=ACTION_SCALE, cost_truncate_y=None):
+    return _abi.DemRolloutCostParams(
+        x_origin=costmap.x_origin, y_origin=costmap.y_origin, resolution=costmap.resolution, rows=costmap.rows,
+        cols=costmap.cols, oob_penalty=oob_penalty, ship_length=ship_length, ship_beam=ship_beam,
+        goal_x=float(goal_xy[0]), goal_y=float(goal_xy[1]),
+        action_center=(C.c_double * 3)(*[float(v) for v in action_center]),
+        action_scale=(C.c_double * 3)(*[float(v) for v in action_scale]),
+        has_truncate=0 if cost_truncate_y is None else 1, reserved=0,
+        truncate_y=0.0 if cost_truncate_y is None else float(cost_truncate_y))
+
+
+def waypoint_costs(eta_hist, costmap, ship_length: float = 0.0, ship_beam: float = 0.0, oob_penalty: float = 1e8,
+                   out=None):
+    """``dem_rollout_waypoint_costs``: (Q, H) float32 costmap value of each
+    pose of the paths eta_hist (H, Q, 3) (hull centre and box corners, max)."""
+    import torch
+    lib = _abi.load_library()
+    eta_hist = eta_hist.contiguous()
+    dt = eta_hist.dtype
+    if dt not in (torch.float32, torch.float64) or eta_hist.dim() != 3 or eta_hist.shape[2] != 3:
+        raise ValueError("eta_hist must be (H,Q,3) float32 or float64")
+    H, Q = int(eta_hist.shape[0]), int(eta_hist.shape[1])
+    grid = _device_grid(costmap)
+    P = _cost_params(costmap, oob_penalty, ship_length, ship_beam)
+    if out is None:
+        out = torch.empty((Q, H), dtype=torch.float32, device=eta_hist.device)
+    rc = lib.dem_rollout_waypoint_costs(_abi.DEM_F64 if dt == torch.float64 else _abi.DEM_F32, Q, H,
+                                        eta_hist.data_ptr(), grid.data_ptr(), C.byref(P), out.data_ptr(),
+                                        C.c_void_p(torch.cuda.current_stream(eta_hist.device).cuda_stream))
+    if rc != _abi.DEM_OK:
+        raise _abi.DemError(rc, "dem_rollout_waypoint_costs failed")
+    return out
+
+
 def path_costs(eta0, eta_hist, controls, costmap, goal_xy, ship_length: float = 0.0, ship_beam: float = 0.0,
                action_center=ACTION_CENTER, action_scale=ACTION_SCALE, oob_penalty: float = 1e8,
                cost_truncate_y: Optional[float] = None, masses=None, vel0=None, vel1=None, system_start=None,
@@ -236,18 +279,9 @@ def path_costs(eta0, eta_hist, controls, costmap, goal_xy, ship_length: float = 
         controls = controls.to(dev, dt).contiguous()
         if tuple(controls.shape) != (H, Q, 3):
             raise ValueError("controls must be (H,Q,3)")
-    grid = costmap.grid
-    if grid is None or not grid.is_cuda or grid.dtype != torch.float32:
-        raise ValueError("costmap.grid must be the float32 device grid")
-    grid = grid.contiguous()
-    P = _abi.DemRolloutCostParams(
-        x_origin=costmap.x_origin, y_origin=costmap.y_origin, resolution=costmap.resolution, rows=costmap.rows,
-        cols=costmap.cols, oob_penalty=oob_penalty, ship_length=ship_length, ship_beam=ship_beam,
-        goal_x=float(goal_xy[0]), goal_y=float(goal_xy[1]),
-        action_center=(C.c_double * 3)(*[float(v) for v in action_center]),
-        action_scale=(C.c_double * 3)(*[float(v) for v in action_scale]),
-        has_truncate=0 if cost_truncate_y is None else 1, reserved=0,
-        truncate_y=0.0 if cost_truncate_y is None else float(cost_truncate_y))
+    grid = _device_grid(costmap)
+    P = _cost_params(costmap, oob_penalty, ship_length, ship_beam, goal_xy, action_center, action_scale,
+                     cost_truncate_y)
     ke = masses is not None
     if ke:
         masses, vel0, vel1 = (t.to(dev, dt).contiguous() for t in (masses, vel0, vel1))

@@ -391,6 +391,25 @@ class FrameStep:
         return self._segment(self.lib.dem_rollout_segment, 3, state, ship_state, controls_K3, v_water_Kn2,
                              v_water_ship_K2, history, check)
 
+    def alloc_history(self, K: int, history=True):
+        """Device buffers of ``K`` frames' history rows in the order of the
+        C ABI's ``DemHistory``: (pos, rot, intact, eta, submergence,
+        J_cumul_incr, F_ice_on_ship); ``history="ship"`` leaves the ice rows
+        out (``None``)."""
+        torch = _tm()
+        if history not in (True, "ship"):
+            raise ValueError("history must be True, False or 'ship'")
+        d, dev = self.dtype, self.device
+        qs = () if self.n_systems == 1 else (self.n_systems,)
+        ice = history is True
+        return (torch.empty((K, self.n, 2), dtype=d, device=dev) if ice else None,
+                torch.empty((K, self.n), dtype=d, device=dev) if ice else None,
+                torch.empty((K, self.n_bonds), dtype=torch.bool, device=dev) if ice else None,
+                torch.empty((K,) + qs + (3,), dtype=d, device=dev),
+                torch.empty((K, self.n), dtype=d, device=dev) if ice else None,
+                torch.empty((K,) + qs, dtype=d, device=dev),
+                torch.empty((K,) + qs + (2,), dtype=d, device=dev))
+
     def _segment(self, fn, row_len, state, ship_state, rows_K, v_water_Kn2, v_water_ship_K2, history, check):
         torch = _tm()
         st = self._ice_in(state)
@@ -409,17 +428,7 @@ class FrameStep:
         hist = None
         chist = None
         if history:
-            if history not in (True, "ship"):
-                raise ValueError("history must be True, False or 'ship'")
-            d, dev = self.dtype, self.device
-            ice = history is True
-            hist = (torch.empty((K, self.n, 2), dtype=d, device=dev) if ice else None,
-                    torch.empty((K, self.n), dtype=d, device=dev) if ice else None,
-                    torch.empty((K, self.n_bonds), dtype=torch.bool, device=dev) if ice else None,
-                    torch.empty((K,) + qs + (3,), dtype=d, device=dev),
-                    torch.empty((K, self.n), dtype=d, device=dev) if ice else None,
-                    torch.empty((K,) + qs, dtype=d, device=dev),
-                    torch.empty((K,) + qs + (2,), dtype=d, device=dev))
+            hist = self.alloc_history(K, history)
             chist = _abi.DemHistory(*[_ptr(t) for t in hist])
         cin, cout = self._c_state(st), self._c_state(out)
         sin, sout = self._c_ship(sh), self._c_ship(sh_out)

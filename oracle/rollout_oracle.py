@@ -37,12 +37,11 @@ def query(grid, meta, x, y, oob_penalty=1e8):
     return (val + oob).astype(f32)
 
 
-def raw_components(traj, u_norm, grid, meta, goal_xy, ship_length=0.0, ship_beam=0.0, cost_truncate_y=None,
-                   oob_penalty=1e8):
-    """[costmap, path length, goal distance, jerk] of one path traj (H+1, 3) with
-    normalised controls u_norm (H, 3) (jax_mbd_planner.py:616-663)."""
+def waypoint_costs(traj, grid, meta, ship_length=0.0, ship_beam=0.0, oob_penalty=1e8):
+    """Costmap value of each pose of traj (W, 3): the query at the hull centre
+    and its four box corners, maximum, or at the centre alone without a hull
+    (jax_mbd_planner.py:616-620)."""
     traj = np.asarray(traj, f32)
-    u_norm = np.asarray(u_norm, f32)
     grid = np.asarray(grid, f32)
     if ship_length > 0 and ship_beam > 0:
         hl, hw = float(ship_length) / 2.0, float(ship_beam) / 2.0
@@ -51,9 +50,18 @@ def raw_components(traj, u_norm, grid, meta, goal_xy, ship_length=0.0, ship_beam
         c, s = np.cos(traj[:, 2:3]), np.sin(traj[:, 2:3])
         wx = traj[:, 0:1] + c * dxb - s * dyb
         wy = traj[:, 1:2] + s * dxb + c * dyb
-        wp = query(grid, meta, wx, wy, oob_penalty).max(axis=1)
-    else:
-        wp = query(grid, meta, traj[:, 0], traj[:, 1], oob_penalty)
+        return query(grid, meta, wx, wy, oob_penalty).max(axis=1)
+    return query(grid, meta, traj[:, 0], traj[:, 1], oob_penalty)
+
+
+def raw_components(traj, u_norm, grid, meta, goal_xy, ship_length=0.0, ship_beam=0.0, cost_truncate_y=None,
+                   oob_penalty=1e8):
+    """[costmap, path length, goal distance, jerk] of one path traj (H+1, 3) with
+    normalised controls u_norm (H, 3) (jax_mbd_planner.py:616-663)."""
+    traj = np.asarray(traj, f32)
+    u_norm = np.asarray(u_norm, f32)
+    grid = np.asarray(grid, f32)
+    wp = waypoint_costs(traj, grid, meta, ship_length, ship_beam, oob_penalty)
     d = np.diff(traj[:, :2], axis=0)
     seg = np.sqrt(np.sum(d ** 2, axis=1) + f32(1e-8))
     if cost_truncate_y is not None:

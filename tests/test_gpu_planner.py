@@ -102,7 +102,7 @@ def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
     from mbd_icenav_b200 import planner
     field = bench.load_field("medium", 0)
     data = planner.generate_dataset(field, n_starts=3, per_start=256, horizon=16, seed=2, device=DEV)
-    assert data.extra.shape == (768, 6 + 32) and torch.isfinite(data.raw).all()
+    assert data.extra.shape == (768, 6 + 48) and torch.isfinite(data.raw).all()
     sur, info = planner.train_surrogate(data, horizon=16, epochs=2, batch=128, device=DEV)
     assert np.isfinite(info["train_loss"][-1])
     sc = planner.make_scene(field, planner.sample_starts(field, 1, np.random.default_rng(9), 16)[0],
@@ -154,4 +154,22 @@ def test_autotune_picks_the_fastest_split_and_caches_it(medium):
     for name, _, _ in autotune.CHOICES:
         autotune.apply(dem.batch.frame_step, name)
         assert torch.equal(dem.terms(Yn), ref), name
+    dem.batch.frame_step.close()
+
+
+def test_channel_scene_leaves_out_the_cleared_elements(medium):
+    """A mid-transit scene: the removed elements are in neither the window nor
+    the costmap (a max over elements, so no cell rises and some fall), and its
+    candidates run."""
+    from mbd_icenav_b200 import planner
+    (e0, rem), = planner.channel_starts(medium, 1, np.random.default_rng(4), 16)
+    sc = planner.make_scene(medium, e0, (2.0, 0.0, 0.0), 16, device=DEV, removed=rem)
+    full = planner.make_scene(medium, e0, (2.0, 0.0, 0.0), 16, device=DEV)
+    assert len(rem) > 0 and not np.isin(rem, sc.window).any()
+    assert set(sc.window.tolist()) == set(full.window.tolist()) - set(rem.tolist())
+    assert (sc.costmap.grid <= full.costmap.grid).all() and (sc.costmap.grid < full.costmap.grid).any()
+    w = planner.CostWeights()
+    Yn = torch.full((4, 16, 2), 0.5, dtype=torch.float32, device=DEV)
+    dem = planner.DemScorer(sc, 4, w)
+    assert torch.isfinite(dem(Yn)).all()
     dem.batch.frame_step.close()

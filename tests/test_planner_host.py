@@ -1,0 +1,60 @@
+"""Host-side planner logic without a GPU: the mid-transit channel starts."""
+import math
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+
+def _lattice_field(spacing=3.0, n=120):
+    """Square elements on a lattice covering ``n * spacing`` metres a side."""
+    xs = (np.arange(n) + 0.5) * spacing
+    cx, cy = np.meshgrid(xs, xs, indexing="ij")
+    cents = np.stack([cx.ravel(), cy.ravel()], 1)
+    h = 0.45 * spacing
+    square = np.array([[-h, -h], [h, -h], [h, h], [-h, h]])
+    return SimpleNamespace(centroids=cents, polygons=[c + square for c in cents], ship_length=60.0, ship_beam=12.0,
+                           dt=0.05, trajectory=np.array([[0.0, -40.0, math.pi / 2]]),
+                           domain=(0.0, n * spacing, 0.0, n * spacing))
+
+
+def test_channel_starts_clear_the_hull_and_the_lane_behind_it():
+    from mbd_icenav_b200 import planner
+    f = _lattice_field()
+    rng = np.random.default_rng(0)
+    radii = planner.element_radii(f)
+    assert radii == pytest.approx(np.full(len(radii), 0.45 * 3.0 * math.sqrt(2)))
+    starts = planner.channel_starts(f, 6, rng, horizon=64, clearance=2.0, channel=100.0)
+    R = planner.reach_radius(f, 64, f.dt)
+    cents = f.centroids
+    for eta, removed in starts:
+        x, y, psi = eta
+        assert abs(psi - math.pi / 2) <= 0.3
+        # the whole reach lies inside the ice
+        assert cents[:, 0].min() + R <= x <= cents[:, 0].max() - R
+        assert cents[:, 1].min() + R <= y <= cents[:, 1].max() - R
+        c, s = math.cos(psi), math.sin(psi)
+        dx, dy = cents[:, 0] - x, cents[:, 1] - y
+        bx, by = c * dx + s * dy, -s * dx + c * dy
+        r = radii + 2.0
+        lane = (bx < 30.0 + r) & (bx > -30.0 - 100.0 - r) & (np.abs(by) < 6.0 + r)
+        assert set(np.nonzero(lane)[0].tolist()) == set(np.asarray(removed).tolist())
+        # ice ahead of the bow and beside the hull stays
+        d = np.hypot(dx, dy)
+        kept = np.setdiff1d(np.nonzero(d < R)[0], removed)
+        assert len(kept) > 300 and (bx[kept] > 30.0).any()
+
+
+def test_channel_starts_need_a_field_larger_than_one_window():
+    from mbd_icenav_b200 import planner
+    with pytest.raises(ValueError):
+        planner.channel_starts(_lattice_field(n=30), 1, np.random.default_rng(0))
+
+
+def test_scene_starts_kinds():
+    from mbd_icenav_b200 import planner
+    f = _lattice_field()
+    out = planner.scene_starts(f, "channel", 2, np.random.default_rng(1))
+    assert len(out) == 2 and all(len(rem) > 0 for _, rem in out)
+    with pytest.raises(ValueError):
+        planner.scene_starts(f, "pack", 1, np.random.default_rng(1))

@@ -15,7 +15,7 @@ from types import SimpleNamespace
 import numpy as np
 import pytest
 
-from oracle.rollout_oracle import raw_components, transferred_ke
+from oracle.rollout_oracle import raw_components, transferred_ke, waypoint_costs
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "rollout_cost_golden.npz")
 RTOL = 1e-5
@@ -68,3 +68,30 @@ def test_gpu_costs_match_reference():
                                   cost_truncate_y=_trunc(g, q)).cpu().numpy()
         np.testing.assert_allclose(out[0, :4], g["raw"][q], rtol=RTOL, atol=1e-6, err_msg=f"path {q}")
         assert out[0, 4] == 0.0  # no masses given: no kinetic energy term
+
+
+@pytest.mark.gpu
+def test_gpu_waypoint_costs_match_oracle():
+    """dem_rollout_waypoint_costs: the per-pose costmap value inside the cost
+    term, for every golden path's poses after step 0, hull and centre-only;
+    within 1e-5 relative (the device's float32 sine and cosine may differ from
+    NumPy's by an ulp, which moves a corner query by as much)."""
+    torch = pytest.importorskip("torch")
+    from mbd_icenav_b200 import rollouts
+    g = np.load(GOLDEN)
+    meta = _meta(g)
+    d = torch.device("cuda", 0)
+    cm = SimpleNamespace(grid=torch.as_tensor(g["grid"], device=d), **meta)
+    for q in range(len(g["traj"])):
+        L, B = float(g["hull"][q, 0]), float(g["hull"][q, 1])
+        tr = torch.as_tensor(g["traj"][q], device=d)
+        got = rollouts.waypoint_costs(tr[1:, None, :], cm, L, B).cpu().numpy()[0]
+        want = waypoint_costs(g["traj"][q][1:], g["grid"], meta, L, B)
+        np.testing.assert_allclose(got, want, rtol=RTOL, atol=1e-6, err_msg=f"path {q}")
+    # several paths at once, laid out (H, Q, 3): row q of the output is path q
+    Hm = min(len(t) for t in g["traj"]) - 1
+    stack = np.stack([t[1:Hm + 1] for t in g["traj"]], 1)
+    got = rollouts.waypoint_costs(torch.as_tensor(stack, device=d), cm, 60.0, 12.0).cpu().numpy()
+    for q in range(stack.shape[1]):
+        np.testing.assert_allclose(got[q], waypoint_costs(stack[:, q], g["grid"], meta, 60.0, 12.0), rtol=RTOL,
+                                   atol=1e-6, err_msg=f"stacked path {q}")
