@@ -473,7 +473,7 @@ def run_ours(args, rank: int, world: int):
     bpf = algorithmic_bytes_per_frame(n, nb, V, N_SUB, n_act, nb_act)
     achieved = bpf / frame_s / 1e9
     peak, peak_kind = peak_hbm()
-    workload = f"{args.config}-seed{args.seed}-{args.dtype}"
+    workload = f"{args.config}{'-allactive' if args.all_active else ''}-seed{args.seed}-{args.dtype}"
     traffic = committed_traffic(workload)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -727,10 +727,10 @@ def run_surrogate(args, rank: int, world: int):
                                     removed=rem)
             plain = planner.DemScorer(sc, cfg.n_sample, w)
             scr = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err,
-                                         n_check=args.sur_check, seed=si)
+                                         n_check=args.sur_check, seed=si, adapt_steps=args.sur_adapt)
             # the configuration's own top-64, for comparison
             scr64 = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=64, max_rel_err=cfg.max_rel_err,
-                                           n_check=args.sur_check, seed=si)
+                                           n_check=args.sur_check, seed=si, adapt_steps=args.sur_adapt)
             # untimed: each DEM batch's work split, tuned on candidates like a plan's
             Yt = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.7, -1, 1)
             split_plain, _ = plain.autotune(Yt)
@@ -739,7 +739,9 @@ def run_surrogate(args, rank: int, world: int):
             (Yp, _), tp = timed(lambda: planner.mbd_plan(plain, cfg, device, seed=si))
             n_fb0 = scr.fallbacks
             (Ys, _), ts = timed(lambda: planner.mbd_plan(scr, cfg, device, seed=si))
+            scr.restore()  # each plan starts from the trained network
             (Ys64, _), ts64 = timed(lambda: planner.mbd_plan(scr64, cfg, device, seed=si))
+            scr64.restore()
             # the plain planner again with other samples: its own spread of plan costs
             Yp2, _ = planner.mbd_plan(plain, cfg, device, seed=si + 1000)
             cp = planner.plan_cost(sc, Yp, scr.dem_k)
@@ -805,7 +807,8 @@ def run_surrogate(args, rank: int, world: int):
                 "batched rollouts)",
         "config": {"workload": f"MBD {cfg.n_sample} samples x {cfg.n_diffuse - 1} reverse steps, horizon {H} x "
                                f"10 substeps, top {cfg.top_k} + {args.sur_check} random re-scored by the DEM, "
-                               f"fallback when the random ones beat the screened best by {cfg.max_rel_err:.0%}",
+                               f"fallback when the random ones beat the screened best by {cfg.max_rel_err:.0%}, "
+                               f"{args.sur_adapt} Adam steps per MBD step on the DEM-scored candidates",
                    "top64": {"speedup_vs_plain_dem": tp / (sum(r["top64"]["screened_s"] for r in rows) / K),
                              "plan_rel_cost_err": [r["top64"]["rel_cost_err"] for r in rows],
                              "fallback_steps": [r["top64"]["fallbacks"] for r in rows],
@@ -1049,6 +1052,8 @@ def main():
     ap.add_argument("--sur-iters", type=int, default=16, help="MBD reverse steps per plan")
     ap.add_argument("--sur-top-k", type=int, default=512, help="best-ranked candidates re-scored by the DEM per step")
     ap.add_argument("--sur-check", type=int, default=64, help="random held-out candidates re-scored per step")
+    ap.add_argument("--sur-adapt", type=int, default=4,
+                    help="Adam steps per MBD step on the candidates the DEM scored (0: the network stays fixed)")
     ap.add_argument("--sur-scenes", choices=("channel", "open"), default="channel",
                     help="plan starts: mid-transit in the pack with the ship's channel cleared, or open water")
     ap.add_argument("--all-active", action="store_true",

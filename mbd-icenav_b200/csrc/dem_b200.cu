@@ -83,6 +83,10 @@ struct DemHandle {
     int* fcoll = nullptr;
     unsigned long long* fmax = nullptr;
     double* part = nullptr;
+    // per force chunk: warm (an element in contact or submerged at the last
+    // cforce) and the stamp of the last frame with a near element
+    uint8_t* cwarm = nullptr;
+    unsigned* cnear = nullptr;
     void* kin[2] = {nullptr, nullptr};
     void* kvel[2] = {nullptr, nullptr};
     void* sp_rot[2] = {nullptr, nullptr};
@@ -374,6 +378,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     a.fcoll = h->fcoll;
     a.fmax = h->fmax;
     a.part = h->part;
+    a.cwarm = h->cwarm;
+    a.cnear = h->cnear;
     for (int i = 0; i < 2; ++i) {
         a.kin[i] = (T*)h->kin[i];
         a.kvel[i] = (T*)h->kvel[i];
@@ -720,6 +726,11 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->fcoll, sizeof(int) * nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fmax, sizeof(unsigned long long) * nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->part, sizeof(double) * 3 * std::max(h->nchunks, 1)))) return fail(rc);
+    {
+        const size_t nc = (size_t)std::max(h->nchunks, 1);
+        if ((rc = dev_alloc(h, &h->cwarm, nc))) return fail(rc);
+        if ((rc = dev_alloc(h, &h->cnear, sizeof(unsigned) * nc))) return fail(rc);
+    }
     if ((rc = dev_alloc(h, &h->sys_of, sizeof(int) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->floe_sys, sizeof(int) * nf))) return fail(rc);
     if ((rc = dev_alloc(h, &h->chunk_info, sizeof(int2) * std::max(h->nchunks, 1)))) return fail(rc);
@@ -754,6 +765,12 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     CREATE_TRY(cudaMemcpy(h->chunk_info, chunks.data(), sizeof(int2) * chunks.size(), cudaMemcpyHostToDevice));
     CREATE_TRY(cudaMemcpy(h->sys_end, sys_end.data(), sizeof(int) * h->nsys, cudaMemcpyHostToDevice));
     CREATE_TRY(cudaMemcpy(h->part_base, part_base.data(), sizeof(int) * (h->nsys + 1), cudaMemcpyHostToDevice));
+    {
+        // every first frame of a call sets the chunk flags; start from "warm"
+        const size_t nc = (size_t)std::max(h->nchunks, 1);
+        CREATE_TRY(cudaMemset(h->cwarm, 1, nc));
+        CREATE_TRY(cudaMemset(h->cnear, 0, sizeof(unsigned) * nc));
+    }
     CREATE_TRY(cudaMemcpy(h->bslot, slots.data(), sizeof(int2) * slots.size(), cudaMemcpyHostToDevice));
     {
         std::vector<int> owner(slots.size(), 0);

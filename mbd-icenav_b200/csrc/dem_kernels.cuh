@@ -151,6 +151,9 @@ struct KArgs {
     int* fcoll;         // (nf) floe touched by the ship this frame
     unsigned long long* fmax;  // (nf) max force magnitude per floe (ordered bits)
     double* part;       // (nchunks * 3) per-chunk sums: soi_x, soi_y, moment
+    // per force chunk, for phase_cforce in a call's later frames
+    uint8_t* cwarm;     // (nchunks) an element in contact or submerged at the last cforce
+    unsigned* cnear;    // (nchunks) frame stamp of the last frame with a near element
     T* kin[2];          // (n,4) {x, y, radius, radius^3} of the substep being read / written
     T* kvel[2];         // (n,2) {vx, vy} of the substep being read / written
     int* esc_list;      // (n) escaped elements of the current detection
@@ -966,6 +969,15 @@ __device__ __forceinline__ HullPose<T> hull_pose(const KArgs<T>& a, const T* eta
     return H;
 }
 
+// Force chunk of element e: chunks of kThreads elements from each system's
+// first element.
+template <typename T>
+__device__ __forceinline__ int chunk_of(const KArgs<T>& a, int e) {
+    if (a.nsys == 1) return e / kThreads;
+    const int s = a.sys_of[e];
+    return a.part_base[s] + (e - (s > 0 ? a.sys_end[s - 1] : 0)) / kThreads;
+}
+
 // ─── P_CULL: elements whose bounding circle reaches the hull; escapes ───────
 template <typename T>
 __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
@@ -983,6 +995,7 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
         a.fcoll[fl] = 0;
         a.fmax[fl] = 0ull;
     }
+    const unsigned fstamp = frame_stamp(a, F);
     for (int e = gtid; e < a.n; e += gsz) {
         typename vec2_of<T>::type p = ld2(F.src.pos, e);
         const T* eta = F.ship_src.eta + 3 * (a.nsys > 1 ? a.sys_of[e] : 0);  // this element's ship
@@ -995,6 +1008,7 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
         if (!(ddx * ddx + ddy * ddy > lim * lim * T(1.0001))) {
             const int slot = atomicAdd(a.near_cnt, 1);
             a.near_list[slot] = e;
+            a.cnear[chunk_of(a, e)] = fstamp;  // phase_cforce runs this chunk
         } else {
             a.cpen[e] = T(0);
             a.cnx[e] = T(0);
@@ -1187,13 +1201,21 @@ __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
         *a.near_cnt = 0;   // P_NEAR is done with it
         *a.comp_cnt = 0;   // P_CULL compacted the queue
     }
+    const unsigned fstamp = frame_stamp(a, F);
     for (int chunk = blockIdx.x; chunk < a.nchunks; chunk += gridDim.x) {
+        // in a call's later frames (state in place) a chunk with no element
+        // near the hull now and none in contact or submerged at the last
+        // cforce is skipped: every one of its elements would store what it
+        // holds (no ship force, no contact force, submergence 0) and its sums
+        // are the zeros it holds
+        if (F.f >= 1 && !a.cwarm[chunk] && a.cnear[chunk] != fstamp) continue;  // uniform over the CTA
         // chunks of kThreads elements start at each system's first element, so a
         // system's sums are grouped as they would be if it were simulated alone
         const int2 ci = a.chunk_info[chunk];
         const int e = ci.y + threadIdx.x;
         const T sx = F.ship_src.eta[3 * ci.x], sy = F.ship_src.eta[3 * ci.x + 1];
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        bool warm = false;
         if (e < a.sys_end[ci.x]) {
             typename vec2_of<T>::type p = ld2(F.src.pos, e);
             const T pen = a.cpen[e], nx = a.cnx[e], ny = a.cny[e];
@@ -1226,6 +1248,7 @@ __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
             st2(a.soi, e, so_x, so_y);
             a.fraw[e] = fm;
             F.dst.sub[e] = new_sub;
+            warm = has || new_sub != T(0);
             if (a.d_pen) a.d_pen[e] = pen;
             const int fl = a.floe_of[e];
             if (has) atomicMax(&a.fcoll[fl], 1);
@@ -1238,10 +1261,12 @@ __device__ void phase_cforce(const KArgs<T>& a, const Frame<T>& F) {
         }
         double r3[3];
         block_sum3<kThreads>(s0, s1, s2, r3);
+        const int any_warm = __syncthreads_or(warm ? 1 : 0);
         if (threadIdx.x == 0) {
             a.part[3 * chunk + 0] = r3[0];
             a.part[3 * chunk + 1] = r3[1];
             a.part[3 * chunk + 2] = r3[2];
+            a.cwarm[chunk] = any_warm ? 1 : 0;
         }
     }
 }

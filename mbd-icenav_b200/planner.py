@@ -328,14 +328,18 @@ class Surrogate:
     def predict(self, scene: PlanScene, Yn, wcost=None):
         """(Q, 3) float64 predicted ice terms [KE, impulse, bonds] of the
         candidates; ``wcost`` (Q, H) from ``rigid_path`` (computed when None)."""
-        torch = _tm()
-        Q = int(Yn.shape[0])
         if wcost is None:
             _, wcost = rigid_path(scene, Yn)
+        return self.predict_features(scene, features(scene, Yn, wcost))
+
+    def predict_features(self, scene: PlanScene, ext):
+        """``predict`` from the candidates' ``features`` rows (Q, 6 + 3H)."""
+        torch = _tm()
+        Q = int(ext.shape[0])
         enc = self.net.encode(scene.patch, tag="plan_enc")
         rows = self.net._buf("plan_rows", (Q,), torch.int32)
         rows.zero_()
-        out = self.net.head(enc, features(scene, Yn, wcost), enc_row=rows, tag="plan_head")
+        out = self.net.head(enc, ext, enc_row=rows, tag="plan_head")
         return self.stats.inverse(out[:, :S.N_OUT])
 
 
@@ -380,10 +384,17 @@ class ScreenedScorer:
     which the best random candidate beats the best screened one (0 when it
     does not): screening that misses better candidates than it keeps shows up
     there.  Above ``max_rel_err`` the step falls back to scoring every
-    candidate with the plain DEM."""
+    candidate with the plain DEM.
+
+    With ``adapt_steps`` > 0 the network also learns the scene as the plan
+    goes: after each step, that many Adam steps (batches of 256, learning rate
+    ``adapt_lr``) on the candidates the DEM has just scored, whose exact ice
+    terms the step has anyway (all of them after a fallback).  ``restore``
+    puts back the network the scorer started from."""
 
     def __init__(self, scene: PlanScene, surrogate: Surrogate, Q: int, weights: CostWeights, top_k: int = 64,
-                 max_rel_err: float = 0.05, n_check: int = 64, seed: int = 0, **frame_kw):
+                 max_rel_err: float = 0.05, n_check: int = 64, seed: int = 0, adapt_steps: int = 0,
+                 adapt_lr: float = 3e-4, **frame_kw):
         torch = _tm()
         self.scene = scene
         self.sur = surrogate
@@ -400,12 +411,18 @@ class ScreenedScorer:
         self.rel_errs: List[float] = []    # per step: how much the best random candidate beats the screened best
         self.pred_errs: List[float] = []   # per step: mean relative error of the predicted totals (top_k)
         self.rollouts = 0
+        self.adapt_steps = int(adapt_steps)
+        self.adapt_lr = float(adapt_lr)
+        self._base = surrogate.net.state() if self.adapt_steps > 0 else None
+        self._ext = None
+        self._pat = None
 
     def predicted(self, Yn):
         """(Q,) float64 predicted totals: rigid-path planner terms + predicted ice terms."""
         torch = _tm()
         planner, wcost = rigid_path(self.scene, Yn)
-        ice = self.sur.predict(self.scene, Yn, wcost)
+        self._ext = features(self.scene, Yn, wcost)
+        ice = self.sur.predict_features(self.scene, self._ext)
         wp = torch.tensor(self.w.planner(), dtype=torch.float64, device=Yn.device)
         wi = torch.tensor(self.w.ice(), dtype=torch.float64, device=Yn.device)
         return planner @ wp + ice @ wi
@@ -423,7 +440,8 @@ class ScreenedScorer:
         pred = self.predicted(Yn)
         top, chk = self.selection(pred)
         idx = torch.cat([top, chk])
-        exact = self.dem_k(Yn[idx].contiguous())
+        terms = self.dem_k.terms(Yn[idx].contiguous())
+        exact = self.dem_k.total(terms)
         e_top, e_chk = exact[:self.k], exact[self.k:]
         best = e_top.min()
         miss = 0.0
@@ -438,10 +456,41 @@ class ScreenedScorer:
                 self.dem_all = DemScorer(self.scene, self.Q, self.w, **self.frame_kw)
             self.fallbacks += 1
             self.rollouts += self.Q
-            return self.dem_all(Yn)
+            all_terms = self.dem_all.terms(Yn)
+            self._adapt(self._ext, all_terms[:, 4:7])
+            return self.dem_all.total(all_terms)
+        self._adapt(self._ext[idx], terms[:, 4:7])
         cost = torch.full_like(pred, float("inf"))
         cost[idx] = exact
         return cost
+
+    def _adapt(self, ext, raw):
+        """``adapt_steps`` Adam steps on rows ``ext`` with exact ice terms ``raw``."""
+        if self.adapt_steps <= 0:
+            return
+        torch = _tm()
+        net = self.sur.net
+        B = 256
+        m = int(ext.shape[0])
+        if m < B:
+            return
+        dev = ext.device
+        if self._pat is None:
+            self._pat = self.scene.patch.expand(B, -1, -1, -1).contiguous()
+            self._grad = torch.empty((B, S.OUT_ROWS), dtype=torch.bfloat16, device=dev)
+            self._loss = torch.empty(1, dtype=torch.float32, device=dev)
+        tgt = self.sur.stats.forward(raw)
+        for _ in range(self.adapt_steps):
+            pick = torch.randperm(m, generator=self.gen, device=dev)[:B]
+            out = net.forward(self._pat, ext[pick].contiguous(), keep=True)
+            sg_ops.mse(out, tgt[pick].contiguous(), S.N_OUT, self._grad, self._loss)
+            net.backward(self._grad)
+            net.adam_step(self.adapt_lr)
+
+    def restore(self):
+        """Put back the network (weights and Adam state) the scorer started from."""
+        if self._base is not None:
+            self.sur.net.load_state(self._base)
 
 
 # ─── MBD (jax_mbd_planner.py:1314-1411) ─────────────────────────────────────

@@ -137,6 +137,19 @@ class SurrogateNet:
     def params(self) -> List[Param]:
         return self.conv + self.fc
 
+    _STATE = ("p", "w", "wt", "b", "m", "v", "mb", "vb", "bw")
+
+    def state(self):
+        """A device copy of the weights and the Adam state (``load_state`` puts it back)."""
+        return [tuple(getattr(q, k).clone() for k in self._STATE) for q in self.params()], self.t
+
+    def load_state(self, st):
+        tensors, t = st
+        for q, xs in zip(self.params(), tensors):
+            for k, x in zip(self._STATE, xs):
+                getattr(q, k).copy_(x)
+        self.t = t
+
     def n_params(self) -> int:
         return sum(int(p.fan_in * p.p.shape[0] + p.p.shape[0]) for p in self.params())
 

@@ -199,3 +199,45 @@ def test_lazy_escapes_with_odd_and_even_substep_counts(golden64, k):
         fs.close()
     _assert_same(out)
     assert out[0][0].elem_active.any()
+
+
+def test_medium_field_scan_equals_single_frame_calls():
+    """A 40-frame call on the 12k-element medium field (its later frames skip
+    the force chunks that stay frozen, far from the hull and dry in the cull
+    and contact-force sweeps) equals 40 one-frame calls (every sweep complete)
+    bit for bit, with the ship pushing into the ice edge."""
+    from mbd_icenav_b200 import rollouts, scene
+    from mbd_icenav_b200.sim import build_sim_context
+    from mbd_icenav_b200.state import build_initial_ice_state, build_initial_ship_state
+    f = scene.make_medium_field(seed=2, n_frames=40)
+    K = 40
+    eta0 = rollouts.ice_edge_pose(f, gap=0.5)
+    d = np.array([np.cos(eta0[2]), np.sin(eta0[2])])
+    path = np.array([[eta0[0] + 2.0 * 0.05 * i * d[0], eta0[1] + 2.0 * 0.05 * i * d[1], eta0[2]]
+                     for i in range(K + 2)])
+    ctx = build_sim_context(f.polygons, f.centroids, f.bonds, eta0[:2], f.ship_length, f.ship_beam, K, f.dt,
+                            (0.0, 0.0), f.thicknesses, f.ship_props, parent_ids=f.parent_ids, verbose=False,
+                            n_ice_steps=f.n_ice_steps, hull_local=f.hull_local, dilation=0.05,
+                            dtype=torch.float32, device="cuda")
+    fs = ctx.frame_step
+    st0 = build_initial_ice_state(f.n, f.centroids, len(f.bonds), ctx.static.initial_floe_of.cpu().numpy(),
+                                  dtype=torch.float32, device="cuda")
+    sh0 = build_initial_ship_state(eta0[:2], float(eta0[2]), dtype=torch.float32, device="cuda")
+    dev = torch.device("cuda", 0)
+    rows = torch.as_tensor(np.concatenate([path[:K], path[1:K + 1]], 1), dtype=torch.float32, device=dev)
+    vw = torch.zeros((K, f.n, 2), dtype=torch.float32, device=dev)
+    st_a, sh_a, h_a = fs.scan_segment(st0, sh0, rows, vw)
+    st, sh = st0, sh0
+    hist = []
+    for i in range(K):
+        st, sh, h = fs.scan_segment(st, sh, rows[i:i + 1], vw[i:i + 1])
+        hist.append(h)
+    for a, b in zip(st_a, st):
+        assert torch.equal(a, b)
+    for a, b in zip(sh_a, sh):
+        assert torch.equal(a, b)
+    for j, ha in enumerate(h_a):
+        if ha is not None:
+            assert torch.equal(ha, torch.cat([h[j] for h in hist])), j
+    assert int(st_a.elem_active.sum()) > 0 and int(st_a.elem_active.sum()) < f.n // 4
+    fs.close()

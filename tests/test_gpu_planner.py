@@ -173,3 +173,37 @@ def test_channel_scene_leaves_out_the_cleared_elements(medium):
     dem = planner.DemScorer(sc, 4, w)
     assert torch.isfinite(dem(Yn)).all()
     dem.batch.frame_step.close()
+
+
+def test_screened_scorer_adapts_on_dem_scored_candidates_and_restores():
+    """With adapt_steps > 0 a step trains the network on the candidates the
+    DEM scored (the weights move, the kept costs stay the exact DEM costs) and
+    restore() puts back the weights and Adam state bit for bit."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from mbd_icenav_b200 import planner
+    field = bench.load_field("medium", 0)
+    data = planner.generate_dataset(field, n_starts=2, per_start=256, horizon=16, seed=3, device=DEV,
+                                    scenes="channel")
+    sur, _ = planner.train_surrogate(data, horizon=16, epochs=1, batch=128, device=DEV)
+    (e0, rem), = planner.channel_starts(field, 1, np.random.default_rng(11), 16)
+    sc = planner.make_scene(field, e0, (2.0, 0.0, 0.0), horizon=16, device=DEV, patch_stats=data.patch_stats,
+                            removed=rem)
+    w = planner.CostWeights()
+    Q, k, r = 512, 256, 64
+    rng = np.random.default_rng(4)
+    Yn = torch.as_tensor(np.clip(rng.normal(0.7, 0.5, (Q, 16, 2)), -1, 1), dtype=torch.float32, device=DEV)
+    before = [q.p.clone() for q in sur.net.params()]
+    t0 = sur.net.t
+    scr = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, n_check=r, max_rel_err=float("inf"), seed=1,
+                                 adapt_steps=2)
+    cost = scr(Yn)
+    kept = torch.isfinite(cost)
+    assert int(kept.sum()) == k + r
+    exact = planner.DemScorer(sc, Q, w)(Yn)
+    assert torch.equal(cost[kept], exact[kept])
+    assert sur.net.t == t0 + 2 and any(not torch.equal(a, q.p) for a, q in zip(before, sur.net.params()))
+    scr.restore()
+    assert sur.net.t == t0 and all(torch.equal(a, q.p) for a, q in zip(before, sur.net.params()))

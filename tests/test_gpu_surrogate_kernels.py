@@ -36,8 +36,11 @@ def _ref_gemm(A, B, bias=None, relu=False, mask=None):
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 128, 128), (300, 200, 200), (1000, 64, 576),
-                                   (4096, 512, 2240), (130, 3, 512), (77, 96, 8), (2048, 128, 1152)])
+                                   (4096, 512, 2240), (130, 3, 512), (77, 96, 8), (2048, 128, 1152),
+                                   (8192, 512, 2304), (16000, 600, 200)])
 def test_gemm_matches_fp32_reference(M, N, K):
+    """Every tile width: 64 (N <= 64), 128, and 256 (N >= 512 with at least 128
+    tiles of 128 x 256: the last two shapes, one with ragged M and N edges)."""
     ops = _ops()
     g = torch.Generator().manual_seed(M * 7 + N * 3 + K)
     A, B = _bf((M, K), g), _bf((N, K), g)
