@@ -731,23 +731,30 @@ def run_surrogate(args, rank: int, world: int):
             # the configuration's own top-64, for comparison
             scr64 = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=64, max_rel_err=cfg.max_rel_err,
                                            n_check=args.sur_check, seed=si, adapt_steps=args.sur_adapt)
+            # the same screening with the network learning the scene as the plan goes
+            scra = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err,
+                                          n_check=args.sur_check, seed=si, adapt_steps=args.sur_compare_adapt)
             # untimed: each DEM batch's work split, tuned on candidates like a plan's
             Yt = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.7, -1, 1)
             split_plain, _ = plain.autotune(Yt)
             split_k, _ = scr.dem_k.autotune(Yt[:scr.dem_k.Q].contiguous())
             scr64.dem_k.autotune(Yt[:scr64.dem_k.Q].contiguous())
+            scra.dem_k.autotune(Yt[:scra.dem_k.Q].contiguous())
             (Yp, _), tp = timed(lambda: planner.mbd_plan(plain, cfg, device, seed=si))
             n_fb0 = scr.fallbacks
             (Ys, _), ts = timed(lambda: planner.mbd_plan(scr, cfg, device, seed=si))
             scr.restore()  # each plan starts from the trained network
             (Ys64, _), ts64 = timed(lambda: planner.mbd_plan(scr64, cfg, device, seed=si))
             scr64.restore()
+            (Ysa, _), tsa = timed(lambda: planner.mbd_plan(scra, cfg, device, seed=si))
+            scra.restore()
             # the plain planner again with other samples: its own spread of plan costs
             Yp2, _ = planner.mbd_plan(plain, cfg, device, seed=si + 1000)
             cp = planner.plan_cost(sc, Yp, scr.dem_k)
             cs = planner.plan_cost(sc, Ys, scr.dem_k)
             cp2 = planner.plan_cost(sc, Yp2, scr.dem_k)
             cs64 = planner.plan_cost(sc, Ys64, scr.dem_k)
+            csa = planner.plan_cost(sc, Ysa, scr.dem_k)
             if si >= args.warmup:
                 rows.append({"plain_s": tp, "screened_s": ts, "plain_cost": cp, "screened_cost": cs,
                              "plain_cost_other_seed": cp2,
@@ -759,14 +766,18 @@ def run_surrogate(args, rank: int, world: int):
                              "work_split": [split_plain, split_k],
                              "top64": {"screened_s": ts64, "screened_cost": cs64,
                                        "rel_cost_err": abs(cs64 - cp) / max(abs(cp), 1e-9),
-                                       "fallbacks": scr64.fallbacks, "check_miss_max": float(np.max(scr64.rel_errs))}})
+                                       "fallbacks": scr64.fallbacks, "check_miss_max": float(np.max(scr64.rel_errs))},
+                             "adaptive": {"screened_s": tsa, "screened_cost": csa,
+                                          "rel_cost_err": abs(csa - cp) / max(abs(cp), 1e-9),
+                                          "fallbacks": scra.fallbacks,
+                                          "check_miss_max": float(np.max(scra.rel_errs))}})
                 sys.stderr.write(f"plan {si}: {json.dumps(rows[-1])}\n")
             plain.batch.frame_step.close()
-            for z in (scr, scr64):
+            for z in (scr, scr64, scra):
                 z.dem_k.batch.frame_step.close()
                 if z.dem_all is not None:
                     z.dem_all.batch.frame_step.close()
-            del plain, scr, scr64
+            del plain, scr, scr64, scra
     # tensor-pipe figure: the screening's own network work on one plan's
     # population, the head over n_sample rows after one encoder pass, timed alone
     sc = planner.make_scene(field, starts[-1][0], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats,
@@ -808,11 +819,16 @@ def run_surrogate(args, rank: int, world: int):
         "config": {"workload": f"MBD {cfg.n_sample} samples x {cfg.n_diffuse - 1} reverse steps, horizon {H} x "
                                f"10 substeps, top {cfg.top_k} + {args.sur_check} random re-scored by the DEM, "
                                f"fallback when the random ones beat the screened best by {cfg.max_rel_err:.0%}, "
-                               f"{args.sur_adapt} Adam steps per MBD step on the DEM-scored candidates",
+                               f"{args.sur_adapt} Adam steps per MBD step on the check set",
                    "top64": {"speedup_vs_plain_dem": tp / (sum(r["top64"]["screened_s"] for r in rows) / K),
                              "plan_rel_cost_err": [r["top64"]["rel_cost_err"] for r in rows],
                              "fallback_steps": [r["top64"]["fallbacks"] for r in rows],
                              "note": "the same plans with only the 64 best-ranked candidates re-scored"},
+                   "adaptive": {"speedup_vs_plain_dem": tp / (sum(r["adaptive"]["screened_s"] for r in rows) / K),
+                                "plan_rel_cost_err": [r["adaptive"]["rel_cost_err"] for r in rows],
+                                "fallback_steps": [r["adaptive"]["fallbacks"] for r in rows],
+                                "note": f"the same plans with {args.sur_compare_adapt} Adam steps per MBD step on "
+                                        f"the check set (every candidate after a fallback)"},
                    "scenes": args.sur_scenes, "windows": [r["window"] for r in rows],
                    "plain_dem_rollouts_per_s": plain_rate, "speedup_vs_plain_dem": value / plain_rate,
                    "plan_rel_cost_err": errs, "plan_rel_cost_err_max": max(errs),
@@ -1052,8 +1068,10 @@ def main():
     ap.add_argument("--sur-iters", type=int, default=16, help="MBD reverse steps per plan")
     ap.add_argument("--sur-top-k", type=int, default=512, help="best-ranked candidates re-scored by the DEM per step")
     ap.add_argument("--sur-check", type=int, default=64, help="random held-out candidates re-scored per step")
-    ap.add_argument("--sur-adapt", type=int, default=4,
-                    help="Adam steps per MBD step on the candidates the DEM scored (0: the network stays fixed)")
+    ap.add_argument("--sur-adapt", type=int, default=0,
+                    help="Adam steps per MBD step on the check set the DEM scored (0: the network stays fixed)")
+    ap.add_argument("--sur-compare-adapt", type=int, default=4,
+                    help="Adam steps per MBD step of the adaptive comparison plans")
     ap.add_argument("--sur-scenes", choices=("channel", "open"), default="channel",
                     help="plan starts: mid-transit in the pack with the ship's channel cleared, or open water")
     ap.add_argument("--all-active", action="store_true",

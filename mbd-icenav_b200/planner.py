@@ -387,10 +387,12 @@ class ScreenedScorer:
     candidate with the plain DEM.
 
     With ``adapt_steps`` > 0 the network also learns the scene as the plan
-    goes: after each step, that many Adam steps (batches of 256, learning rate
-    ``adapt_lr``) on the candidates the DEM has just scored, whose exact ice
-    terms the step has anyway (all of them after a fallback).  ``restore``
-    puts back the network the scorer started from."""
+    goes: after each step, that many Adam steps (batches of up to 256,
+    learning rate ``adapt_lr``) on the step's unbiased DEM samples, whose exact
+    ice terms the step has anyway: the random check set, or every candidate
+    after a fallback.  (The screened top-k are the network's own picks;
+    training on them teaches it that its picks are good.)  ``restore`` puts
+    back the network the scorer started from."""
 
     def __init__(self, scene: PlanScene, surrogate: Surrogate, Q: int, weights: CostWeights, top_k: int = 64,
                  max_rel_err: float = 0.05, n_check: int = 64, seed: int = 0, adapt_steps: int = 0,
@@ -459,7 +461,8 @@ class ScreenedScorer:
             all_terms = self.dem_all.terms(Yn)
             self._adapt(self._ext, all_terms[:, 4:7])
             return self.dem_all.total(all_terms)
-        self._adapt(self._ext[idx], terms[:, 4:7])
+        if self.n_check:
+            self._adapt(self._ext[chk], terms[self.k:, 4:7])
         cost = torch.full_like(pred, float("inf"))
         cost[idx] = exact
         return cost
@@ -470,21 +473,21 @@ class ScreenedScorer:
             return
         torch = _tm()
         net = self.sur.net
-        B = 256
         m = int(ext.shape[0])
-        if m < B:
+        B = min(256, m)
+        if B < 16:
             return
         dev = ext.device
         if self._pat is None:
-            self._pat = self.scene.patch.expand(B, -1, -1, -1).contiguous()
-            self._grad = torch.empty((B, S.OUT_ROWS), dtype=torch.bfloat16, device=dev)
+            self._pat = self.scene.patch.expand(256, -1, -1, -1).contiguous()
+            self._grad = torch.empty((256, S.OUT_ROWS), dtype=torch.bfloat16, device=dev)
             self._loss = torch.empty(1, dtype=torch.float32, device=dev)
         tgt = self.sur.stats.forward(raw)
         for _ in range(self.adapt_steps):
             pick = torch.randperm(m, generator=self.gen, device=dev)[:B]
-            out = net.forward(self._pat, ext[pick].contiguous(), keep=True)
-            sg_ops.mse(out, tgt[pick].contiguous(), S.N_OUT, self._grad, self._loss)
-            net.backward(self._grad)
+            out = net.forward(self._pat[:B], ext[pick].contiguous(), keep=True)
+            sg_ops.mse(out, tgt[pick].contiguous(), S.N_OUT, self._grad[:B], self._loss)
+            net.backward(self._grad[:B])
             net.adam_step(self.adapt_lr)
 
     def restore(self):
