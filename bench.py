@@ -783,7 +783,7 @@ def run_surrogate(args, rank: int, world: int):
     sc = planner.make_scene(field, starts[-1][0], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats,
                             removed=starts[-1][1])
     Yn = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.5, -1, 1)
-    ext = planner.features(sc, Yn, planner.rigid_path(sc, Yn)[1])
+    ext = planner.features(sc, Yn, *planner.rigid_path(sc, Yn)[1:])
     rows0 = torch.zeros(cfg.n_sample, dtype=torch.int32, device=device)
     enc = sur.net.encode(sc.patch, tag="bench_enc")
     for _ in range(3):

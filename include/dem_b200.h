@@ -392,6 +392,30 @@ int dem_ship_rollout(const DemParams* params, int32_t dtype, int32_t n_rollouts,
                      const void* nu0, const void* controls, const void* v_water_ship, void* eta_hist, void* nu_out,
                      void* stream);
 
+/* Features of dem_rollout_sweep_features, and its limits. */
+#define DEM_SWEEP_FEATURES 8
+#define DEM_SWEEP_MAX_ELEMENTS 65536
+#define DEM_SWEEP_MAX_HORIZON 512
+
+/* What each candidate's rigid-ship path sweeps through the plan's ice window
+ * (no reference counterpart: inputs of the screening surrogate, beside the
+ * path's costmap values).  Poses: eta0[q] (Q,3) and eta_hist[t, q] (H,Q,3)
+ * of `dtype`, from dem_ship_rollout.  An element e of the window (positions
+ * (n,2), radii, masses (n,) of `dtype`) is hit at the first pose t = 0..H
+ * whose frame puts its centroid inside the hull box grown by its radius
+ * (|x| < half_len + r, |y| < half_beam + r); the hit's velocity is the path's
+ * step velocity (pose t - pose t-1) / dt (the first step's at t = 0) and v_n
+ * its component towards the centroid, clamped at 0.  out (Q, 8) float32 =
+ * [elements hit, their mass, sum 0.5 m |v|^2, sum m v_n,
+ * sum m (H + 1 - t) / (H + 1), sum 0.5 m v_n^2, bonds (bond_i, bond_j (nb)
+ * int32 window indices) with one end hit, bonds with both ends hit], summed in
+ * double in a fixed order.  Device arrays; n <= DEM_SWEEP_MAX_ELEMENTS,
+ * 1 <= horizon <= DEM_SWEEP_MAX_HORIZON. */
+int dem_rollout_sweep_features(int32_t dtype, int32_t n_rollouts, int32_t horizon, const void* eta0,
+                               const void* eta_hist, int32_t n, const void* positions, const void* radii,
+                               const void* masses, int32_t n_bonds, const int32_t* bond_i, const int32_t* bond_j,
+                               double half_len, double half_beam, double dt, float* out, void* stream);
+
 /* Largest n accepted by dem_ship_contact_noalloc. */
 #define DEM_CONTACT_NOALLOC_MAX_ELEMENTS 262144
 

@@ -119,7 +119,7 @@ EXPORTS = ("dem_create", "dem_frame_step", "dem_scan_segment", "dem_sync_status"
            "dem_set_capacity", "dem_set_launch_mode", "dem_set_work_split", "dem_get_info", "dem_set_profiling",
            "dem_get_phase_times", "dem_get_error", "dem_destroy", "dem_version", "dem_debug_fail_barrier", "dem_ke_costmap", "dem_rollout_segment",
            "dem_rollout_costs", "dem_debug_record_contacts", "dem_rollout_ice_terms", "dem_ship_rollout",
-           "dem_rollout_waypoint_costs")
+           "dem_rollout_waypoint_costs", "dem_rollout_sweep_features")
 
 _LIB = None
 
@@ -165,6 +165,8 @@ def load_library(path: str = None):
     lib.dem_rollout_costs.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, C.POINTER(DemRolloutCostParams), _vp,
                                       _vp, _vp, _vp, _vp]
     lib.dem_rollout_waypoint_costs.argtypes = [_i, _i, _i, _vp, _vp, C.POINTER(DemRolloutCostParams), _vp, _vp]
+    lib.dem_rollout_sweep_features.argtypes = [_i, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _d, _d, _d,
+                                               _vp, _vp]
     lib.dem_version.restype = C.c_char_p
     _bind_surrogate(lib)
     for name in EXPORTS:

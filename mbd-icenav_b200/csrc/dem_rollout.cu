@@ -307,3 +307,141 @@ extern "C" int dem_rollout_ice_terms(int32_t dtype, int32_t n_systems, int32_t h
                                                                    bond_start, intact0, intact1, out);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
+
+// ════════════════════════════════════════════════════════════════════════════
+// dem_rollout_sweep_features: what a candidate's rigid-ship path sweeps
+// through the plan's ice window, one CTA per candidate.  No counterpart in the
+// reference.  An element is hit at the first pose t (0..H) at which its
+// centroid, in the frame of that pose, lies inside the hull box grown by the
+// element's radius r: |x| < half_len + r and |y| < half_beam + r.  The hit's
+// ship velocity is the path's step velocity (pose t - pose t-1) / dt (the
+// first step's for t = 0), and v_n its component towards the element's
+// centroid, clamped at 0.  Per candidate, in double with fixed-order sums (run
+// to run identical):
+//   [0] elements hit, [1] their mass, [2] sum 0.5 m |v|^2, [3] sum m v_n,
+//   [4] sum m (H + 1 - t) / (H + 1) (early hits weigh more), [5] sum 0.5 m v_n^2,
+//   [6] bonds with exactly one end hit, [7] bonds with both ends hit.
+// The geometry runs in float32 (cos and sin of the heading rounded from
+// double), unfused, as a NumPy float32 evaluation of the same expressions.
+// ════════════════════════════════════════════════════════════════════════════
+namespace {
+
+constexpr int kSwThreads = 256;
+constexpr int kSwFeatures = DEM_SWEEP_FEATURES;
+constexpr int kSwMaxElements = DEM_SWEEP_MAX_ELEMENTS;  // hit bits in shared memory: 8 KB
+constexpr int kSwMaxHorizon = DEM_SWEEP_MAX_HORIZON;
+
+struct SwArgs {
+    int Q, H, n, nb;
+    float hl, hw, inv_dt;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kSwThreads) sweep_kernel(const SwArgs c, const T* __restrict__ eta0,
+                                                           const T* __restrict__ hist, const T* __restrict__ pos,
+                                                           const T* __restrict__ radii, const T* __restrict__ mass,
+                                                           const int* __restrict__ bi, const int* __restrict__ bj,
+                                                           float* __restrict__ out) {
+    __shared__ float4 pose[kSwMaxHorizon + 1];  // x, y, cos, sin
+    __shared__ float2 pvel[kSwMaxHorizon + 1];
+    __shared__ unsigned hit[kSwMaxElements / 32];
+    __shared__ double red[kSwThreads];
+    const int q = blockIdx.x;
+    const int H = c.H;
+    for (int t = threadIdx.x; t <= H; t += blockDim.x) {
+        const T* p = (t == 0) ? eta0 + 3 * (size_t)q : hist + ((size_t)(t - 1) * c.Q + q) * 3;
+        const double psi = (double)p[2];
+        pose[t] = make_float4((float)p[0], (float)p[1], (float)cos(psi), (float)sin(psi));
+    }
+    for (int w = threadIdx.x; w < (c.n + 31) / 32; w += blockDim.x) hit[w] = 0u;
+    __syncthreads();
+    for (int t = threadIdx.x; t <= H; t += blockDim.x) {
+        const int a = (t == 0) ? 1 : t;  // the first step's velocity at the start pose
+        pvel[t] = make_float2((pose[a].x - pose[a - 1].x) * c.inv_dt, (pose[a].y - pose[a - 1].y) * c.inv_dt);
+    }
+    __syncthreads();
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int e = threadIdx.x; e < c.n; e += blockDim.x) {
+        const float ex = (float)pos[2 * (size_t)e], ey = (float)pos[2 * (size_t)e + 1];
+        const float r = (float)radii[e];
+        // a centroid inside the grown box lies within its half-diagonal of the
+        // pose (the margin covers the rounding of the rotation): a cheaper
+        // first test that rejects no hit
+        const float gl = c.hl + r, gw = c.hw + r;
+        const float lim2 = (gl * gl + gw * gw) * 1.001f + 1e-3f;
+        for (int t = 0; t <= H; ++t) {
+            const float4 p = pose[t];
+            const float dx = ex - p.x, dy = ey - p.y;
+            if (dx * dx + dy * dy > lim2) continue;
+            const float bx = p.z * dx + p.w * dy;
+            const float by = p.z * dy - p.w * dx;
+            if (!(fabsf(bx) < gl && fabsf(by) < gw)) continue;
+            const double m = (double)mass[e];
+            const double vx = (double)pvel[t].x, vy = (double)pvel[t].y;
+            const double dd = sqrt((double)dx * (double)dx + (double)dy * (double)dy);
+            const double vn = fmax(0.0, (vx * (double)dx + vy * (double)dy) / fmax(dd, 1e-6));
+            acc[0] += 1.0;
+            acc[1] += m;
+            acc[2] += 0.5 * m * (vx * vx + vy * vy);
+            acc[3] += m * vn;
+            acc[4] += m * (double)(H + 1 - t) / (double)(H + 1);
+            acc[5] += 0.5 * m * vn * vn;
+            atomicOr(&hit[e >> 5], 1u << (e & 31));
+            break;
+        }
+    }
+    __syncthreads();
+    double b1 = 0.0, b2 = 0.0;
+    for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
+        const int i = bi[b], j = bj[b];
+        if (i < 0 || i >= c.n || j < 0 || j >= c.n) continue;
+        const bool hi = (hit[i >> 5] >> (i & 31)) & 1u, hj = (hit[j >> 5] >> (j & 31)) & 1u;
+        b1 += (hi != hj) ? 1.0 : 0.0;
+        b2 += (hi && hj) ? 1.0 : 0.0;
+    }
+    const double v[kSwFeatures] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], b1, b2};
+    for (int k = 0; k < kSwFeatures; ++k) {
+        red[threadIdx.x] = v[k];
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[(size_t)q * kSwFeatures + k] = (float)red[0];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+extern "C" int dem_rollout_sweep_features(int32_t dtype, int32_t n_rollouts, int32_t horizon, const void* eta0,
+                                          const void* eta_hist, int32_t n, const void* positions, const void* radii,
+                                          const void* masses, int32_t n_bonds, const int32_t* bond_i,
+                                          const int32_t* bond_j, double half_len, double half_beam, double dt,
+                                          float* out, void* stream) {
+    if ((dtype != DEM_F32 && dtype != DEM_F64) || n_rollouts < 1 || horizon < 1 || horizon > kSwMaxHorizon)
+        return DEM_ERR_INVALID;
+    if (n < 0 || n > kSwMaxElements || n_bonds < 0 || !(dt > 0.0) || !(half_len >= 0.0) || !(half_beam >= 0.0))
+        return DEM_ERR_INVALID;
+    if (!eta0 || !eta_hist || !out || (n > 0 && (!positions || !radii || !masses)) ||
+        (n_bonds > 0 && (!bond_i || !bond_j)))
+        return DEM_ERR_INVALID;
+    SwArgs c{};
+    c.Q = n_rollouts;
+    c.H = horizon;
+    c.n = n;
+    c.nb = n_bonds;
+    c.hl = (float)half_len;
+    c.hw = (float)half_beam;
+    c.inv_dt = (float)(1.0 / dt);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == DEM_F32)
+        sweep_kernel<float><<<n_rollouts, kSwThreads, 0, st>>>(c, (const float*)eta0, (const float*)eta_hist,
+                                                                (const float*)positions, (const float*)radii,
+                                                                (const float*)masses, bond_i, bond_j, out);
+    else
+        sweep_kernel<double><<<n_rollouts, kSwThreads, 0, st>>>(c, (const double*)eta0, (const double*)eta_hist,
+                                                                 (const double*)positions, (const double*)radii,
+                                                                 (const double*)masses, bond_i, bond_j, out);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}

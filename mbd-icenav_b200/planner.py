@@ -103,6 +103,7 @@ class PlanScene:
     params: object           # DemParams (vessel constants for the rigid rollout)
     dtype: object
     device: object
+    sweep: object = None     # device inputs of dem_rollout_sweep_features (``sweep_inputs``)
 
 
 PATCH_CELLS = S.PATCH
@@ -227,18 +228,26 @@ def physical_controls(Yn):
     return torch.stack([X, torch.zeros_like(X), N], -1).transpose(0, 1).contiguous()
 
 
-def features(scene: PlanScene, Yn, wcost):
-    """(Q, 6 + 3H) fp32 network inputs besides the patch: ship state [u/5, v/2,
-    r/0.1, cos psi, sin psi, 0], the normalised controls step by step, and
+# scales of the sweep features before log1p: elements, kg, J, N s, kg, J, bonds, bonds
+SWEEP_SCALE = (1.0, 1e3, 1e3, 1e3, 1e3, 1e3, 1.0, 1.0)
+
+
+def features(scene: PlanScene, Yn, wcost, sweep):
+    """(Q, 6 + 3H + 8) fp32 network inputs besides the patch: ship state [u/5,
+    v/2, r/0.1, cos psi, sin psi, 0], the normalised controls step by step,
     log1p of ``wcost`` (Q, H), the costmap value at each pose of the
-    candidate's rigid-ship path (``rigid_path``)."""
+    candidate's rigid-ship path, and log1p of ``sweep`` (Q, 8), what that path
+    sweeps through the ice window, over ``SWEEP_SCALE`` (both from
+    ``rigid_path``)."""
     torch = _tm()
     Q, H, _ = Yn.shape
     e, v = scene.eta0, scene.nu0
     ship = torch.tensor([v[0] / 5.0, v[1] / 2.0, v[2] / 0.1, math.cos(e[2]), math.sin(e[2]), 0.0],
                         dtype=torch.float32, device=Yn.device)
     path = torch.log1p(torch.clamp(wcost.float(), min=0.0))
-    return torch.cat([ship.expand(Q, S.N_SHIP), Yn.reshape(Q, 2 * H).float(), path], 1).contiguous()
+    sc = torch.tensor(SWEEP_SCALE, dtype=torch.float32, device=Yn.device)
+    sw = torch.log1p(torch.clamp(sweep.float(), min=0.0) / sc)
+    return torch.cat([ship.expand(Q, S.N_SHIP), Yn.reshape(Q, 2 * H).float(), path, sw], 1).contiguous()
 
 
 # ─── target transforms ──────────────────────────────────────────────────────
@@ -325,12 +334,11 @@ class Surrogate:
         self.stats = stats
         self.patch_stats = patch_stats
 
-    def predict(self, scene: PlanScene, Yn, wcost=None):
+    def predict(self, scene: PlanScene, Yn):
         """(Q, 3) float64 predicted ice terms [KE, impulse, bonds] of the
-        candidates; ``wcost`` (Q, H) from ``rigid_path`` (computed when None)."""
-        if wcost is None:
-            _, wcost = rigid_path(scene, Yn)
-        return self.predict_features(scene, features(scene, Yn, wcost))
+        candidates (their rigid-ship paths from ``rigid_path``)."""
+        _, wcost, sweep = rigid_path(scene, Yn)
+        return self.predict_features(scene, features(scene, Yn, wcost, sweep))
 
     def predict_features(self, scene: PlanScene, ext):
         """``predict`` from the candidates' ``features`` rows (Q, 6 + 3H)."""
@@ -348,10 +356,53 @@ def rigid_terms(scene: PlanScene, Yn, out=None):
     return rigid_path(scene, Yn, out)[0]
 
 
+def sweep_inputs(scene: PlanScene):
+    """The window's elements (start positions, radii, masses) and its bonds in
+    window indices, on the device (cached on the scene)."""
+    if scene.sweep is not None:
+        return scene.sweep
+    torch = _tm()
+    st = scene.static
+    w = np.asarray(scene.window, np.int64)
+    local = -np.ones(np.asarray(st.masses).shape[0], np.int64)
+    local[w] = np.arange(len(w))
+    bi, bj = np.asarray(st.bond_i, np.int64), np.asarray(st.bond_j, np.int64)
+    keep = (local[bi] >= 0) & (local[bj] >= 0)
+    dev, d = scene.device, scene.dtype
+    scene.sweep = SimpleNamespace(
+        n=len(w), nb=int(keep.sum()),
+        pos=torch.as_tensor(np.asarray(scene.field.centroids, np.float64)[w], dtype=d, device=dev).contiguous(),
+        radii=torch.as_tensor(np.asarray(st.radii, np.float64)[w], dtype=d, device=dev),
+        masses=torch.as_tensor(np.asarray(st.masses, np.float64)[w], dtype=d, device=dev),
+        bi=torch.as_tensor(local[bi[keep]], dtype=torch.int32, device=dev),
+        bj=torch.as_tensor(local[bj[keep]], dtype=torch.int32, device=dev))
+    return scene.sweep
+
+
+def sweep_features(scene: PlanScene, eta0, hist):
+    """``dem_rollout_sweep_features``: (Q, 8) float32, what each pose path
+    eta0 (Q, 3), hist (H, Q, 3) sweeps through the scene's ice window."""
+    torch = _tm()
+    lib = _abi.load_library()
+    H, Q, _ = hist.shape
+    w = sweep_inputs(scene)
+    out = torch.empty((Q, S.N_SWEEP), dtype=torch.float32, device=hist.device)
+    f = scene.field
+    rc = lib.dem_rollout_sweep_features(_abi.DEM_F64 if hist.dtype == torch.float64 else _abi.DEM_F32, Q, H,
+                                        eta0.data_ptr(), hist.data_ptr(), w.n, w.pos.data_ptr(),
+                                        w.radii.data_ptr(), w.masses.data_ptr(), w.nb, w.bi.data_ptr(),
+                                        w.bj.data_ptr(), 0.5 * f.ship_length, 0.5 * f.ship_beam, float(f.dt),
+                                        out.data_ptr(), torch.cuda.current_stream(hist.device).cuda_stream)
+    if rc != _abi.DEM_OK:
+        raise _abi.DemError(rc, "dem_rollout_sweep_features failed")
+    return out
+
+
 def rigid_path(scene: PlanScene, Yn, out=None):
     """The candidates' rigid-ship paths (``dem_ship_rollout``): their (Q, 4)
-    float64 planner components and the (Q, H) float32 costmap value at each
-    pose (``dem_rollout_waypoint_costs``)."""
+    float64 planner components, the (Q, H) float32 costmap value at each pose
+    (``dem_rollout_waypoint_costs``) and the (Q, 8) float32 sweep features
+    (``sweep_features``)."""
     torch = _tm()
     lib = _abi.load_library()
     Q, H, _ = Yn.shape
@@ -369,7 +420,7 @@ def rigid_path(scene: PlanScene, Yn, out=None):
     comp = rollouts.path_costs(eta0, hist, u, scene.costmap, scene.goal, scene.field.ship_length,
                                scene.field.ship_beam, out=out)
     wcost = rollouts.waypoint_costs(hist, scene.costmap, scene.field.ship_length, scene.field.ship_beam)
-    return comp[:, :4], wcost
+    return comp[:, :4], wcost, sweep_features(scene, eta0, hist)
 
 
 class ScreenedScorer:
@@ -422,8 +473,8 @@ class ScreenedScorer:
     def predicted(self, Yn):
         """(Q,) float64 predicted totals: rigid-path planner terms + predicted ice terms."""
         torch = _tm()
-        planner, wcost = rigid_path(self.scene, Yn)
-        self._ext = features(self.scene, Yn, wcost)
+        planner, wcost, sweep = rigid_path(self.scene, Yn)
+        self._ext = features(self.scene, Yn, wcost, sweep)
         ice = self.sur.predict_features(self.scene, self._ext)
         wp = torch.tensor(self.w.planner(), dtype=torch.float64, device=Yn.device)
         wi = torch.tensor(self.w.ice(), dtype=torch.float64, device=Yn.device)
@@ -674,7 +725,7 @@ def generate_dataset(field, n_starts: int, per_start: int, horizon: int = 64, se
         Yn = sample_training_controls(rng, per_start, horizon, sc.device)
         dem = DemScorer(sc, per_start, w, **frame_kw)
         terms = dem.terms(Yn)
-        extras.append(features(sc, Yn, rigid_path(sc, Yn)[1]))
+        extras.append(features(sc, Yn, *rigid_path(sc, Yn)[1:]))
         plans.append(terms[:, :4].clone())
         raws.append(terms[:, 4:7].clone())
         start_of.append(torch.full((per_start,), si, dtype=torch.int32, device=sc.device))
@@ -695,9 +746,10 @@ def mirror_rows(patches, extra):
     the patch flipped left-right (x about the ship), sway velocity, yaw rate,
     cos(heading) and every yaw control negated.  The hull is symmetric, so the
     mirrored scene has the same ice terms, and the mirrored path meets the
-    same costmap values; the patch is centred on the ship."""
+    same costmap values and sweeps the same ice; the patch is centred on the
+    ship."""
     torch = _tm()
-    H = (int(extra.shape[1]) - S.N_SHIP) // S.N_STEP
+    H = (int(extra.shape[1]) - S.N_SHIP - S.N_SWEEP) // S.N_STEP
     patches.copy_(torch.flip(patches, dims=[2]))
     extra[:, 1] = -extra[:, 1]
     extra[:, 2] = -extra[:, 2]

@@ -13,8 +13,9 @@ Network (per sample):
        channels (64 -> 32 -> 16 -> 8 -> 4 pixels), as im2col + GEMM
     -> flatten 4 x 4 x 128 = 2048
   [2048 | ship state (6) | controls (H x 2) | log1p of the costmap value at
-  each pose of the candidate's rigid-ship path (H)] zero-padded to a multiple
-  of 64
+  each pose of the candidate's rigid-ship path (H) | log1p of what that path
+  sweeps through the ice window (8: elements hit, their mass, kinetic-energy
+  and momentum proxies, bonds cut)] zero-padded to a multiple of 64
     -> 3 x [fully connected 512, ReLU] -> fully connected 3
   outputs: the standardised log1p transforms of (ice kinetic energy
   transferred, hull impulse, bonds broken).
@@ -54,6 +55,7 @@ N_OUT = 3
 OUT_ROWS = 64  # stored rows of the output layer (N_OUT live)
 N_SHIP = 6
 N_STEP = 3  # per-step inputs: normalised surge and yaw controls, the path's costmap value
+N_SWEEP = 8  # what the rigid-ship path sweeps through the ice window (dem_rollout_sweep_features)
 
 
 def kpad_of(c_in: int) -> int:
@@ -66,7 +68,7 @@ def enc_dim() -> int:
 
 
 def x_dim(horizon: int) -> int:
-    return ((enc_dim() + N_SHIP + N_STEP * horizon + 63) // 64) * 64
+    return ((enc_dim() + N_SHIP + N_STEP * horizon + N_SWEEP + 63) // 64) * 64
 
 
 def flops_per_sample(horizon: int) -> dict:
@@ -105,7 +107,7 @@ class SurrogateNet:
         self.device = torch.device(device)
         self.horizon = int(horizon)
         self.xdim = x_dim(horizon)
-        self.n_extra = N_SHIP + N_STEP * self.horizon
+        self.n_extra = N_SHIP + N_STEP * self.horizon + N_SWEEP
         gen = torch.Generator().manual_seed(seed)
         self.conv: List[Param] = []
         for cin, cout in CONV:

@@ -92,3 +92,56 @@ def transferred_ke(masses, v0, v1, system_start):
     e = 0.5 * m * ((b ** 2).sum(1) - (a ** 2).sum(1))
     s = np.asarray(system_start)
     return np.array([e[s[q]:s[q + 1]].sum() for q in range(len(s) - 1)])
+
+
+def sweep_features(eta0, hist, pos, radii, masses, bond_i, bond_j, half_len, half_beam, dt):
+    """What each rigid-ship pose path sweeps through an ice window: (Q, 8)
+    float64, the definition ``dem_rollout_sweep_features`` implements (it has
+    no reference counterpart; the screening surrogate reads it).  Pose 0 is
+    eta0[q], pose t the row hist[t - 1, q].  Element e is hit at the first pose
+    whose frame puts its centroid inside the hull box grown by its radius
+    (|x| < half_len + r, |y| < half_beam + r); the geometry is float32 and
+    unfused (cos and sin of the heading rounded from float64), the sums
+    float64.  Columns: elements hit, their mass, sum 0.5 m |v|^2, sum m v_n,
+    sum m (H + 1 - t) / (H + 1), sum 0.5 m v_n^2 (v the path's step velocity
+    (pose t - pose t-1) / dt, the first step's at t = 0; v_n its component
+    towards the centroid, clamped at 0), bonds with one end hit, bonds with
+    both ends hit."""
+    eta0 = np.asarray(eta0, np.float64)
+    hist = np.asarray(hist, np.float64)
+    H, Q = hist.shape[0], hist.shape[1]
+    P = np.concatenate([eta0[None], hist], 0)  # (H + 1, Q, 3)
+    px, py = P[..., 0].astype(f32), P[..., 1].astype(f32)
+    cs, sn = np.cos(P[..., 2]).astype(f32), np.sin(P[..., 2]).astype(f32)
+    inv = f32(1.0 / dt)
+    vx = np.empty_like(px)
+    vy = np.empty_like(py)
+    vx[1:] = (px[1:] - px[:-1]) * inv
+    vy[1:] = (py[1:] - py[:-1]) * inv
+    vx[0], vy[0] = vx[1], vy[1]
+    ex, ey = np.asarray(pos, np.float64)[:, 0].astype(f32), np.asarray(pos, np.float64)[:, 1].astype(f32)
+    r = np.asarray(radii, np.float64).astype(f32)
+    m = np.asarray(masses, np.float64).astype(f32).astype(np.float64)
+    gl, gw = f32(half_len) + r, f32(half_beam) + r
+    out = np.zeros((Q, 8))
+    bi, bj = np.asarray(bond_i, np.int64), np.asarray(bond_j, np.int64)
+    for q in range(Q):
+        dx = ex[None, :] - px[:, q, None]  # (H + 1, n) float32
+        dy = ey[None, :] - py[:, q, None]
+        bx = cs[:, q, None] * dx + sn[:, q, None] * dy
+        by = cs[:, q, None] * dy - sn[:, q, None] * dx
+        inside = (np.abs(bx) < gl[None, :]) & (np.abs(by) < gw[None, :])
+        hit = inside.any(0)
+        t = np.argmax(inside, 0)[hit]
+        e = np.nonzero(hit)[0]
+        vxe, vye = vx[t, q].astype(np.float64), vy[t, q].astype(np.float64)
+        ddx, ddy = dx[t, e].astype(np.float64), dy[t, e].astype(np.float64)
+        dd = np.sqrt(ddx * ddx + ddy * ddy)
+        vn = np.maximum(0.0, (vxe * ddx + vye * ddy) / np.maximum(dd, 1e-6))
+        me = m[e]
+        hb = np.zeros(len(ex), bool)
+        hb[e] = True
+        out[q] = [len(e), me.sum(), (0.5 * me * (vxe * vxe + vye * vye)).sum(), (me * vn).sum(),
+                  (me * (H + 1 - t) / (H + 1)).sum(), (0.5 * me * vn * vn).sum(),
+                  np.count_nonzero(hb[bi] != hb[bj]), np.count_nonzero(hb[bi] & hb[bj])]
+    return out

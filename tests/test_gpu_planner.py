@@ -207,3 +207,46 @@ def test_screened_scorer_adapts_on_dem_scored_candidates_and_restores():
     assert sur.net.t == t0 + 2 and any(not torch.equal(a, q.p) for a, q in zip(before, sur.net.params()))
     scr.restore()
     assert sur.net.t == t0 and all(torch.equal(a, q.p) for a, q in zip(before, sur.net.params()))
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_sweep_features_match_oracle(medium, dtype):
+    """dem_rollout_sweep_features on the rigid-ship paths of random candidates
+    through a real window = the oracle's restatement: counts exact, sums
+    within float32 rounding of the float64 totals."""
+    from mbd_icenav_b200 import planner
+    from oracle.rollout_oracle import sweep_features
+    sc = _scene(medium, dtype=dtype)
+    rng = np.random.default_rng(3)
+    Q, H = 48, 16
+    Yn = torch.as_tensor(rng.uniform(-1, 1, (Q, H, 2)), dtype=torch.float32, device=DEV)
+    Yn[:, :, 0] = torch.abs(Yn[:, :, 0])  # forward: most paths reach ice
+    u = planner.physical_controls(Yn).to(dtype)
+    import ctypes as C
+    from mbd_icenav_b200 import _abi
+    lib = _abi.load_library()
+    eta0 = torch.as_tensor(np.tile(sc.eta0, (Q, 1)), dtype=dtype, device=DEV)
+    nu0 = torch.as_tensor(np.tile(sc.nu0, (Q, 1)), dtype=dtype, device=DEV)
+    hist = torch.empty((H, Q, 3), dtype=dtype, device=DEV)
+    rc = lib.dem_ship_rollout(C.byref(sc.params), _abi.DEM_F64 if dtype == torch.float64 else _abi.DEM_F32, Q, H,
+                              eta0.data_ptr(), nu0.data_ptr(), u.data_ptr(), None, hist.data_ptr(), None, None)
+    assert rc == _abi.DEM_OK
+    got = planner.sweep_features(sc, eta0, hist).cpu().numpy().astype(np.float64)
+    w = planner.sweep_inputs(sc)
+    ref = sweep_features(eta0.cpu().numpy(), hist.cpu().numpy(), w.pos.cpu().numpy(), w.radii.cpu().numpy(),
+                         w.masses.cpu().numpy(), w.bi.cpu().numpy(), w.bj.cpu().numpy(),
+                         0.5 * medium.ship_length, 0.5 * medium.ship_beam, medium.dt)
+    assert (ref[:, 0] > 0).sum() >= Q // 2, "most candidate paths must sweep ice"
+    for k in (0, 6, 7):
+        np.testing.assert_array_equal(got[:, k], ref[:, k])
+    np.testing.assert_allclose(got, ref, rtol=1e-6, atol=0)
+    # the same paths again: identical bits (fixed-order sums)
+    again = planner.sweep_features(sc, eta0, hist).cpu().numpy().astype(np.float64)
+    np.testing.assert_array_equal(again, got)
+    # the rigid-path features the screening reads carry them
+    _, wcost, sweep = planner.rigid_path(sc, Yn)
+    ext = planner.features(sc, Yn, wcost, sweep)
+    assert ext.shape == (Q, 6 + 3 * H + 8)
+    np.testing.assert_allclose(ext[:, -8:].cpu().numpy(),
+                               np.log1p(np.maximum(sweep.cpu().numpy(), 0) / np.array(planner.SWEEP_SCALE)),
+                               rtol=1e-5, atol=1e-6)

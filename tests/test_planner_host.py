@@ -58,3 +58,26 @@ def test_scene_starts_kinds():
     assert len(out) == 2 and all(len(rem) > 0 for _, rem in out)
     with pytest.raises(ValueError):
         planner.scene_starts(f, "pack", 1, np.random.default_rng(1))
+
+
+def test_sweep_features_oracle_known_answer():
+    """A ship surging along +x at 2 m/s meets one element 10 m ahead: hit at
+    the pose whose grown hull box first holds its centroid."""
+    from oracle.rollout_oracle import sweep_features
+    H, dt = 20, 0.5
+    eta0 = np.zeros((1, 3))
+    hist = np.zeros((H, 1, 3))
+    hist[:, 0, 0] = np.arange(1, H + 1) * 1.0  # 1 m per step
+    pos = np.array([[10.0, 0.0], [10.0, 30.0], [11.5, 0.5]])
+    radii = np.array([1.0, 1.0, 0.5])
+    masses = np.array([1000.0, 500.0, 200.0])
+    f = sweep_features(eta0, hist, pos, radii, masses, [0, 1, 0], [1, 2, 2], 5.0, 2.0, dt)[0]
+    # element 0: |10 - x| < 6 first at x = 5 (t = 5); element 2: |11.5 - x| < 5.5
+    # first at x = 7 (t = 7); element 1 is never within the beam
+    vn2 = 2.0 * 4.5 / np.hypot(4.5, 0.5)
+    assert f[0] == 2 and f[1] == 1200.0
+    assert f[2] == pytest.approx(0.5 * 1200.0 * 4.0)
+    assert f[3] == pytest.approx(1000.0 * 2.0 + 200.0 * vn2)
+    assert f[4] == pytest.approx(1000.0 * (H + 1 - 5) / (H + 1) + 200.0 * (H + 1 - 7) / (H + 1))
+    assert f[5] == pytest.approx(0.5 * 1000.0 * 4.0 + 0.5 * 200.0 * vn2 ** 2)
+    assert f[6] == 2 and f[7] == 1  # bonds (0,1), (1,2) cut; (0,2) both hit
