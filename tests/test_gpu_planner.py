@@ -102,7 +102,7 @@ def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
     from mbd_icenav_b200 import planner
     field = bench.load_field("medium", 0)
     data = planner.generate_dataset(field, n_starts=3, per_start=256, horizon=16, seed=2, device=DEV)
-    assert data.extra.shape == (768, 6 + 48) and torch.isfinite(data.raw).all()
+    assert data.extra.shape == (768, 6 + 48 + 8) and torch.isfinite(data.raw).all()
     sur, info = planner.train_surrogate(data, horizon=16, epochs=2, batch=128, device=DEV)
     assert np.isfinite(info["train_loss"][-1])
     sc = planner.make_scene(field, planner.sample_starts(field, 1, np.random.default_rng(9), 16)[0],
