@@ -110,6 +110,8 @@ struct DemHandle {
     std::vector<int> sys_start_h;  // (nsys + 1) element offsets
     void* sprow = nullptr;     // (6,) setpoint row of dem_frame_step
     unsigned* bar = nullptr;
+    unsigned* bar_groups = nullptr;
+    int bar_group_cap = 0;  // group words allocated
     // contact-set recording (dem_debug_record_contacts; caller-owned device arrays)
     int2* crec = nullptr;
     unsigned* crec_cnt = nullptr;
@@ -441,6 +443,7 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
         a.h_F = (T*)hist->F_ice_on_ship;
     }
     a.bar = h->bar;
+    a.bar_groups = h->bar_groups;
     a.status = h->status;
     a.stats = h->stats;
     a.crec = h->crec;
@@ -473,6 +476,8 @@ int launch(DemHandle* h, const DemIceState* in, DemIceState* out, const DemShipS
     const int k = h->P.n_ice_steps;
     const int per_frame = dem::phases_per_frame(k);
     if (h->mode == DEM_LAUNCH_PERSISTENT) {
+        if (dem::kBarGroup > 0 && (h->grid_blocks + dem::kBarGroup - 1) / dem::kBarGroup > h->bar_group_cap)
+            return set_err(h, DEM_ERR_INVALID, "persistent grid exceeds the barrier's group words");
         int lo = 0, hi = K * per_frame;
         void* args[] = {(void*)&a, (void*)&lo, (void*)&hi};
         CUDA_TRY(h, cudaLaunchCooperativeKernel((const void*)dem::dem_frames_kernel<T>, dim3(h->grid_blocks),
@@ -709,16 +714,27 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     {
         // the per-call counters in one block, cleared by one memset per call:
-        // esc_cnt, dirty_cnt, work_cnt, lazy_cnt (k + 2 each), bar (2), near_cnt (1)
+        // esc_cnt, dirty_cnt, work_cnt, lazy_cnt (k + 2 each), bar (2), near_cnt
+        // (1), then, from the next 128-byte line, the grid barrier's group words
+        // (one line each)
         const size_t k2 = (size_t)h->P.n_ice_steps + 2;
-        if ((rc = dev_alloc(h, &h->counters, sizeof(int) * (4 * k2 + 3)))) return fail(rc);
-        h->counters_bytes = sizeof(int) * (4 * k2 + 3);
+        const size_t stride = (size_t)dem::kBarGroupStride;
+        const size_t groups_at = ((4 * k2 + 3 + stride - 1) / stride) * stride;
+        // enough groups for the largest persistent grid: every SM full of CTAs
+        // of kThreads threads (the grid is sized by occupancy later)
+        const size_t max_grid = (size_t)h->sm_count * (2048 / dem::kThreads);
+        const size_t n_groups = dem::kBarGroup > 0 ? (max_grid + dem::kBarGroup - 1) / dem::kBarGroup : 0;
+        h->bar_group_cap = (int)n_groups;
+        const size_t words = groups_at + n_groups * stride;
+        if ((rc = dev_alloc(h, &h->counters, sizeof(int) * words))) return fail(rc);
+        h->counters_bytes = sizeof(int) * words;
         h->esc_cnt = reinterpret_cast<unsigned*>(h->counters);
         h->dirty_cnt = h->counters + k2;
         h->work_cnt = h->counters + 2 * k2;
         h->lazy_cnt = h->counters + 3 * k2;
         h->bar = reinterpret_cast<unsigned*>(h->counters + 4 * k2);
         h->near_cnt = h->counters + 4 * k2 + 2;
+        h->bar_groups = reinterpret_cast<unsigned*>(h->counters + groups_at);
     }
     if ((rc = dev_alloc(h, &h->soi, es * 2 * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fraw, es * n))) return fail(rc);
@@ -788,7 +804,7 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = reset_broad_phase(h, 0))) return fail(rc);
     CREATE_TRY(cudaMemset(h->status, 0, sizeof(int)));
     CREATE_TRY(cudaMemset(h->stats, 0, sizeof(long long) * 8));
-    CREATE_TRY(cudaMemset(h->bar, 0, sizeof(unsigned) * 2));
+    CREATE_TRY(cudaMemset(h->counters, 0, h->counters_bytes));
     if (nb) {
         int n_slots = 2 * nb;
         int blocks = (n_slots + 255) / 256;

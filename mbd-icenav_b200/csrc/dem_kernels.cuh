@@ -185,7 +185,8 @@ struct KArgs {
     T *d_pen, *d_fmag, *d_F, *d_J;
     T *h_pos, *h_rot, *h_eta, *h_sub, *h_J, *h_F;
     uint8_t* h_intact;
-    unsigned* bar;        // [count, generation]
+    unsigned* bar;        // top arrival word of the grid barrier
+    unsigned* bar_groups; // group arrival words, kBarGroupStride apart (kBarGroup > 0)
     // contact-set recording (parity aid, off when crec is null): every pair
     // whose contact term a force phase computes goes to crec as {e, o}, seen
     // from the active element e; crec_marks[f * k_sub + s] = pairs recorded
@@ -249,19 +250,53 @@ __device__ __forceinline__ unsigned frame_stamp(const KArgs<T>& a, const Frame<T
 // ─── grid barrier (bounded) ──────────────────────────────────────────────────
 // Returns false (and records DEM_ERR_TIMEOUT) if the wait exceeds its limit;
 // callers then return.
+//
+// Arrival counts use flip words: of the n arrivals at a word, the first CTA of
+// the set adds 2^31 - (n - 1) and every other one adds 1, so the arrivals of
+// one barrier sum to 2^31, bit 31 of the word flips exactly at the last
+// arrival (the one whose add carries into bit 31), and no word needs a reset
+// between barriers.  With DEM_BAR_GROUP = g > 0 the CTAs arrive in groups of g
+// consecutive CTAs, each group on a word of its own 128-byte line
+// (a.bar_groups); the last arrival of a group carries it to the top word
+// a.bar, and every CTA polls a.bar.  The hottest word then takes
+// ceil(grid / g) atomics per barrier instead of one per CTA.
+#ifndef DEM_BAR_GROUP
+#define DEM_BAR_GROUP 0
+#endif
+constexpr int kBarGroup = DEM_BAR_GROUP;
+constexpr int kBarGroupStride = 32;  // words between group counters (128 bytes)
+
 template <typename T>
 __device__ bool grid_barrier(const KArgs<T>& a) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        // CTA 0 adds 2^31 - (gridDim.x - 1), every other CTA adds 1: the arrivals
-        // of one barrier sum to 2^31, so bit 31 of the word flips exactly when the
-        // last CTA arrives, and the word needs no reset between barriers
-        const unsigned inc = (blockIdx.x == 0) ? 0x80000000u - (gridDim.x - 1u) : 1u;
-        // the arrival is a release at GPU scope (cumulative over the CTA's writes
-        // ordered before it by __syncthreads), the polls are acquires: the
-        // pattern orders every CTA's phase writes before every CTA's next phase
-        const unsigned old = atom_add_release_u32(a.bar, inc);
+        // the arrivals are releases at GPU scope, cumulative over the CTA's
+        // writes ordered before them by __syncthreads; a group arrival is an
+        // acquire too, so that the group's last arrival, which reads every
+        // earlier arrival of its group, carries their writes into its release
+        // on the top word; the polls are acquires: the pattern orders every
+        // CTA's phase writes before every CTA's next phase
+        unsigned old;
+        if (kBarGroup > 0) {
+            const unsigned g = blockIdx.x / (unsigned)kBarGroup;
+            const unsigned first = g * (unsigned)kBarGroup;
+            const unsigned size = min((unsigned)kBarGroup, gridDim.x - first);
+            const unsigned ginc = (blockIdx.x == first) ? 0x80000000u - (size - 1u) : 1u;
+            const unsigned gold = atom_add_acqrel_u32(a.bar_groups + (size_t)g * kBarGroupStride, ginc);
+            const unsigned n_groups = (gridDim.x + (unsigned)kBarGroup - 1u) / (unsigned)kBarGroup;
+            if (((gold + ginc) ^ gold) & 0x80000000u) {
+                // this group's last arrival: carry the group to the top word
+                const unsigned tinc = (g == 0u) ? 0x80000000u - (n_groups - 1u) : 1u;
+                atom_add_release_u32(a.bar, tinc);
+            }
+            // every word flips once per barrier, so the group word's bit 31
+            // before this arrival is the top word's before the barrier
+            old = gold;
+        } else {
+            const unsigned inc = (blockIdx.x == 0) ? 0x80000000u - (gridDim.x - 1u) : 1u;
+            old = atom_add_release_u32(a.bar, inc);
+        }
         int ok = 1;
         unsigned long long t0 = 0;
         for (unsigned it = 0; ((ld_acquire_u32(a.bar) ^ old) & 0x80000000u) == 0u; ++it) {

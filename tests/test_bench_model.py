@@ -15,13 +15,13 @@ def test_all_active_count_of_the_large_field():
     assert bench.algorithmic_bytes_per_frame(N, NB, V, K) == 439_430_367
 
 
-def test_frozen_elements_carry_their_state_over_at_49_bytes():
+def test_frozen_elements_carry_their_state_over_at_49_bytes_once_per_frame():
     full = bench.algorithmic_bytes_per_frame(N, NB, V, K)
     frozen = bench.algorithmic_bytes_per_frame(N, NB, V, K, n_act=0, nb_act=0)
-    assert full - frozen == K * ((89 - 49) * N + 17 * NB)
+    assert full - frozen == K * (89 * N + 17 * NB) - 49 * N
     # in place (frames after the first of a call) they carry nothing over
     inplace = bench.algorithmic_bytes_per_frame(N, NB, V, K, n_act=0, nb_act=0, in_place=True)
-    assert frozen - inplace == K * 49 * N
+    assert frozen - inplace == 49 * N
     assert inplace == N * (9 * V + 64) + 50 * NB
 
 
@@ -31,3 +31,12 @@ def test_active_counts_on_cpu_tensors():
     bi = torch.tensor([0, 1, 2], dtype=torch.int32)
     bj = torch.tensor([1, 2, 4], dtype=torch.int32)
     assert bench.active_counts(act, bi, bj) == (2, 1)
+
+
+def test_reference_arm_slabs_cover_the_field_once():
+    import numpy as np
+    sizes = bench.field_slabs(N, 16)
+    assert sum(sizes) == N and max(sizes) - min(sizes) <= 1
+    order = np.argsort(np.random.default_rng(0).random(N), kind="stable")
+    parts = np.array_split(order, 16)
+    assert sorted(np.concatenate(parts).tolist()) == list(range(N))
