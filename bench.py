@@ -735,12 +735,17 @@ def run_surrogate(args, rank: int, world: int):
             # the same screening with the network learning the scene as the plan goes
             scra = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err,
                                           n_check=args.sur_check, seed=si, adapt_steps=args.sur_compare_adapt)
+            # the same screening with a band below the top-k checked, and scored in full on a miss
+            scrd = planner.ScreenedScorer(sc, sur, cfg.n_sample, w, top_k=cfg.top_k, max_rel_err=cfg.max_rel_err,
+                                          n_check=args.sur_check, seed=si, adapt_steps=args.sur_adapt,
+                                          deepen=args.sur_deepen)
             # untimed: each DEM batch's work split, tuned on candidates like a plan's
             Yt = torch.clamp(torch.randn((cfg.n_sample, H, 2), device=device) * 0.3 + 0.7, -1, 1)
             split_plain, _ = plain.autotune(Yt)
             split_k, _ = scr.dem_k.autotune(Yt[:scr.dem_k.Q].contiguous())
             scr64.dem_k.autotune(Yt[:scr64.dem_k.Q].contiguous())
             scra.dem_k.autotune(Yt[:scra.dem_k.Q].contiguous())
+            scrd.dem_k.autotune(Yt[:scrd.dem_k.Q].contiguous())
             (Yp, _), tp = timed(lambda: planner.mbd_plan(plain, cfg, device, seed=si))
             n_fb0 = scr.fallbacks
             (Ys, _), ts = timed(lambda: planner.mbd_plan(scr, cfg, device, seed=si))
@@ -749,6 +754,8 @@ def run_surrogate(args, rank: int, world: int):
             scr64.restore()
             (Ysa, _), tsa = timed(lambda: planner.mbd_plan(scra, cfg, device, seed=si))
             scra.restore()
+            (Ysd, _), tsd = timed(lambda: planner.mbd_plan(scrd, cfg, device, seed=si))
+            scrd.restore()
             # the plain planner again with other samples: its own spread of plan costs
             Yp2, _ = planner.mbd_plan(plain, cfg, device, seed=si + 1000)
             cp = planner.plan_cost(sc, Yp, scr.dem_k)
@@ -756,6 +763,7 @@ def run_surrogate(args, rank: int, world: int):
             cp2 = planner.plan_cost(sc, Yp2, scr.dem_k)
             cs64 = planner.plan_cost(sc, Ys64, scr.dem_k)
             csa = planner.plan_cost(sc, Ysa, scr.dem_k)
+            csd = planner.plan_cost(sc, Ysd, scr.dem_k)
             if si >= args.warmup:
                 rows.append({"plain_s": tp, "screened_s": ts, "plain_cost": cp, "screened_cost": cs,
                              "plain_cost_other_seed": cp2,
@@ -771,14 +779,17 @@ def run_surrogate(args, rank: int, world: int):
                              "adaptive": {"screened_s": tsa, "screened_cost": csa,
                                           "rel_cost_err": abs(csa - cp) / max(abs(cp), 1e-9),
                                           "fallbacks": scra.fallbacks,
-                                          "check_miss_max": float(np.max(scra.rel_errs))}})
+                                          "check_miss_max": float(np.max(scra.rel_errs))},
+                             "deepen": {"screened_s": tsd, "screened_cost": csd,
+                                        "rel_cost_err": abs(csd - cp) / max(abs(cp), 1e-9),
+                                        "fallbacks": scrd.fallbacks, "deepened": scrd.deepened,
+                                        "band_miss_max": float(np.max(scrd.band_errs)),
+                                        "check_miss_max": float(np.max(scrd.rel_errs))}})
                 sys.stderr.write(f"plan {si}: {json.dumps(rows[-1])}\n")
             plain.batch.frame_step.close()
-            for z in (scr, scr64, scra):
-                z.dem_k.batch.frame_step.close()
-                if z.dem_all is not None:
-                    z.dem_all.batch.frame_step.close()
-            del plain, scr, scr64, scra
+            for z in (scr, scr64, scra, scrd):
+                z.close()
+            del plain, scr, scr64, scra, scrd
     # tensor-pipe figure: the screening's own network work on one plan's
     # population, the head over n_sample rows after one encoder pass, timed alone
     sc = planner.make_scene(field, starts[-1][0], (2.0, 0.0, 0.0), H, device=device, patch_stats=data.patch_stats,
@@ -830,6 +841,13 @@ def run_surrogate(args, rank: int, world: int):
                                 "fallback_steps": [r["adaptive"]["fallbacks"] for r in rows],
                                 "note": f"the same plans with {args.sur_compare_adapt} Adam steps per MBD step on "
                                         f"the check set (every candidate after a fallback)"},
+                   "deepen": {"speedup_vs_plain_dem": tp / (sum(r["deepen"]["screened_s"] for r in rows) / K),
+                              "plan_rel_cost_err": [r["deepen"]["rel_cost_err"] for r in rows],
+                              "fallback_steps": [r["deepen"]["fallbacks"] for r in rows],
+                              "deepened_steps": [r["deepen"]["deepened"] for r in rows],
+                              "note": f"the same plans with half the check drawn from the {args.sur_deepen} "
+                                      f"candidates ranked below the top {cfg.top_k}, all of which the DEM scores "
+                                      f"when that half beats the screened best"},
                    "scenes": args.sur_scenes, "windows": [r["window"] for r in rows],
                    "plain_dem_rollouts_per_s": plain_rate, "speedup_vs_plain_dem": value / plain_rate,
                    "plan_rel_cost_err": errs, "plan_rel_cost_err_max": max(errs),
@@ -1094,6 +1112,8 @@ def main():
                     help="Adam steps per MBD step on the check set the DEM scored (0: the network stays fixed)")
     ap.add_argument("--sur-compare-adapt", type=int, default=4,
                     help="Adam steps per MBD step of the adaptive comparison plans")
+    ap.add_argument("--sur-deepen", type=int, default=1536,
+                    help="band below the top-k for the deepening comparison plans (ScreenedScorer deepen)")
     ap.add_argument("--sur-scenes", choices=("channel", "open"), default="channel",
                     help="plan starts: mid-transit in the pack with the ship's channel cleared, or open water")
     ap.add_argument("--all-active", action="store_true",

@@ -437,6 +437,14 @@ class ScreenedScorer:
     there.  Above ``max_rel_err`` the step falls back to scoring every
     candidate with the plain DEM.
 
+    With ``deepen`` > 0 the check is split: half of it is drawn from the band
+    of the ``deepen`` candidates ranked just below the top_k, half from the
+    rest.  When the band sample beats the screened best by more than
+    ``max_rel_err`` (but the rest does not), the DEM scores the whole band too
+    and those candidates keep their exact costs (``deepened`` counts such
+    steps): a ranking that misses near its cut costs a band instead of the
+    whole population.  A miss in the rest still falls back.
+
     With ``adapt_steps`` > 0 the network also learns the scene as the plan
     goes: after each step, that many Adam steps (batches of up to 256,
     learning rate ``adapt_lr``) on the step's unbiased DEM samples, whose exact
@@ -447,7 +455,7 @@ class ScreenedScorer:
 
     def __init__(self, scene: PlanScene, surrogate: Surrogate, Q: int, weights: CostWeights, top_k: int = 64,
                  max_rel_err: float = 0.05, n_check: int = 64, seed: int = 0, adapt_steps: int = 0,
-                 adapt_lr: float = 3e-4, **frame_kw):
+                 adapt_lr: float = 3e-4, deepen: int = 0, **frame_kw):
         torch = _tm()
         self.scene = scene
         self.sur = surrogate
@@ -455,6 +463,11 @@ class ScreenedScorer:
         self.Q = Q
         self.k = top_k
         self.n_check = max(0, min(n_check, Q - top_k))
+        self.deepen = max(0, min(int(deepen), Q - top_k - (self.n_check + 1) // 2))
+        self.n_band = min(self.n_check // 2, self.deepen)  # band part of the check
+        self.dem_band = None
+        self.deepened = 0
+        self.band_errs: List[float] = []   # per step: how much the best band sample beats the screened best
         self.max_rel_err = max_rel_err
         self.dem_k = DemScorer(scene, top_k + self.n_check, weights, **frame_kw)
         self.dem_all = None
@@ -481,26 +494,46 @@ class ScreenedScorer:
         return planner @ wp + ice @ wi
 
     def selection(self, pred):
-        """(screened top_k indices ascending by prediction, random check indices)."""
+        """(screened top_k indices ascending by prediction, check indices, the
+        band of ``deepen`` candidates below the top_k or None).  With a band,
+        the first ``n_band`` check indices are drawn from it, the others from
+        the rest; without one, all from the rest."""
         torch = _tm()
         order = torch.argsort(pred)
-        top, rest = order[:self.k], order[self.k:]
-        pick = torch.randperm(rest.numel(), generator=self.gen, device=pred.device)[:self.n_check]
-        return top, rest[pick]
+        top = order[:self.k]
+        if self.deepen == 0:
+            rest = order[self.k:]
+            pick = torch.randperm(rest.numel(), generator=self.gen, device=pred.device)[:self.n_check]
+            return top, rest[pick], None
+        band, rest = order[self.k:self.k + self.deepen], order[self.k + self.deepen:]
+        bp = torch.randperm(band.numel(), generator=self.gen, device=pred.device)[:self.n_band]
+        rp = torch.randperm(rest.numel(), generator=self.gen, device=pred.device)[:self.n_check - self.n_band]
+        return top, torch.cat([band[bp], rest[rp]]), band
+
+    @staticmethod
+    def _beats(best, others) -> float:
+        """How much the best of ``others`` beats ``best``, relative to it (0 when it does not)."""
+        if others.numel() == 0:
+            return 0.0
+        m = others.min()
+        return float(((best - m) / m.abs().clamp(min=1e-9)).clamp(min=0.0).item())
 
     def __call__(self, Yn):
         torch = _tm()
         pred = self.predicted(Yn)
-        top, chk = self.selection(pred)
+        top, chk, band = self.selection(pred)
         idx = torch.cat([top, chk])
         terms = self.dem_k.terms(Yn[idx].contiguous())
         exact = self.dem_k.total(terms)
         e_top, e_chk = exact[:self.k], exact[self.k:]
         best = e_top.min()
-        miss = 0.0
-        if self.n_check:
-            miss = float(((best - e_chk.min()) / e_chk.min().abs().clamp(min=1e-9)).clamp(min=0.0).item())
+        nb = self.n_band if band is not None else 0
+        band_miss = self._beats(best, e_chk[:nb])
+        if nb:
+            best = torch.minimum(best, e_chk[:nb].min())
+        miss = self._beats(best, e_chk[nb:])
         self.rel_errs.append(miss)
+        self.band_errs.append(band_miss)
         self.pred_errs.append(float(((pred[top] - e_top).abs() / e_top.abs().clamp(min=1e-9)).mean().item()))
         self.rollouts += idx.numel()
         if miss > self.max_rel_err:
@@ -512,11 +545,24 @@ class ScreenedScorer:
             all_terms = self.dem_all.terms(Yn)
             self._adapt(self._ext, all_terms[:, 4:7])
             return self.dem_all.total(all_terms)
-        if self.n_check:
+        if self.n_check and self.adapt_steps > 0:
             self._adapt(self._ext[chk], terms[self.k:, 4:7])
         cost = torch.full_like(pred, float("inf"))
         cost[idx] = exact
+        if band is not None and band_miss > self.max_rel_err:
+            # the ranking misses near its cut: the DEM scores the whole band
+            if self.dem_band is None:
+                self.dem_band = DemScorer(self.scene, self.deepen, self.w, **self.frame_kw)
+            self.deepened += 1
+            self.rollouts += self.deepen
+            cost[band] = self.dem_band(Yn[band].contiguous())
         return cost
+
+    def close(self):
+        """Release the DEM handles of the scorer's batches."""
+        for d in (self.dem_k, self.dem_all, self.dem_band):
+            if d is not None:
+                d.batch.frame_step.close()
 
     def _adapt(self, ext, raw):
         """``adapt_steps`` Adam steps on rows ``ext`` with exact ice terms ``raw``."""

@@ -132,6 +132,25 @@ def test_screened_step_uses_dem_costs_for_top_k_and_falls_back():
     Ys, m2 = planner.mbd_plan(scr, cfg, DEV, seed=0)
     assert Yp.shape == (16, 2) and Ys.shape == (16, 2) and len(m1) == len(m2) == 2
     assert np.isfinite(planner.plan_cost(sc, Ys, scr.dem_k))
+    # deepening: predictions that put the DEM's best candidates in the band
+    # below the top_k and its worst in the top_k; the band's check sample then
+    # beats the screened best while the rest cannot beat the band, so the DEM
+    # scores the whole band and nothing falls back
+    D = 64
+    dp = planner.ScreenedScorer(sc, sur, Q, w, top_k=k, n_check=r, max_rel_err=0.0, seed=5, deepen=D)
+    order = torch.argsort(exact)  # ascending true cost
+    fake = torch.empty_like(exact)
+    fake[order[Q - k:]] = torch.arange(k, dtype=fake.dtype, device=DEV)             # worst -> top_k
+    fake[order[:D]] = k + torch.arange(D, dtype=fake.dtype, device=DEV)            # best -> band
+    fake[order[D:Q - k]] = k + D + torch.arange(Q - k - D, dtype=fake.dtype, device=DEV)
+    dp.predicted = lambda Y: fake
+    dc = dp(Yn)
+    assert dp.deepened == 1 and dp.fallbacks == 0 and dp.band_errs[-1] > 0 and dp.rel_errs[-1] == 0.0
+    kept = torch.isfinite(dc)
+    assert kept[order[:D]].all() and kept[order[Q - k:]].all()
+    assert int(kept.sum()) == k + D + (r - r // 2)  # top_k, the band, the rest's check sample
+    assert torch.equal(dc[kept], exact[kept])
+    dp.close()
 
 
 def test_autotune_picks_the_fastest_split_and_caches_it(medium):
