@@ -81,3 +81,32 @@ def test_sweep_features_oracle_known_answer():
     assert f[4] == pytest.approx(1000.0 * (H + 1 - 5) / (H + 1) + 200.0 * (H + 1 - 7) / (H + 1))
     assert f[5] == pytest.approx(0.5 * 1000.0 * 4.0 + 0.5 * 200.0 * vn2 ** 2)
     assert f[6] == 2 and f[7] == 1  # bonds (0,1), (1,2) cut; (0,2) both hit
+
+
+def test_screened_selection_splits_the_check_between_band_and_rest():
+    """ScreenedScorer.selection on CPU tensors: the top_k lowest predictions,
+    then the check drawn from the band below them (deepen) and from the rest,
+    disjoint; without a band, the check comes from everything below the top_k."""
+    import torch
+    from mbd_icenav_b200.planner import ScreenedScorer
+    Q, k, r, D = 200, 10, 8, 40
+    pred = torch.randperm(Q, generator=torch.Generator().manual_seed(0)).double()
+    order = torch.argsort(pred)
+
+    def scorer(deepen):
+        return SimpleNamespace(k=k, n_check=r, deepen=deepen, n_band=min(r // 2, deepen),
+                               gen=torch.Generator().manual_seed(1))
+
+    top, chk, band = ScreenedScorer.selection(scorer(D), pred)
+    assert torch.equal(top, order[:k]) and torch.equal(band, order[k:k + D])
+    assert chk.numel() == r and len(set(chk.tolist()) | set(top.tolist())) == k + r
+    assert set(chk[:r // 2].tolist()) <= set(band.tolist())
+    assert set(chk[r // 2:].tolist()) <= set(order[k + D:].tolist())
+    top0, chk0, band0 = ScreenedScorer.selection(scorer(0), pred)
+    assert band0 is None and torch.equal(top0, top)
+    assert set(chk0.tolist()) <= set(order[k:].tolist()) and chk0.numel() == r
+    # the check's measure: how much the best of the others beats the best, relative to it
+    beats = ScreenedScorer._beats
+    assert beats(torch.tensor(10.0), torch.tensor([12.0, 8.0])) == pytest.approx(0.25)
+    assert beats(torch.tensor(10.0), torch.tensor([12.0])) == 0.0
+    assert beats(torch.tensor(10.0), torch.tensor([])) == 0.0
