@@ -703,6 +703,7 @@ def run_surrogate(args, rank: int, world: int):
     data = planner.generate_dataset(field, n_starts=args.sur_starts, per_start=args.sur_per_start, horizon=H,
                                     seed=args.seed + 100 * rank, device=device, scenes=args.sur_scenes)
     gen_s = time.time() - t0
+    rank_corr = planner.within_scene_rank_corr(data)
     sur, info = planner.train_surrogate(data, horizon=H, epochs=args.sur_epochs, batch=256, device=device,
                                         seed=args.seed)
     cfg = planner.MBDConfig(horizon=H, n_sample=args.sur_samples, n_diffuse=args.sur_iters + 1,
@@ -856,7 +857,8 @@ def run_surrogate(args, rank: int, world: int):
                    "train": {"samples": info["train_samples"], "holdout_samples": info["holdout_samples"],
                              "epochs": args.sur_epochs, "steps": info["steps"], "seconds": info["seconds"],
                              "holdout_mse_std_units": info["holdout_loss"], "train_loss": info["train_loss"],
-                             "data_seconds": gen_s, "starts": args.sur_starts, "per_start": args.sur_per_start},
+                             "data_seconds": gen_s, "starts": args.sur_starts, "per_start": args.sur_per_start,
+                             "within_scene_rank_corr": rank_corr},
                    "network": {"params": sur.net.n_params(), "flops_per_sample_fwd": fl},
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak_tf, "unit": "TFLOP/s",

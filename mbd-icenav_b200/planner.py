@@ -871,6 +871,37 @@ def train_surrogate(data: Dataset, horizon: int = 64, epochs: int = 8, batch: in
                  "train_samples": int(len(train_idx)), "holdout_samples": int(len(hold_idx))}
 
 
+def within_scene_rank_corr(data: Dataset) -> dict:
+    """Mean over the dataset's starts of the Spearman rank correlation, among
+    one start's candidates, between each network input summary and each ice
+    term: the sweep features (``SWEEP_SCALE`` order) and the sum of the path's
+    log costmap values, against [KE, impulse, bonds].  How well an input can
+    rank the candidates of one scene, which is what screening needs."""
+    from scipy.stats import rankdata
+    extra = data.extra.detach().cpu().numpy().astype(np.float64)
+    raw = data.raw.detach().cpu().numpy().astype(np.float64)
+    so = data.start_of.detach().cpu().numpy()
+    H = (extra.shape[1] - S.N_SHIP - S.N_SWEEP) // S.N_STEP
+    names = ["elements_hit", "mass_hit", "ke_proxy", "momentum_proxy", "mass_early", "ke_normal_proxy",
+             "bonds_cut", "bonds_inside", "path_costmap"]
+    path = extra[:, S.N_SHIP + 2 * H:S.N_SHIP + 3 * H].sum(1, keepdims=True)
+    feats = np.concatenate([extra[:, S.N_SHIP + 3 * H:], path], 1)
+    acc = np.zeros((len(names), 3))
+    cnt = np.zeros((len(names), 3))
+    for st in np.unique(so):
+        m = so == st
+        for j in range(len(names)):
+            fr = rankdata(feats[m, j])
+            for k in range(3):
+                tr = rankdata(raw[m, k])
+                if np.std(fr) > 0 and np.std(tr) > 0:
+                    acc[j, k] += np.corrcoef(fr, tr)[0, 1]
+                    cnt[j, k] += 1
+    mean = np.where(cnt > 0, acc / np.maximum(cnt, 1), np.nan)
+    return {nm: {"ke": float(mean[j, 0]), "impulse": float(mean[j, 1]), "bonds": float(mean[j, 2])}
+            for j, nm in enumerate(names)}
+
+
 def holdout_error(sur: Surrogate, data: Dataset, idx, tgt) -> float:
     """Mean squared error of the standardised targets on held-out samples."""
     torch = _tm()

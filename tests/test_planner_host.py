@@ -110,3 +110,31 @@ def test_screened_selection_splits_the_check_between_band_and_rest():
     assert beats(torch.tensor(10.0), torch.tensor([12.0, 8.0])) == pytest.approx(0.25)
     assert beats(torch.tensor(10.0), torch.tensor([12.0])) == 0.0
     assert beats(torch.tensor(10.0), torch.tensor([])) == 0.0
+
+
+def test_within_scene_rank_corr_on_a_synthetic_dataset():
+    """The diagnostic ranks each start's candidates on its own: a feature that
+    orders the ice terms within every start scores 1 even when the starts'
+    levels differ, and a reversed one -1."""
+    import torch
+    from mbd_icenav_b200 import planner
+    from mbd_icenav_b200 import surrogate as S
+    H, per, starts = 4, 16, 3
+    n = per * starts
+    rng = np.random.default_rng(0)
+    extra = np.zeros((n, S.N_SHIP + S.N_STEP * H + S.N_SWEEP), np.float32)
+    raw = np.zeros((n, 3))
+    for s in range(starts):
+        v = rng.permutation(per).astype(np.float64) + 100.0 * (starts - s)
+        rows = slice(s * per, (s + 1) * per)
+        raw[rows, 0] = v
+        raw[rows, 1] = v
+        raw[rows, 2] = v
+        extra[rows, S.N_SHIP + 3 * H] = v - 100.0 * (starts - s) + 7.0 * s  # same order, other level
+        extra[rows, S.N_SHIP + 3 * H + 1] = -v                               # reversed
+        extra[rows, S.N_SHIP + 2 * H:S.N_SHIP + 3 * H] = rng.random((per, H))
+    data = planner.Dataset(None, torch.as_tensor(np.repeat(np.arange(starts), per)), torch.as_tensor(extra),
+                           torch.as_tensor(raw), None, (0.0, 1.0))
+    rc = planner.within_scene_rank_corr(data)
+    assert rc["elements_hit"]["ke"] == pytest.approx(1.0) and rc["mass_hit"]["bonds"] == pytest.approx(-1.0)
+    assert abs(rc["path_costmap"]["impulse"]) < 0.6 and set(rc) >= {"bonds_cut", "path_costmap"}
