@@ -705,12 +705,12 @@ int dem_create(const DemParams* params, const DemStatic* s, int dtype, int devic
     if ((rc = dev_alloc(h, &h->comp_cnt, sizeof(int)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->esc_list, sizeof(int) * n))) return fail(rc);
     if ((rc = dev_alloc(h, &h->dirty_list, sizeof(int) * n))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * (size_t)dem::kActBins * std::max(n, 1)))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->act_list, sizeof(int) * (size_t)dem::kActLists * std::max(n, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->lazy_list, sizeof(int) * std::max(n, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->bstamp, sizeof(unsigned) * std::max(nb, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fb_list, sizeof(int) * std::max(nb, 1)))) return fail(rc);
     if ((rc = dev_alloc(h, &h->fb_cnt, sizeof(int)))) return fail(rc);
-    if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int) * dem::kActBins))) return fail(rc);
+    if ((rc = dev_alloc(h, &h->act_cnt, sizeof(int) * dem::kActLists))) return fail(rc);
     if ((rc = dev_alloc(h, &h->slot_owner, sizeof(int) * slots.size()))) return fail(rc);
     {
         // the per-call counters in one block, cleared by one memset per call:

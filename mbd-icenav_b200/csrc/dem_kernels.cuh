@@ -160,11 +160,11 @@ struct KArgs {
     int* dirty_list;    // (n) elements whose list is rebuilt
     int* dirty_cnt;     // (k_sub + 2) lists to rebuild, per substep
     int* work_cnt;      // (k_sub + 2) element chunks handed out dynamically, per substep
-    int* act_list;      // (kActBins * n) elements active this frame, by work bin (built by phase_reduce)
+    int* act_list;      // (kActLists * n) elements active this frame, then by work bin (built by phase_reduce)
     unsigned* bstamp;   // (nb) frame stamp of the bonds with an active end (set by phase_reduce)
     int* fb_list;       // (nb) the frame's bonds with an active end, each once (phase_reduce)
     int* fb_cnt;        // (1) entries of fb_list
-    int* act_cnt;       // (kActBins) entries of each bin of act_list
+    int* act_cnt;       // (kActLists) entries of the list and of each bin
     unsigned round_base;  // first dirty stamp of this call minus one (advanced by the host)
     int fail_phase;       // test hook: the last CTA skips the barrier after this phase (-1: off)
     ForceConst<T> fc;     // force-phase constants
@@ -1014,37 +1014,23 @@ __device__ __forceinline__ int chunk_of(const KArgs<T>& a, int e) {
 }
 
 // ─── active list, binned by work ────────────────────────────────────────────
-// phase_reduce lists the frame's active elements in kActBins lists of n
-// entries each (act_list + b * n, counted by act_cnt[b]) by their work in a
-// substep: the larger of their bond slot and candidate counts, in bins
-// [0, 6), [6, 9), [9, 12) and from 12 with four bins.  The force phases take
-// the bins one after another as one list (act_elem), so the lanes of a warp
-// hold elements of like work.  The order of the elements does not change any
-// result: each element sums its own terms.  One bin is the default: with
-// four, a frame with every element active on the 250k-element field ran
-// 6 % faster, but the bench's frame, with a few hundred active elements, 8 %
-// slower (the bin counts are read and shared at the start of every force
-// phase, on its critical path).
+// phase_reduce lists the frame's active elements in act_list (n entries,
+// counted by act_cnt[0]).  With kActBins > 1 it also lists them in kActBins
+// bins of n entries each (act_list + (1 + b) * n, counted by act_cnt[1 + b])
+// by their work in a substep: the larger of their bond slot and candidate
+// counts, in bins [0, 6), [6, 9), [9, 12) and from 12 with four bins.  The
+// thread-per-element path of the force phases takes the bins one after
+// another as one list, so the lanes of a warp hold elements of like work; the
+// warp-per-element path, which a frame with few active elements takes, reads
+// the plain list.  The order of the elements does not change any result: each
+// element sums its own terms.
 #ifndef DEM_ACT_BINS
 #define DEM_ACT_BINS 1
 #endif
 constexpr int kActBins = DEM_ACT_BINS;
+constexpr int kActLists = kActBins > 1 ? 1 + kActBins : 1;
 
 __device__ __forceinline__ int act_bin(int work) { return min(max((work - 3) / 3, 0), kActBins - 1); }
-
-// entry i of the binned active list (i < the sum of the bins' counts)
-template <typename T>
-__device__ __forceinline__ int act_elem(const KArgs<T>& a, const int* bins, int i) {
-    int b = 0;
-#pragma unroll
-    for (int k = 0; k < kActBins - 1; ++k) {
-        if (b == k && i >= bins[k]) {
-            i -= bins[k];
-            b = k + 1;
-        }
-    }
-    return a.act_list[(size_t)b * a.n + i];
-}
 
 // ─── P_CULL: elements whose bounding circle reaches the hull; escapes ───────
 template <typename T>
@@ -1055,7 +1041,7 @@ __device__ void phase_cull(const KArgs<T>& a, const Frame<T>& F) {
     // nothing reads the grid in this phase: drop stale entries queued last frame
     compact_buckets(a);
     if (gtid == 0) {
-        for (int b = 0; b < kActBins; ++b) a.act_cnt[b] = 0;  // read last by the previous frame's force phases
+        for (int b = 0; b < kActLists; ++b) a.act_cnt[b] = 0;  // read last by the previous frame's force phases
         *a.fb_cnt = 0;   // read last by the previous frame's fracture
     }
     // per-floe scratch of this frame (read last by the previous frame's fracture)
@@ -1626,11 +1612,14 @@ __device__ void phase_reduce(const KArgs<T>& a, const Frame<T>& F) {
             // the frame's active list, binned by the element's work in a
             // substep (bond slots and candidates, of which the thread path
             // walks the longer), so that the lanes of a warp end together
-            int bin = 0;
-            if (kActBins > 1 && ae) bin = act_bin(max(a.boff[e + 1] - a.boff[e], a.ncnt[e]));
+            warp_append(a.act_list, a.act_cnt, ae, e);
+            if (kActBins > 1) {
+                int bin = 0;
+                if (ae) bin = act_bin(max(a.boff[e + 1] - a.boff[e], a.ncnt[e]));
 #pragma unroll
-            for (int b = 0; b < kActBins; ++b)
-                warp_append(a.act_list + (size_t)b * a.n, &a.act_cnt[b], ae && bin == b, e);
+                for (int b = 0; b < kActBins; ++b)
+                    warp_append(a.act_list + (size_t)(1 + b) * a.n, &a.act_cnt[1 + b], ae && bin == b, e);
+            }
         }
         // the bond slot records of the active elements for this frame (only
         // active elements read them); crack front = the element touches a bond
@@ -2155,12 +2144,6 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     const ForceCtx<T> cx = force_ctx(a, F, s);
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsz = gridDim.x * blockDim.x;
-    // entries of each bin of the active list (constant during the phase)
-    __shared__ int s_abin[kActBins];
-    if (kActBins > 1) {
-        if ((int)threadIdx.x < kActBins) s_abin[threadIdx.x] = *((volatile int*)&a.act_cnt[threadIdx.x]);
-        __syncthreads();
-    }
     int* esc_ctr = (int*)&a.esc_cnt[s + 1];
     int* lazy_ctr = &a.lazy_cnt[s + 1];
     const int warp = gtid >> 5, nwarps = gsz >> 5, lane = threadIdx.x & 31;
@@ -2222,7 +2205,7 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     if (a.force_split == DEM_SPLIT_WARP || (a.force_split == DEM_SPLIT_AUTO && na <= 2 * nw2)) {
         // at most two active elements per warp: a warp per element
         for (int i = warp - skip; i < na; i += nw2) {
-            const int e = act_elem(a, s_abin, i);
+            const int e = a.act_list[i];
             if (has_dirty && a.dirty[e] == round) continue;
             const int code = force_element_warp(a, F, cx, e);
             if (lane == 0 && code == 2) a.esc_list[atomicAdd(esc_ctr, 1)] = e;
@@ -2243,11 +2226,29 @@ __device__ void phase_force(const KArgs<T>& a, const Frame<T>& F, int s, unsigne
     const int nchunks = (na + 31) >> 5;
     int c = warp - skip;
     int* ctr = &a.work_cnt[s];
+    // with work bins: lane k < kActBins holds the entries of bin k
+    int bcnt = 0;
+    if (kActBins > 1 && lane < kActBins) bcnt = *((volatile int*)&a.act_cnt[1 + lane]);
     while (c < nchunks) {
         int next = 0;
         if (lane == 0) next = nw2 + atomicAdd(ctr, 1);
         const int i = c * 32 + lane;
-        const int e = (i < na) ? act_elem(a, s_abin, i) : -1;
+        int e = -1;
+        if (kActBins > 1) {
+            // entry i of the bins taken one after another (the warp is converged here)
+            int off = i, b = 0;
+#pragma unroll
+            for (int k = 0; k < kActBins - 1; ++k) {
+                const int ck = __shfl_sync(0xffffffffu, bcnt, k);
+                if (b == k && off >= ck) {
+                    off -= ck;
+                    b = k + 1;
+                }
+            }
+            if (i < na) e = a.act_list[(size_t)(1 + b) * a.n + off];
+        } else if (i < na) {
+            e = a.act_list[i];
+        }
         if (e >= 0 && !(has_dirty && a.dirty[e] == round)) {
             const int code = force_element(a, F, cx, e);
             if (!cx.last) {
@@ -2526,9 +2527,7 @@ __global__ void __launch_bounds__(kThreads, DEM_MIN_BLOCKS) dem_frames_kernel(co
                 // escapes of the previous substep); the counters are read
                 // together, before any branch on them
                 const int nd = *((volatile int*)&a.dirty_cnt[s]);
-                int na = 0;
-#pragma unroll
-                for (int b = 0; b < kActBins; ++b) na += *((volatile int*)&a.act_cnt[b]);
+                const int na = *((volatile int*)a.act_cnt);
                 phase_force(a, F, s, round, all ? 0 : nd, (cnt == 0u) ? n_lazy : 0, na);
             }
         }
