@@ -545,8 +545,9 @@ class ScreenedScorer:
             all_terms = self.dem_all.terms(Yn)
             self._adapt(self._ext, all_terms[:, 4:7])
             return self.dem_all.total(all_terms)
-        if self.n_check and self.adapt_steps > 0:
-            self._adapt(self._ext[chk], terms[self.k:, 4:7])
+        if self.n_check > nb and self.adapt_steps > 0:
+            # the rest's check sample: drawn at random, unlike the top_k and the band
+            self._adapt(self._ext[chk[nb:]], terms[self.k + nb:, 4:7])
         cost = torch.full_like(pred, float("inf"))
         cost[idx] = exact
         if band is not None and band_miss > self.max_rel_err:
