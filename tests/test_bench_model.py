@@ -40,3 +40,16 @@ def test_reference_arm_slabs_cover_the_field_once():
     order = np.argsort(np.random.default_rng(0).random(N), kind="stable")
     parts = np.array_split(order, 16)
     assert sorted(np.concatenate(parts).tolist()) == list(range(N))
+
+
+def test_reference_arm_runs_the_whole_small_field_on_cpu():
+    """bench.py --impl reference on the small field: every element of the field
+    is stepped, as one slab per process, and the line carries the reference
+    arm's keys."""
+    import argparse
+    args = argparse.Namespace(config="small", seed=0, steps=2, warmup=3, horizon=64)
+    line = bench.run_reference(args)
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "elem-steps/s"
+    cfg = line["config"]
+    assert cfg["elements"] == sum(cfg["elements_per_process"]) == bench.load_field("small", 0).n
+    assert line["cpu_baseline"]["cores"] == cfg["processes"] and line["e2e"]["h2d_bytes_per_step"] == 0
