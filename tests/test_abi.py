@@ -67,3 +67,24 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.dem_frame_step(None, None, None, None, None, None, None, None, None, None, None, None) \
         == _abi.DEM_ERR_INVALID
     assert lib.dem_destroy(None) == _abi.DEM_OK
+
+
+def test_sweep_features_rejects_bad_arguments_without_a_gpu():
+    """dem_rollout_sweep_features checks its sizes and pointers before any CUDA call."""
+    from mbd_icenav_b200 import _abi
+    lib = _abi.load_library()
+    f32 = _abi.DEM_F32
+    p = 16  # any non-null value: nothing is dereferenced before the checks fail
+    args = dict(dtype=f32, Q=4, H=8, eta0=p, hist=p, n=10, pos=p, radii=p, mass=p, nb=0, bi=None, bj=None,
+                hl=30.0, hw=6.0, dt=0.05, out=p)
+
+    def call(**kw):
+        a = dict(args, **kw)
+        return lib.dem_rollout_sweep_features(a["dtype"], a["Q"], a["H"], a["eta0"], a["hist"], a["n"], a["pos"],
+                                              a["radii"], a["mass"], a["nb"], a["bi"], a["bj"], a["hl"], a["hw"],
+                                              a["dt"], a["out"], None)
+
+    bad = [dict(dtype=7), dict(Q=0), dict(H=0), dict(H=513), dict(n=65537), dict(n=-1), dict(dt=0.0),
+           dict(hl=-1.0), dict(eta0=None), dict(out=None), dict(pos=None), dict(nb=3), dict(hist=None)]
+    for kw in bad:
+        assert call(**kw) == _abi.DEM_ERR_INVALID, kw
